@@ -1,0 +1,306 @@
+"""Device pipeline for one problem layout: S, C^-1, Fisher, QML, lnL.
+
+The host code here only sequences device kernels from ``libcfb200.so`` on a
+CUDA stream; device memory comes from PyTorch.  Stages (reference
+counterparts in brackets):
+
+* ``signal``       S = sum_l C~_l kernels  [cosmocore/signal_kernels.py:390-537]
+* ``spd_inverse``  C^-1 by the Jacobi-scaled Cholesky inverse
+                   [cosmocore/basics/linalg.py:152-219]
+* ``fisher_qml``   per spectrum: derivative blocks dC_b of all its bins in one
+                   pass, A_b = C^-1 dC_b (and A_b^T) on the DMMA GEMM, Fisher
+                   traces as dense contractions against every earlier
+                   spectrum, noise bias and quadratic forms from the same
+                   derivative blocks  [qube/fisher.py:501-607,
+                   qube/spectra.py:1124-1186]
+* ``lnl``          batched S(theta) + s N, Cholesky, chi2 and ln|C| from the
+                   factor  [picslike/picslike.py:568-664]
+
+Memory layout in HBM: all matrices row-major FP64.  A_b is kept per column
+segment (one field's rows) as n x (nbins * m) slabs for every spectrum seen
+so far; A_b^T slabs only for the spectrum being processed.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import layout as lay
+from ._lib import check, lib, ptr, stream
+
+F64 = torch.float64
+
+
+def _off(t: torch.Tensor, elems: int) -> int:
+    return t.data_ptr() + int(elems) * t.element_size()
+
+
+class Engine:
+    """Device-resident tables of one layout and the kernels that use them."""
+
+    def __init__(self, L: lay.Layout, device=None):
+        self.L = L
+        self.dev = torch.device(device) if device is not None else torch.device("cuda")
+        self.lib = lib()
+        self.vec = [torch.from_numpy(np.ascontiguousarray(f.vectors.T)).to(self.dev, F64)
+                    for f in L.fields]
+        W = L.param_weights()
+        nb, Lmax = L.nbins, L.lmax_signal
+        tabs, bins = [], []
+        for s in range(L.nspectra):
+            t = np.zeros(Lmax + 1)
+            b = np.full(Lmax + 1, -1, dtype=np.int32)
+            for k in range(nb):
+                lo, hi = int(L.bin_lmins[k]), min(int(L.bin_lmaxs[k]), Lmax)
+                if lo <= hi:
+                    b[lo: hi + 1] = k
+                    t[lo: hi + 1] = W[s * nb + k, lo: hi + 1]
+            tabs.append(t)
+            bins.append(b)
+        self.deriv_tab = torch.from_numpy(np.stack(tabs)).to(self.dev, F64)
+        self.deriv_bin = torch.from_numpy(np.stack(bins)).to(self.dev, torch.int32)
+        self.block_of_spec = {}
+        for bi, blk in enumerate(L.blocks):
+            for s in blk.spectra:
+                self.block_of_spec[s] = bi
+
+    # ------------------------------------------------------------------
+    def _launch_block(self, blk, mode, tabs, bin_of, out, ld, row_off, col_off, bin_stride,
+                      outT, ldT, rowT_off, colT_off, binT_stride, batch=1, tstride=0, ostride=0):
+        L = self.L
+        fa, fb = L.fields[blk.fa], L.fields[blk.fb]
+        va, vb = self.vec[blk.fa], self.vec[blk.fb]
+        t0, t1, t2 = (tabs + [None, None, None])[:3]
+        rc = self.lib.cf_build_block(
+            blk.kind, mode, fa.npix, va.data_ptr(), fb.npix, vb.data_ptr(), L.lmax_signal,
+            t0, t1, t2, bin_of, out, ld, row_off, col_off, bin_stride, outT, ldT, rowT_off,
+            colT_off, binT_stride, batch, tstride, ostride, stream())
+        check(rc, "cf_build_block")
+
+    def signal(self, cl_table, out: torch.Tensor | None = None) -> torch.Tensor:
+        """S (n x n) or a batch (B x n x n) from beam-smoothed C_l tables.
+
+        ``cl_table``: (nspectra, L+1) or (B, nspectra, L+1) in spectrum order.
+        """
+        L = self.L
+        cl = torch.as_tensor(cl_table, dtype=F64, device=self.dev).contiguous()
+        batched = cl.dim() == 3
+        B = cl.shape[0] if batched else 1
+        n, Lp = L.n, L.lmax_signal + 1
+        if out is None:
+            out = torch.zeros((B, n, n) if batched else (n, n), dtype=F64, device=self.dev)
+        tstride = L.nspectra * Lp
+        for blk in L.blocks:
+            fa, fb = L.fields[blk.fa], L.fields[blk.fb]
+            by_mode = {L.spectra[k].mode: k for k in blk.spectra}
+            if blk.kind in (lay.KIND_00_AUTO, lay.KIND_00_CROSS):
+                order = [blk.spectra[0]]
+            elif blk.kind == lay.KIND_22_AUTO:
+                order = [by_mode.get(0), by_mode.get(1), by_mode.get(2)]
+            else:
+                order = [by_mode.get(0), by_mode.get(1)]
+            tabs = [None if k is None else _off(cl, k * Lp) for k in order]
+            if tabs[0] is None:
+                continue
+            self._launch_block(blk, -1, tabs, None, out.data_ptr(), n, fb.offset, fa.offset, 0,
+                               out.data_ptr(), n, fa.offset, fb.offset, 0, batch=B,
+                               tstride=tstride, ostride=n * n)
+        return out
+
+    # ------------------------------------------------------------------
+    def spd_inverse(self, A: torch.Tensor) -> torch.Tensor:
+        """In place Jacobi-scaled Cholesky inverse of one SPD matrix or a batch."""
+        n = A.shape[-1]
+        B = A.shape[0] if A.dim() == 3 else 1
+        ws = self.lib.cf_spd_inverse_workspace(n, B)
+        work = torch.empty(ws // 8 + 1, dtype=F64, device=A.device)
+        info = torch.zeros(B, dtype=torch.int32, device=A.device)
+        check(self.lib.cf_spd_inverse(n, A.data_ptr(), n, n * n, B, work.data_ptr(), info.data_ptr(),
+                                      stream()), "cf_spd_inverse")
+        bad = info.cpu()
+        if int(bad.abs().max()) != 0:
+            raise ValueError(f"dpotrf failed with info={int(bad[bad != 0][0])}")
+        return A
+
+    def gemm(self, A, B, C=None, alpha=1.0, beta=0.0, transa=False, transb=False, CT=None):
+        M = A.shape[1] if transa else A.shape[0]
+        K = A.shape[0] if transa else A.shape[1]
+        N = B.shape[0] if transb else B.shape[1]
+        if C is None:
+            C = torch.empty((M, N), dtype=F64, device=A.device)
+        check(self.lib.cf_dgemm(int(transa), int(transb), M, N, K, alpha, A.data_ptr(), A.stride(0), 0,
+                                B.data_ptr(), B.stride(0), 0, beta, C.data_ptr(), C.stride(0), 0,
+                                ptr(CT), CT.stride(0) if CT is not None else 0, 0, 1, 0, stream()),
+              "cf_dgemm")
+        return C
+
+    # ------------------------------------------------------------------
+    def _deriv_blocks(self, s: int):
+        """Derivative blocks of every bin of spectrum s, in one build pass."""
+        L = self.L
+        blk = L.blocks[self.block_of_spec[s]]
+        fa, fb = L.fields[blk.fa], L.fields[blk.fb]
+        nb, Lp = L.nbins, L.lmax_signal + 1
+        mode = L.spectra[s].mode
+        tab = [_off(self.deriv_tab, s * Lp)]
+        bins = _off(self.deriv_bin, s * Lp)
+        if blk.kind in (lay.KIND_00_AUTO, lay.KIND_22_AUTO):
+            m = fa.nrows
+            D = torch.zeros((m, nb * m), dtype=F64, device=self.dev)
+            self._launch_block(blk, mode, tab, bins, D.data_ptr(), nb * m, 0, 0, m,
+                               D.data_ptr(), nb * m, 0, 0, m)
+            return blk, {"auto": D}
+        R, Cc = fb.nrows, fa.nrows
+        Dba = torch.zeros((R, nb * Cc), dtype=F64, device=self.dev)
+        Dab = torch.zeros((Cc, nb * R), dtype=F64, device=self.dev)
+        self._launch_block(blk, mode, tab, bins, Dba.data_ptr(), nb * Cc, 0, 0, Cc,
+                           Dab.data_ptr(), nb * R, 0, 0, R)
+        return blk, {"ba": Dba, "ab": Dab}
+
+    def derivative_dense(self, p: int) -> torch.Tensor:
+        """Full n x n dC_p (test helper; the Fisher path never forms it)."""
+        L = self.L
+        s, b = divmod(p, L.nbins)
+        blk, D = self._deriv_blocks(s)
+        fa, fb = L.fields[blk.fa], L.fields[blk.fb]
+        out = torch.zeros((L.n, L.n), dtype=F64, device=self.dev)
+        if "auto" in D:
+            m = fa.nrows
+            out[fa.offset: fa.offset + m, fa.offset: fa.offset + m] = D["auto"][:, b * m:(b + 1) * m]
+        else:
+            R, Cc = fb.nrows, fa.nrows
+            blkba = D["ba"][:, b * Cc:(b + 1) * Cc]
+            out[fb.offset: fb.offset + R, fa.offset: fa.offset + Cc] = blkba
+            out[fa.offset: fa.offset + Cc, fb.offset: fb.offset + R] = D["ab"][:, b * R:(b + 1) * R]
+        return out
+
+    def fisher_qml(self, Cinv: torch.Tensor, N: torch.Tensor | None = None,
+                   maps: torch.Tensor | None = None, want_fisher: bool = True):
+        """F (P x P), raw bias (P,), raw q (nsims x P) by per-spectrum passes."""
+        L = self.L
+        n, nb, P = L.n, L.nbins, L.n_params
+        dev = self.dev
+        F = torch.zeros((P, P), dtype=F64, device=dev)
+        bias = torch.zeros(P, dtype=F64, device=dev) if N is not None else None
+        Y = None
+        nsims = 0
+        if maps is not None:
+            X = maps.to(dev, F64).contiguous()
+            nsims = X.shape[1]
+            Y = self.gemm(Cinv, X)
+            q = torch.zeros((nsims, P), dtype=F64, device=dev)
+        else:
+            q = None
+        M = None
+        if N is not None:
+            M = self.gemm(Cinv, self.gemm(N, Cinv))
+        X_slabs = {}
+        seg = {i: (f.offset, f.nrows) for i, f in enumerate(L.fields)}
+        cols_of = {}
+        for s2 in range(L.nspectra):
+            blk, D = self._deriv_blocks(s2)
+            fa, fb = L.fields[blk.fa], L.fields[blk.fb]
+            # ---- noise bias and quadratic forms from the derivative blocks
+            if M is not None or Y is not None:
+                if "auto" in D:
+                    args = (D["auto"], fa.nrows, fa.nrows, fa.offset, fa.offset, 0.5)
+                else:
+                    args = (D["ba"], fb.nrows, fa.nrows, fb.offset, fa.offset, 1.0)
+                Dm, R, Cc, ro, co, scale = args
+                for m0 in range(0, max(nsims, 1), 4):
+                    use_y = Y is not None and m0 < nsims
+                    check(self.lib.cf_qml_reduce_f64(
+                        nb, R, Cc, Dm.data_ptr(), Dm.stride(0), Cc,
+                        ptr(M) if m0 == 0 else None, n, ro, co,
+                        _off(Y, m0) if use_y else None, nsims, min(4, nsims - m0) if use_y else 0,
+                        ro, co, scale, _off(bias, s2 * nb) if (bias is not None and m0 == 0) else None,
+                        _off(q, m0 * P + s2 * nb) if use_y else None, P, stream()), "cf_qml_reduce_f64")
+            if not want_fisher:
+                continue
+            # ---- A_b slabs (and their transposes) for this spectrum
+            XT = {}
+            if "auto" in D:
+                sa = blk.fa
+                off, m = seg[sa]
+                Xs = torch.empty((n, nb * m), dtype=F64, device=dev)
+                XTs = torch.empty((nb * m, n), dtype=F64, device=dev)
+                self.gemm(Cinv[:, off:off + m], D["auto"], C=Xs, CT=XTs)
+                X_slabs[(s2, sa)] = Xs
+                XT[sa] = XTs
+                cols_of[s2] = [sa]
+            else:
+                (oa, ma), (ob, mb) = seg[blk.fa], seg[blk.fb]
+                Xa = torch.empty((n, nb * ma), dtype=F64, device=dev)
+                XTa = torch.empty((nb * ma, n), dtype=F64, device=dev)
+                self.gemm(Cinv[:, ob:ob + mb], D["ba"], C=Xa, CT=XTa)
+                Xb = torch.empty((n, nb * mb), dtype=F64, device=dev)
+                XTb = torch.empty((nb * mb, n), dtype=F64, device=dev)
+                self.gemm(Cinv[:, oa:oa + ma], D["ab"], C=Xb, CT=XTb)
+                X_slabs[(s2, blk.fa)] = Xa
+                X_slabs[(s2, blk.fb)] = Xb
+                XT[blk.fa] = XTa
+                XT[blk.fb] = XTb
+                cols_of[s2] = [blk.fa, blk.fb]
+            del D
+            # ---- Fisher traces of this spectrum against every spectrum so far
+            for s1 in range(s2 + 1):
+                for ss in cols_of[s1]:
+                    s_off, m_s = seg[ss]
+                    Xs = X_slabs[(s1, ss)]
+                    for tt in cols_of[s2]:
+                        t_off, m_t = seg[tt]
+                        Yt = XT[tt]
+                        check(self.lib.cf_trace_contract_f64(
+                            nb, nb, m_t, m_s, _off(Xs, t_off * Xs.stride(0)), m_s, Xs.stride(0),
+                            _off(Yt, s_off), m_t * n, n, 0.5, F.data_ptr(), P, s1 * nb, s2 * nb,
+                            int(s1 != s2), 0, stream()), "cf_trace_contract_f64")
+            del XT
+        del X_slabs
+        return F, bias, q
+
+    # ------------------------------------------------------------------
+    def potrf(self, A: torch.Tensor) -> torch.Tensor:
+        n = A.shape[-1]
+        B = A.shape[0] if A.dim() == 3 else 1
+        info = torch.zeros(B, dtype=torch.int32, device=A.device)
+        check(self.lib.cf_potrf(n, A.data_ptr(), n, n * n, B, info.data_ptr(), stream()), "cf_potrf")
+        return info
+
+    def lnl(self, cl_tables, N: torch.Tensor, maps: torch.Tensor, noise_scale=None):
+        """chi2 (B x nsims), ln|C| (B,), lnL (B x nsims), info (B,) for a batch of points."""
+        cl = torch.as_tensor(cl_tables, dtype=F64, device=self.dev)
+        if cl.dim() == 2:
+            cl = cl[None]
+        B = cl.shape[0]
+        n = self.L.n
+        C = self.signal(cl)
+        sc = None
+        if noise_scale is not None:
+            sc = torch.as_tensor(noise_scale, dtype=F64, device=self.dev).reshape(B).contiguous()
+        check(self.lib.cf_axpby(n * n, 1.0, C.data_ptr(), n * n, 1.0, ptr(sc), N.data_ptr(), 0,
+                                C.data_ptr(), n * n, B, stream()), "cf_axpby")
+        info = self.potrf(C)
+        X = maps.to(self.dev, F64).contiguous()
+        nsims = X.shape[1]
+        z = torch.empty((B * nsims, n), dtype=F64, device=self.dev)
+        chi2 = torch.empty((B, nsims), dtype=F64, device=self.dev)
+        logdet = torch.empty(B, dtype=F64, device=self.dev)
+        check(self.lib.cf_chi2_logdet(n, C.data_ptr(), n, n * n, B, X.data_ptr(), nsims, 0, nsims,
+                                      z.data_ptr(), chi2.data_ptr(), logdet.data_ptr(), stream()),
+              "cf_chi2_logdet")
+        return chi2, logdet, -0.5 * (chi2 + logdet[:, None]), info
+
+
+def qml_solve(E: Engine, cls: dict, N: torch.Tensor, maps: torch.Tensor):
+    """S, C^-1, F, q, bias, F^-1, C_hat on the device (plain FP64)."""
+    L = E.L
+    S = E.signal(L.smoothed_cl_table(cls))
+    Cinv = S + N
+    E.spd_inverse(Cinv)
+    F, bias, q = E.fisher_qml(Cinv, N, maps)
+    Finv = E.spd_inverse(F.clone())
+    if L.remove_nb:
+        q = q - bias[None, :]
+    return dict(S=S, Cinv=Cinv, fisher=F, q=q, bias=bias, invfisher=Finv,
+                clhat=E.gemm(q, Finv), noise_bias=E.gemm(bias[None, :], Finv)[0])
