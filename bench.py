@@ -1,0 +1,362 @@
+#!/usr/bin/env python
+"""QML solves/s on the TQU nside-16 problem (n = 5952 pixels, 276 Fisher parameters).
+
+One step = one complete QML solve for one map: signal matrix S, C = S + N,
+C^-1, the 276 x 276 Fisher matrix, raw bandpowers q, noise bias, F^-1 and
+C_hat.  ``value`` is whole-job solves/s with every input already resident in
+HBM; ``e2e`` is the same metric through the drop-in ``Fisher`` / ``Spectra``
+API with host inputs (pinned) copied in and results copied out each step.
+
+``--impl reference`` times the CPU restatement of the reference algorithm
+(the oracle: C build with OpenMP, LAPACK/OpenBLAS linear algebra) on a
+bounded sample of the same problem and extrapolates it to a full solve.
+
+Multi-GPU (``torchrun``): the path does not shard (north_star: one GPU per
+problem), so N GPUs run N independent replicas; time is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+WORKLOAD = "config1_tqu_nside16_qml"
+METRIC = "QML solves/s (TQU nside16, n=5952, 276 bandpowers)"
+UNIT = "solves/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--lmax", type=int, default=None,
+                    help="override the inference lmax (smaller profiling case; not a bench line)")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------------
+# CPU baseline: oracle on a bounded sample of the workload, extrapolated
+# --------------------------------------------------------------------------
+def cpu_sample(pb, L, k_params: int = 2):
+    """Time S, C^-1, k parameters (dC, A = C^-1 dC, bias, q) and their traces.
+
+    Extrapolates t_fixed + 276 t_param + 276*277/2 t_trace to one full solve.
+    """
+    from oracle import oracle as orc
+
+    t0 = time.perf_counter()
+    S = orc.signal_matrix(L, L.smoothed_cl_table(pb.cls))
+    t_s = time.perf_counter() - t0
+    N = pb.noise
+    t0 = time.perf_counter()
+    Cinv = orc.matrix_inverse_symm(S + N)
+    Y = Cinv @ pb.extra["maps"]
+    M = Cinv @ (N @ Cinv)
+    t_inv = time.perf_counter() - t0
+    W = L.param_weights()
+    picks = np.linspace(0, L.n_params - 1, k_params).astype(int)
+    A, AT = [], []
+    t0 = time.perf_counter()
+    for p in picks:
+        dC = orc.binned_derivative(L, int(p), W)
+        a = Cinv @ dC
+        A.append(a)
+        AT.append(np.ascontiguousarray(a.T))
+        _ = 0.5 * orc.trace_product(M, dC)
+        _ = 0.5 * np.sum(Y * (dC @ Y))
+    t_param = (time.perf_counter() - t0) / k_params
+    t0 = time.perf_counter()
+    ntr = 0
+    for i in range(k_params):
+        for j in range(i, k_params):
+            orc.trace_product(A[i], A[j], AT[j])
+            ntr += 1
+    t_trace = (time.perf_counter() - t0) / ntr
+    P = L.n_params
+    total = t_s + t_inv + P * t_param + P * (P + 1) / 2 * t_trace
+    sample = (f"S + C^-1 + {k_params} of {P} parameters (dC, A=C^-1 dC, bias, q) + {ntr} traces, "
+              f"extrapolated: t_S {t_s:.2f}s + t_inv {t_inv:.2f}s + {P} x {t_param:.2f}s + "
+              f"{P * (P + 1) // 2} x {t_trace:.3f}s = {total:.0f}s per solve")
+    return 1.0 / total, sample, total
+
+
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference(args):
+    """Reference arm: the oracle restatement on host cores (rank 0 only)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from cosmoforge_b200 import workloads
+    from cosmoforge_b200.layout import build_layout
+
+    pb = workloads.config1()
+    L = build_layout(pb.params, pb.mask, pb.beam)
+    pb.extra["maps"] = np.random.default_rng(0).standard_normal((L.n, 1))
+    vals = []
+    sample = ""
+    for i in range(args.warmup + args.steps):
+        v, sample, _ = cpu_sample(pb, L, k_params=1)
+        if i >= args.warmup:
+            vals.append(v)
+    v = statistics.median(vals)
+    cores = cpu_threads()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)", "config": {"workload": WORKLOAD, "n_pixels": L.n,
+                                                 "n_params": L.n_params, "nsims": 1},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------
+# GPU arm
+# --------------------------------------------------------------------------
+class ClockSampler:
+    def __init__(self, index: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+        self.index = index
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=clocks.sm,clocks.max.sm,"
+                 "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.p is not None:
+            self.p.terminate()
+            self.p.wait()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 7 and parts[0].isdigit():
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [int(r[0]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[3 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": int(rows[0][1]), "reasons": reasons,
+                "samples": len(rows)}
+
+
+def fp64_peak_tflops(torch):
+    """Measured FP64 tensor peak: cuBLAS DGEMM 8192^3, best of 3 (for the FP64 roofline)."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    best = 1e9
+    for _ in range(3):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del a, b
+    return 2 * 8192**3 / best / 1e12
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+
+    from cosmoforge_b200 import _lib, engine, qube, workloads
+    from cosmoforge_b200.layout import build_layout
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    pb = workloads.config1()
+    if args.lmax is not None:
+        pb.params["lmax"] = args.lmax
+    L = build_layout(pb.params, pb.mask, pb.beam)
+    dev = torch.device("cuda", local)
+    E = engine.Engine(L, dev)
+    N = torch.from_numpy(pb.noise).to(dev)
+    X = qube.draw_maps(L, pb.cls, N, nsims=1, seed=0, device=dev)
+    cl_tab = torch.from_numpy(L.smoothed_cl_table(pb.cls)).to(dev)
+    lib = _lib.lib()
+
+    def step():
+        S = E.signal(cl_tab)
+        C = S.add_(N)
+        E.spd_inverse(C)
+        if args.precision == "mixed":
+            from cosmoforge_b200 import engine_mixed
+
+            F, bias, q = engine_mixed.fisher_qml(E, C, N, X)
+        else:
+            F, bias, q = E.fisher_qml(C, N, X)
+        Finv = E.spd_inverse(F.clone())
+        if L.remove_nb:
+            q = q - bias[None, :]
+        return E.gemm(q, Finv)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    E.probe = {}
+    barrier()
+    torch.cuda.synchronize()
+    n0 = lib.cf_launch_count()
+    with ClockSampler(local) as clk:
+        t_start = torch.cuda.Event(enable_timing=True)
+        t_end = torch.cuda.Event(enable_timing=True)
+        t_start.record()
+        for _ in range(args.steps):
+            out = step()
+        t_end.record()
+        torch.cuda.synchronize()
+    barrier()
+    launches = (lib.cf_launch_count() - n0) // max(args.steps, 1)
+    elapsed = t_start.elapsed_time(t_end) / 1e3
+    t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    elapsed = float(t.item())
+    value = world * args.steps / elapsed
+    clocks = clk.summary()
+    tags = E.probe
+    E.probe = None
+    dom = "a_gemm"
+    recs = tags.get(dom, [])
+    k_time = sum(a.elapsed_time(b) for a, b, _ in recs) / 1e3
+    k_work = sum(w for _, _, w in recs)
+    n_launch = max(len(recs), 1)
+    assert bool(torch.isfinite(out).all())
+
+    # ---- end-to-end through the public API, host inputs and outputs ----
+    Nh = torch.from_numpy(pb.noise).pin_memory()
+    Xh = X.cpu().pin_memory()
+    h2d = Nh.numel() * 8 + Xh.numel() * 8
+    e2e_times = []
+    d2h = 0
+    for i in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        f = qube.Fisher(pb.params, basis=False, mask=pb.mask, noise_cov1=Nh, cls_data=pb.cls,
+                        beam=pb.beam, precision=args.precision, device=dev)
+        f.run()
+        s = qube.Spectra(pb.params, fisher=f, maps1=Xh)
+        s.run()
+        clhat = s.get_power_spectra()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        d2h = (f.fisher.nbytes + s.qml_results.nbytes + s.qml_noise_bias.nbytes + s.invfisher.nbytes
+               + clhat.nbytes)
+        if i > 0:
+            e2e_times.append(dt)
+    tt = torch.tensor([max(e2e_times) if e2e_times else float("nan")], dtype=torch.float64,
+                      device=dev)
+    if world > 1:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    e2e_value = world / float(tt.item()) if e2e_times else None
+
+    line = None
+    if rank == 0:
+        import json as _json
+
+        peaks = {}
+        pk = ROOT / "MEASURED_PEAKS.json"
+        if pk.exists():
+            peaks = _json.loads(pk.read_text())
+        if args.precision == "fp64":
+            peak = fp64_peak_tflops(torch)
+            peak_src = "measured cuBLAS DGEMM 8192^3 in this run (FP64 tensor)"
+        else:
+            peak = peaks.get("bf16_tflops", 1590.0)
+            peak_src = "MEASURED_PEAKS.json bf16_tflops" if peaks else "fallback 1.59 PFLOP/s"
+        achieved = k_work / k_time / 1e12 if k_time > 0 else 0.0
+        traffic = None
+        tf = ROOT / "profiles" / "traffic.json"
+        if tf.exists():
+            traffic = _json.loads(tf.read_text()).get(f"{dom}_{args.precision}")
+        cpu = None
+        if not args.no_cpu_baseline:
+            pbc = workloads.config1()
+            pbc.extra["maps"] = X.cpu().numpy()
+            v, sample, _ = cpu_sample(pbc, L, k_params=2)
+            cpu = {"value": v, "unit": UNIT, "cores": cpu_threads(), "kind": "port", "sample": sample}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "bf16x3/f32+f64",
+            "data": "synthetic (seeded): config-1 TQU problem, x ~ N(0, C) drawn on device",
+            "config": {"workload": WORKLOAD, "n_pixels": L.n, "n_params": L.n_params, "nsims": 1,
+                       "lmax_signal": L.lmax_signal, "precision": args.precision,
+                       "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (C^-1 283 MB, "
+                       "A_b slabs 56 GB)"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "roofline": {"bound": "tensor", "kernel": dom, "achieved": achieved, "peak": peak,
+                         "peak_source": peak_src, "unit": "TFLOP/s", "frac": achieved / peak,
+                         "traffic": traffic, "launches_timed": n_launch,
+                         "work_per_launch": k_work / n_launch},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "gpu_launches": int(launches),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -23,6 +23,7 @@ _i, _l, _d, _p, _sz = C.c_int, C.c_long, C.c_double, C.c_void_p, C.c_size_t
 
 SIGNATURES = {
     "cf_version": (_i, []),
+    "cf_launch_count": (C.c_ulonglong, []),
     "cf_build_block": (_i, [_i, _i, _i, _p, _i, _p, _i, _p, _p, _p, _p, _p, _l, _l, _l, _l, _p, _l,
                             _l, _l, _l, _i, _l, _l, _p]),
     "cf_dgemm": (_i, [_i, _i, _i, _i, _i, _d, _p, _l, _l, _p, _l, _l, _d, _p, _l, _l, _p, _l, _l,

@@ -11,9 +11,14 @@
 
 #define CF_PI 3.14159265358979323846
 
-// Return CF_ERR_CUDA from the enclosing function if the last launch failed.
+// Number of kernels this library has launched (host-side count, read by
+// cf_launch_count); every launch site goes through CF_CHECK_LAUNCH.
+extern unsigned long long g_cf_launch_count;
+
+// Count the launch and return CF_ERR_CUDA from the enclosing function if it failed.
 #define CF_CHECK_LAUNCH()                                  \
     do {                                                   \
+        ++g_cf_launch_count;                               \
         cudaError_t e_ = cudaGetLastError();               \
         if (e_ != cudaSuccess) return CF_ERR_CUDA;         \
     } while (0)

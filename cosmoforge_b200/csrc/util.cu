@@ -55,4 +55,8 @@ extern "C" int cf_transpose(int R, int C, const double* A, long lda, double* B, 
     return CF_OK;
 }
 
+unsigned long long g_cf_launch_count = 0;
+
+extern "C" unsigned long long cf_launch_count(void) { return g_cf_launch_count; }
+
 extern "C" int cf_version(void) { return 1; }

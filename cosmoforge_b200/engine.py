@@ -60,6 +60,7 @@ class Engine:
             bins.append(b)
         self.deriv_tab = torch.from_numpy(np.stack(tabs)).to(self.dev, F64)
         self.deriv_bin = torch.from_numpy(np.stack(bins)).to(self.dev, torch.int32)
+        self.probe = None  # {tag: [(start_event, end_event, work)]} when timing kernels
         self.block_of_spec = {}
         for bi, blk in enumerate(L.blocks):
             for s in blk.spectra:
@@ -123,16 +124,34 @@ class Engine:
             raise ValueError(f"dpotrf failed with info={int(bad[bad != 0][0])}")
         return A
 
-    def gemm(self, A, B, C=None, alpha=1.0, beta=0.0, transa=False, transb=False, CT=None):
+    def _probe_begin(self, tag):
+        if self.probe is None:
+            return None
+        ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        ev[0].record()
+        return ev
+
+    def _probe_end(self, tag, ev, work):
+        if ev is not None:
+            ev[1].record()
+            self.probe.setdefault(tag, []).append((ev[0], ev[1], float(work)))
+
+    def gemm(self, A, B, C=None, alpha=1.0, beta=0.0, transa=False, transb=False, CT=None, tag=None):
         M = A.shape[1] if transa else A.shape[0]
         K = A.shape[0] if transa else A.shape[1]
         N = B.shape[0] if transb else B.shape[1]
         if C is None:
             C = torch.empty((M, N), dtype=F64, device=A.device)
+        ev = self._probe_begin(tag) if tag else None
+        if tag:
+            torch.cuda.nvtx.range_push(tag)
         check(self.lib.cf_dgemm(int(transa), int(transb), M, N, K, alpha, A.data_ptr(), A.stride(0), 0,
                                 B.data_ptr(), B.stride(0), 0, beta, C.data_ptr(), C.stride(0), 0,
                                 ptr(CT), CT.stride(0) if CT is not None else 0, 0, 1, 0, stream()),
               "cf_dgemm")
+        if tag:
+            torch.cuda.nvtx.range_pop()
+            self._probe_end(tag, ev, 2.0 * M * N * K)
         return C
 
     # ------------------------------------------------------------------
@@ -225,7 +244,7 @@ class Engine:
                 off, m = seg[sa]
                 Xs = torch.empty((n, nb * m), dtype=F64, device=dev)
                 XTs = torch.empty((nb * m, n), dtype=F64, device=dev)
-                self.gemm(Cinv[:, off:off + m], D["auto"], C=Xs, CT=XTs)
+                self.gemm(Cinv[:, off:off + m], D["auto"], C=Xs, CT=XTs, tag="a_gemm")
                 X_slabs[(s2, sa)] = Xs
                 XT[sa] = XTs
                 cols_of[s2] = [sa]
@@ -233,10 +252,10 @@ class Engine:
                 (oa, ma), (ob, mb) = seg[blk.fa], seg[blk.fb]
                 Xa = torch.empty((n, nb * ma), dtype=F64, device=dev)
                 XTa = torch.empty((nb * ma, n), dtype=F64, device=dev)
-                self.gemm(Cinv[:, ob:ob + mb], D["ba"], C=Xa, CT=XTa)
+                self.gemm(Cinv[:, ob:ob + mb], D["ba"], C=Xa, CT=XTa, tag="a_gemm")
                 Xb = torch.empty((n, nb * mb), dtype=F64, device=dev)
                 XTb = torch.empty((nb * mb, n), dtype=F64, device=dev)
-                self.gemm(Cinv[:, oa:oa + ma], D["ab"], C=Xb, CT=XTb)
+                self.gemm(Cinv[:, oa:oa + ma], D["ab"], C=Xb, CT=XTb, tag="a_gemm")
                 X_slabs[(s2, blk.fa)] = Xa
                 X_slabs[(s2, blk.fb)] = Xb
                 XT[blk.fa] = XTa

@@ -1,0 +1,359 @@
+"""Drop-in ``Fisher`` and ``Spectra`` with the reference's constructor and outputs.
+
+Same signatures, seams and result layouts as ``qube.Fisher``
+(``qube/fisher.py:141-266, 826-1049``) and ``qube.Spectra``
+(``qube/spectra.py:205-395, 1358-1733``): the parameter axis is
+spectrum-major, bin-minor in ``spectra_list`` order; power spectra are
+(nsims, n_params); ``noise_cov1`` is rebound to C^-1 after ``run()`` and the
+injected N stays in ``reduced_noise_cov1``.  The computation runs on the GPU
+through ``libcfb200.so``; host copies of the n x n matrices are made only
+when those attributes are read.
+
+Supported: the pixel-space estimator (``basis=False`` / ``"pixel"``; the
+default ``None`` is served by the same exact pixel path), SYMMETRIC spectra,
+auto-spectra (``do_cross=False``), injected arrays.  The harmonic / compressed
+bases, pixel filters and file inputs raise ``NotImplementedError``.
+
+``precision``: ``"fp64"`` (plain FP64 everywhere) or ``"mixed"`` (BF16x3 /
+FP32 tensor-core traces with FP64 refinement, see ``engine_mixed``).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import engine as eng
+from . import layout as lay
+from . import params as prm
+
+_LAYOUT_CACHE: dict = {}
+
+
+def _layout(p: dict, mask, beam) -> lay.Layout:
+    """Layouts are pure functions of (geometry params, mask, beam): cache them."""
+    mask = np.asarray(mask, dtype=np.float64)
+    key = (p["nside"], tuple(p["spins"]), tuple(p["labels"]), p.get("ordering", "RING"),
+           p.get("lmin"), p.get("lmax"), p.get("lmax_signal"), p.get("delta_ell"),
+           str(p.get("bin_lmins")), str(p.get("bin_lmaxs")), p.get("output_convention"),
+           bool(p.get("remove_nb", True)), mask.tobytes().__hash__(),
+           None if beam is None else np.asarray(beam, dtype=np.float64).tobytes().__hash__())
+    L = _LAYOUT_CACHE.get(key)
+    if L is None:
+        L = lay.build_layout(p, mask, beam)
+        if len(_LAYOUT_CACHE) > 16:
+            _LAYOUT_CACHE.clear()
+        _LAYOUT_CACHE[key] = L
+    L.nsims = int(p.get("nsims") or 1)
+    return L
+
+
+def _check_basis(basis):
+    if basis is None or basis is False or basis == "pixel":
+        return
+    if isinstance(basis, dict) and basis.get("method", "pixel") == "pixel" and not (
+            set(basis) & {"epsilon", "compression_target", "mode_fraction"}):
+        return
+    raise NotImplementedError(f"basis={basis!r}: only the exact pixel-space path is implemented")
+
+
+def _check_kwargs(kwargs):
+    for k in ("pixel_filter",):
+        if kwargs.get(k) is not None:
+            raise NotImplementedError(f"{k} is not supported by the device path")
+
+
+class _Base:
+    def __init__(self, params, params_file, mask, noise_cov1, noise_cov2, cls_data, fiducial_cls,
+                 beam, precision, device, kwargs):
+        self.params = prm.as_namespace(prm.resolve(params, params_file))
+        _check_kwargs(kwargs)
+        if self.params.do_cross:
+            raise NotImplementedError("do_cross=True (two-map cross spectra) is not supported")
+        if mask is None or noise_cov1 is None or (cls_data is None and fiducial_cls is None):
+            raise NotImplementedError("inject mask, noise_cov1 and cls_data (file inputs unsupported)")
+        self._mask = mask
+        self._noise_in = noise_cov1
+        self._cls = cls_data if cls_data is not None else fiducial_cls
+        self._beam = beam
+        if precision not in ("fp64", "mixed"):
+            raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
+        self.precision = precision
+        self.device = torch.device(device) if device is not None else torch.device("cuda")
+        self.rank = 0
+        self.size = 1
+
+    @property
+    def lmax_signal(self) -> int:
+        v = getattr(self.params, "lmax_signal", None)
+        return 4 * self.params.nside if v is None else int(v)
+
+    def _setup(self):
+        p = vars(self.params)
+        self.layout = _layout(p, self._mask, self._beam)
+        L = self.layout
+        n = L.n
+        N = self._noise_in
+        if isinstance(N, torch.Tensor):
+            if tuple(N.shape) != (n, n):
+                raise ValueError(f"injected noise covariance has shape {tuple(N.shape)}, expected ({n}, {n})")
+            self._dev_N = N.to(self.device, torch.float64)
+        else:
+            N = np.asarray(N, dtype=np.float64)
+            if N.shape != (n, n):
+                raise ValueError(f"injected noise covariance has shape {N.shape}, expected ({n}, {n})")
+            self._dev_N = torch.from_numpy(np.ascontiguousarray(N)).to(self.device, non_blocking=True)
+        self.npixs = [f.npix for f in L.fields]
+        self.spectra_list = L.labels()
+        self.beam_smoothing = L.beam_smoothing_vector()
+        self.n_params = L.n_params
+        self.bins = lay_bins(L)
+
+
+class lay_bins:
+    """Read-only view of the bins with the reference's attribute names."""
+
+    def __init__(self, L: lay.Layout):
+        self.lmins = np.asarray(L.bin_lmins)
+        self.lmaxs = np.asarray(L.bin_lmaxs)
+        self.nbins = L.nbins
+        self.lmin = int(self.lmins[0])
+        self.lmax = int(self.lmaxs[-1])
+        self.lmid = (self.lmins + self.lmaxs) / 2.0
+        self.dl = self.lmaxs - self.lmins + 1
+
+
+class Fisher(_Base):
+    """Fisher matrix F_ij = 1/2 Tr[C^-1 dC^i C^-1 dC^j] on the GPU."""
+
+    def __init__(self, params=None, basis=None, cache_derivatives: bool = False, symmetry_mode=None,
+                 mask=None, noise_cov1=None, noise_cov2=None, cls_data=None, fiducial_cls=None,
+                 beam=None, *, params_file=None, precision: str = "fp64", device=None, **kwargs):
+        _check_basis(basis)
+        if symmetry_mode not in (None, "SYMMETRIC", "symmetric") and getattr(
+                symmetry_mode, "name", "SYMMETRIC") != "SYMMETRIC":
+            raise NotImplementedError("only SymmetryMode.SYMMETRIC is supported")
+        super().__init__(params, params_file, mask, noise_cov1, noise_cov2, cls_data, fiducial_cls,
+                         beam, precision, device, kwargs)
+        self._cache_derivatives = cache_derivatives
+        self.fisher = None
+        self._dev_S = None
+        self._dev_Cinv = None
+        self._host = {}
+        self.timings = {}
+
+    # -- reference attributes, downloaded lazily --------------------------
+    def _host_of(self, key, t):
+        if key not in self._host:
+            self._host[key] = t.cpu().numpy()
+        return self._host[key]
+
+    @property
+    def signal_matrix(self):
+        return None if self._dev_S is None else self._host_of("S", self._dev_S)
+
+    @property
+    def noise_cov1(self):
+        if self._dev_Cinv is None:
+            return self._noise_in
+        return self._host_of("Cinv", self._dev_Cinv)
+
+    @property
+    def reduced_noise_cov1(self):
+        return self._noise_in if self._dev_Cinv is not None else None
+
+    # -- pipeline ---------------------------------------------------------
+    def run(self) -> None:
+        self._setup()
+        L = self.layout
+        self.engine = eng.Engine(L, self.device)
+        self._host = {}
+        self._dev_S = self.engine.signal(L.smoothed_cl_table(self._cls))
+        C = self._dev_S + self._dev_N
+        self._dev_Cinv = self.engine.spd_inverse(C)
+        self.compute()
+
+    def compute(self) -> None:
+        if self.precision == "mixed":
+            from . import engine_mixed
+
+            F = engine_mixed.fisher(self.engine, self._dev_Cinv)
+        else:
+            F, _, _ = self.engine.fisher_qml(self._dev_Cinv)
+        self._dev_F = F
+        self.fisher = F.cpu().numpy()
+
+    # -- accessors (qube/fisher.py:826-1049) -------------------------------
+    def get_fisher_matrix(self):
+        return self.fisher
+
+    def get_window_matrix(self):
+        return self.get_fisher_matrix()
+
+    def get_error_bars(self, *, as_dict: bool = False):
+        if self.fisher is None:
+            return None
+        Finv = self.engine.spd_inverse(self._dev_F.clone()).cpu().numpy()
+        err = np.sqrt(np.diag(Finv))
+        return self._to_dict(err) if as_dict else err
+
+    def get_bandpower_slices(self):
+        if self.spectra_list is None:
+            return None
+        return self.layout.bandpower_slices()
+
+    def get_fisher_block(self, label_i: str, label_j: str | None = None):
+        F = self.get_fisher_matrix()
+        sl = self.get_bandpower_slices()
+        if F is None or sl is None:
+            return None
+        label_j = label_i if label_j is None else label_j
+        for lab in (label_i, label_j):
+            if lab not in sl:
+                raise KeyError(f"Unknown spectrum label {lab!r}. Legal labels: {list(sl)}")
+        return F[sl[label_i], sl[label_j]]
+
+    def _to_dict(self, flat):
+        sl = self.layout.bandpower_slices()
+        flat = np.asarray(flat)
+        return {k: flat[..., v] for k, v in sl.items()}
+
+
+class Spectra(_Base):
+    """QML power spectra C_hat = (q - b) F^-1 on the GPU (qube/spectra.py)."""
+
+    def __init__(self, params=None, fisher: Fisher | None = None, basis=None, mask=None,
+                 noise_cov1=None, noise_cov2=None, cls_data=None, fiducial_cls=None, beam=None,
+                 maps1=None, maps2=None, *, params_file=None, precision: str | None = None,
+                 device=None, **kwargs):
+        _check_basis(basis)
+        if fisher is not None:
+            self.fisher_instance = fisher
+            params = params if params is not None else vars(fisher.params)
+            mask = fisher._mask if mask is None else mask
+            noise_cov1 = fisher._noise_in if noise_cov1 is None else noise_cov1
+            cls_data = fisher._cls if cls_data is None else cls_data
+            beam = fisher._beam if beam is None else beam
+            precision = precision or fisher.precision
+            device = device if device is not None else fisher.device
+        else:
+            self.fisher_instance = None
+        super().__init__(params, params_file, mask, noise_cov1, noise_cov2, cls_data, fiducial_cls,
+                         beam, precision or "fp64", device, kwargs)
+        if maps1 is None:
+            raise NotImplementedError("inject maps1 (file inputs unsupported)")
+        self._maps_in = maps1
+        self.qml_results = None
+        self.qml_noise_bias = None
+        self.invfisher = None
+        self.inv_fisher_sqrt = None
+
+    def _fisher(self) -> Fisher:
+        f = self.fisher_instance
+        if f is None:
+            f = Fisher(vars(self.params), mask=self._mask, noise_cov1=self._noise_in,
+                       cls_data=self._cls, beam=self._beam, precision=self.precision,
+                       device=self.device)
+            self.fisher_instance = f
+        if f.fisher is None:
+            f.run()
+        return f
+
+    def run(self) -> None:
+        f = self._fisher()
+        self.layout = f.layout
+        L = self.layout
+        E = f.engine
+        self.spectra_list = f.spectra_list
+        self.beam_smoothing = f.beam_smoothing
+        self.bins = f.bins
+        self.n_params = L.n_params
+        maps = self._maps_in
+        if isinstance(maps, torch.Tensor):
+            X = maps.to(self.device, torch.float64)
+        else:
+            X = torch.from_numpy(np.ascontiguousarray(np.asarray(maps, dtype=np.float64)))
+            X = X.to(self.device, non_blocking=True)
+        nsims = self.params.nsims or X.shape[1]
+        if tuple(X.shape) != (L.n, nsims):
+            raise ValueError(f"injected maps have shape {tuple(X.shape)}, expected ({L.n}, {nsims})")
+        _, bias, q = E.fisher_qml(f._dev_Cinv, f._dev_N, X, want_fisher=False)
+        if L.remove_nb:
+            q = q - bias[None, :]
+        self._dev_invF = E.spd_inverse(f._dev_F.clone())
+        self._dev_q = q
+        self._dev_b = bias
+        self._dev_clhat = E.gemm(q, self._dev_invF)
+        self._dev_nb = E.gemm(bias[None, :], self._dev_invF)[0]
+        self.qml_results = q.cpu().numpy()
+        self.qml_noise_bias = bias.cpu().numpy()
+        self.invfisher = self._dev_invF.cpu().numpy()
+        self.fisher_normalized = f.fisher
+
+    # -- outputs (qube/spectra.py:1340-1733) -------------------------------
+    def _inv_sqrt(self):
+        if self.inv_fisher_sqrt is None:
+            Fd = self.fisher_instance._dev_F
+            w, V = torch.linalg.eigh(Fd)
+            thr = w.max() * 1e-12
+            inv = torch.where(w > thr, 1.0 / torch.sqrt(torch.clamp(w, min=1e-300)), torch.zeros_like(w))
+            self.inv_fisher_sqrt = ((V * inv[None, :]) @ V.T).cpu().numpy()
+        return self.inv_fisher_sqrt
+
+    def get_power_spectra(self, mode: str = "deconvolved", *, as_dict: bool = False):
+        valid = ("deconvolved", "decorrelated", "convolved")
+        if mode not in valid:
+            raise ValueError(f"mode must be one of {valid}, got '{mode}'")
+        if self.qml_results is None:
+            return None
+        if mode == "deconvolved":
+            res = self._dev_clhat.cpu().numpy()
+        elif mode == "decorrelated":
+            res = self.qml_results @ self._inv_sqrt()
+        else:
+            W = self.fisher_instance.fisher
+
+            def convolve(theory):
+                if isinstance(theory, dict):
+                    theory = np.concatenate([np.asarray(theory[s]) for s in self.spectra_list])
+                return W @ np.asarray(theory)
+
+            y = self.qml_results
+            if as_dict:
+                return self._to_dict(y), W, convolve
+            return y, W, convolve
+        return self._to_dict(res) if as_dict else res
+
+    def get_noise_bias(self):
+        return None if self.qml_noise_bias is None else self._dev_nb.cpu().numpy()
+
+    def get_covariance(self, mode: str = "deconvolved"):
+        if mode == "deconvolved":
+            return self.invfisher
+        if mode == "decorrelated":
+            return np.eye(self.n_params)
+        if mode == "convolved":
+            return self.fisher_instance.fisher
+        raise ValueError(f"unknown mode {mode!r}")
+
+    def get_error_bars(self, mode: str = "deconvolved", *, as_dict: bool = False):
+        err = np.sqrt(np.diag(self.get_covariance(mode)))
+        return self._to_dict(err) if as_dict else err
+
+    def _to_dict(self, flat):
+        sl = self.layout.bandpower_slices()
+        flat = np.asarray(flat)
+        return {k: flat[..., v] for k, v in sl.items()}
+
+
+def draw_maps(L: lay.Layout, cls: dict, N: torch.Tensor, nsims: int, seed: int = 0,
+              device=None) -> torch.Tensor:
+    """x ~ N(0, S + N) drawn on the device: x = chol(C) z with z from ``seed``."""
+    E = eng.Engine(L, device)
+    C = E.signal(L.smoothed_cl_table(cls)) + N
+    info = E.potrf(C)
+    if int(info.abs().max()) != 0:
+        raise ValueError("covariance is not positive definite")
+    g = torch.Generator(device=C.device).manual_seed(int(seed))
+    z = torch.randn((L.n, nsims), dtype=torch.float64, device=C.device, generator=g)
+    return E.gemm(torch.tril(C), z)

@@ -176,9 +176,11 @@ def logdet_chol(C: np.ndarray) -> float:
     return 2.0 * float(np.sum(np.log(np.diag(Lc))))
 
 
-def trace_product(A: np.ndarray, B: np.ndarray) -> float:
-    """Tr(A B) = sum_ij A_ij B_ji (linalg.py:66-98)."""
-    return float(np.einsum("ij,ji->", A, B))
+def trace_product(A: np.ndarray, B: np.ndarray, BT: np.ndarray | None = None) -> float:
+    """Tr(A B) = sum_ij A_ij B_ji (linalg.py:66-98); pass BT = B^T if already formed."""
+    if BT is None:
+        BT = np.ascontiguousarray(B.T)
+    return float(np.vdot(A.ravel(), BT.ravel()))
 
 
 def fisher(L: lay.Layout, Cinv: np.ndarray, params=None) -> np.ndarray:
@@ -187,10 +189,11 @@ def fisher(L: lay.Layout, Cinv: np.ndarray, params=None) -> np.ndarray:
     idx = list(range(L.n_params)) if params is None else list(params)
     W = L.param_weights()
     A = [Cinv @ binned_derivative(L, p, W) for p in idx]
+    AT = [np.ascontiguousarray(a.T) for a in A]
     F = np.zeros((P, P))
     for a in range(P):
         for b in range(a, P):
-            F[a, b] = F[b, a] = 0.5 * trace_product(A[a], A[b])
+            F[a, b] = F[b, a] = 0.5 * trace_product(A[a], A[b], AT[b])
     return F
 
 
