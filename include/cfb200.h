@@ -1,0 +1,165 @@
+/*
+ * cfb200.h - C ABI of libcfb200.so, the B200 (sm_100a) device library for
+ * CosmoForge's pixel-space QML / Fisher / pixel-likelihood path.
+ *
+ * Conventions
+ *   - Every pointer argument named as a matrix / vector / table is a DEVICE
+ *     pointer (allocated by the caller, e.g. with PyTorch or cudaMalloc).
+ *   - Matrices are row-major FP64 with an explicit leading dimension (ld,
+ *     in elements); batched calls take element strides between problems.
+ *   - `stream` is a cudaStream_t passed as void*; calls are asynchronous on
+ *     it unless stated.
+ *   - Return value: CF_OK (0) or a negative CF_ERR_* code.  Per-problem
+ *     numerical status (non positive-definite pivots) is written to a
+ *     device `info` array, LAPACK style: 0 ok, k > 0 the leading minor of
+ *     order k is not positive.
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   cosmocore/signal_kernels.py      signal_matrix, compute_signal_matrix,
+ *                                    compute_00/22/02_contribution, do_derivative_step
+ *   cosmocore/basis/pixel.py         PixelBasis.get_binned_derivative_direct
+ *   cosmocore/basics/linalg.py       matrix_inverse_symm, cholesky_factor,
+ *                                    matrix_slogdet_symm, matrix_trace, matrix_mult
+ *   qube/fisher.py                   Fisher.compute (A_b and trace loops)
+ *   qube/spectra.py                  Spectra._compute_qml_spectra_traditional
+ *   picslike/picslike.py             PICSLike._compute_likelihood_point
+ */
+#ifndef CFB200_H
+#define CFB200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CF_OK 0
+#define CF_ERR_ARG -1         /* invalid argument */
+#define CF_ERR_CUDA -2        /* a kernel launch or CUDA runtime call failed */
+#define CF_ERR_TIMEOUT -3     /* a bounded device wait ran out */
+#define CF_ERR_UNSUPPORTED -4 /* valid but not implemented combination */
+
+/* Block kinds of cf_build_block (which field pair a block of S couples). */
+#define CF_KIND_00_AUTO 0  /* spin-0 field with itself */
+#define CF_KIND_00_CROSS 1 /* two different spin-0 fields */
+#define CF_KIND_22_AUTO 2  /* spin-2 field with itself: rows/cols [Q | U] */
+#define CF_KIND_02 3       /* rows: spin-2 field [Q | U], cols: spin-0 field */
+
+/* Library version (>= 1). */
+int cf_version(void);
+
+/* Number of kernels the library has launched so far in this process. */
+unsigned long long cf_launch_count(void);
+
+/*
+ * Fused pixel-pair builder: one block of the signal matrix S, or the binned
+ * derivatives dC_b of every bin of one spectrum, from one pass of the
+ * Legendre / spin-2 recurrences per pixel pair.
+ * Replaces: cosmocore/signal_kernels.py:164-387 (compute_00/22/02_contribution,
+ * the per-pair loops), :390-537 (compute_signal_matrix / signal_matrix),
+ * :715-829 (do_derivative_step), cosmocore/basis/pixel.py:802-950
+ * (get_binned_derivative_direct).
+ *   kind, mode   CF_KIND_*; mode < 0 builds the signal (t0..t2 are the
+ *                block's beam-smoothed C_l: 00 -> t0 = C_l; 22 -> EE, BB, EB;
+ *                02 -> TE, TB); mode >= 0 builds derivatives of one spectrum
+ *                (22: 0 EE, 1 BB, 2 EB; 02: 0 TE, 1 TB) with t0 = w_l b_l^2.
+ *   na, va       column field: pixel count and pointings, SoA x[na] y[na] z[na]
+ *   nb, vb       row field (== column field for *_AUTO kinds)
+ *   lmax         last multipole of the recurrence (<= 512)
+ *   bin_of       int[lmax+1]: output bin of each l, -1 = none; NULL = one bin
+ *   out, ld, row_off, col_off, bin_stride
+ *                entry (r, c) of bin b goes to
+ *                out[(row_off + r) * ld + col_off + b * bin_stride + c]
+ *   outT, ...    its mirror (c, r) goes to
+ *                outT[(rowT_off + c) * ldT + colT_off + b * binT_stride + r]
+ *   batch, tstride, ostride
+ *                batch of problems: tables advance by tstride, out/outT by ostride
+ */
+int cf_build_block(int kind, int mode, int na, const double* va, int nb, const double* vb, int lmax,
+                   const double* t0, const double* t1, const double* t2, const int* bin_of,
+                   double* out, long ld, long row_off, long col_off, long bin_stride, double* outT,
+                   long ldT, long rowT_off, long colT_off, long binT_stride, int batch, long tstride,
+                   long ostride, void* stream);
+
+/*
+ * FP64 GEMM on the DMMA tensor pipe: C = alpha op(A) op(B) + beta C, with an
+ * optional transposed copy CT = C^T (NULL to skip) and a batch dimension.
+ * transa / transb: 0 = A is M x K / B is K x N; 1 = A given as K x M / B as N x K.
+ * lower_only: skip output tiles strictly above the diagonal.
+ * Replaces: cosmocore/basics/linalg.py:18-32 (matrix_mult, np.matmul).
+ */
+int cf_dgemm(int transa, int transb, int M, int N, int K, double alpha, const double* A, long lda,
+             long strideA, const double* B, long ldb, long strideB, double beta, double* C, long ldc,
+             long strideC, double* CT, long ldct, long strideCT, int batch, int lower_only,
+             void* stream);
+
+/*
+ * Blocked lower Cholesky factorisation in place (batch of n x n matrices).
+ * info: int[batch], zeroed by the caller.
+ * Replaces: cosmocore/basics/linalg.py:362-406 (cholesky_factor, LAPACK dpotrf).
+ */
+int cf_potrf(int n, double* A, long lda, long strideA, int batch, int* info, void* stream);
+
+/* Y = L^-1 for lower-triangular L (batch).  Replaces the dpotri half of
+ * cosmocore/basics/linalg.py:152-219. */
+int cf_trtri_lower(int n, const double* L, long lda, long strideL, double* Y, long ldy, long strideY,
+                   int batch, void* stream);
+
+/* Bytes of workspace cf_spd_inverse needs for `batch` problems of order n. */
+size_t cf_spd_inverse_workspace(int n, int batch);
+
+/*
+ * In place inverse of SPD matrices with the reference's Jacobi scaling:
+ * D = diag(|A_ii|^-1/2), L L^T = D A D, A^-1 = D (L L^T)^-1 D.
+ * work: cf_spd_inverse_workspace(n, batch) bytes of device memory.
+ * Replaces: cosmocore/basics/linalg.py:152-219 (matrix_inverse_symm).
+ */
+int cf_spd_inverse(int n, double* A, long lda, long strideA, int batch, void* work, int* info,
+                   void* stream);
+
+/*
+ * Fisher trace contraction, split-K on the DMMA pipe:
+ *   F[(p_off+p) ldF + q_off+q] += scale sum_{k<K1, l<K2} X[p sXp + k ldX + l] Y[q sYq + k ldY + l]
+ * (and the mirror entry when sym != 0), p < P1, q < P2.  F must be zeroed
+ * first; splits <= 0 picks 4 CTAs per SM.
+ * Replaces: qube/fisher.py:557-607 (trace loop), cosmocore/basics/linalg.py:66-98
+ * (matrix_trace).
+ */
+int cf_trace_contract_f64(int P1, int P2, int K1, int K2, const double* X, long sXp, long ldX,
+                          const double* Y, long sYq, long ldY, double scale, double* F, long ldF,
+                          long p_off, long q_off, int sym, int splits, void* stream);
+
+/*
+ * QML reductions over the derivative blocks D_p (R x Ccols, p-th block at
+ * D + p sDp, row stride ldD) of one spectrum:
+ *   bias[p] += scale sum_{r,c} M[(mro+r) ldM + mco+c] D_p[r, c]            (M may be NULL)
+ *   q[m ldq + p] += scale sum_{r,c} Y[(yro+r) ldY + m] D_p[r, c] Y[(yco+c) ldY + m],  m < nsims <= 4
+ * Replaces: qube/spectra.py:1124-1186 (q_b = y^T dC_b y / 2, bias_b = Tr(C^-1 N C^-1 dC_b) / 2).
+ */
+int cf_qml_reduce_f64(int P, int R, int Ccols, const double* D, long ldD, long sDp, const double* M,
+                      long ldM, long mro, long mco, const double* Y, long ldY, int nsims, long yro,
+                      long yco, double scale, double* bias, double* q, long ldq, void* stream);
+
+/*
+ * chi2[b nrhs + m] = |L_b^-1 x_{b,m}|^2 and logdet[b] = 2 sum ln (L_b)_ii
+ * from lower Cholesky factors (batch).  X: n x nrhs (ldx), strideX = 0 shares
+ * it across the batch; z_work: batch * nrhs * n doubles.
+ * Replaces: picslike/picslike.py:643-664 (chi2 einsum with C^-1) and
+ * cosmocore/basics/linalg.py:430-474 (matrix_slogdet_symm).
+ */
+int cf_chi2_logdet(int n, const double* L, long lda, long strideL, int batch, const double* X, long ldx,
+                   long strideX, int nrhs, double* z_work, double* chi2, double* logdet, void* stream);
+
+/* Z_b = a X_b + c_b W_b (c_b = cvec[b] if cvec else c; strideW = 0 shares W).
+ * Used for C = S + s N (picslike/picslike.py:301-319, qube/fisher.py:311-344). */
+int cf_axpby(long count, double a, const double* X, long strideX, double c, const double* cvec,
+             const double* W, long strideW, double* Z, long strideZ, int batch, void* stream);
+
+/* B = A^T for an R x C row-major A. */
+int cf_transpose(int R, int C, const double* A, long lda, double* B, long ldb, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CFB200_H */
