@@ -18,6 +18,7 @@ CF_ERR_ARG = -1
 CF_ERR_CUDA = -2
 CF_ERR_TIMEOUT = -3
 CF_ERR_UNSUPPORTED = -4
+CF_ERR_TOO_LARGE = -5
 
 _i, _l, _d, _p, _sz = C.c_int, C.c_long, C.c_double, C.c_void_p, C.c_size_t
 
@@ -32,6 +33,8 @@ SIGNATURES = {
     "cf_trtri_lower": (_i, [_i, _p, _l, _l, _p, _l, _l, _i, _p]),
     "cf_spd_inverse_workspace": (_sz, [_i, _i]),
     "cf_spd_inverse": (_i, [_i, _p, _l, _l, _i, _p, _p, _p]),
+    "cf_spd_inverse_static_max_n": (_i, []),
+    "cf_spd_inverse_static": (_i, [_i, _p, _l, _p, _p]),
     "cf_trace_contract_f64": (_i, [_i, _i, _i, _i, _p, _l, _l, _p, _l, _l, _d, _p, _l, _l, _l, _i, _i,
                                    _p]),
     "cf_qml_reduce_f64": (_i, [_i, _i, _i, _p, _l, _l, _p, _l, _l, _l, _p, _l, _i, _l, _l, _d, _p,
@@ -76,7 +79,8 @@ def check(rc: int, what: str = "") -> None:
     if rc == CF_OK:
         return
     names = {CF_ERR_ARG: "invalid argument", CF_ERR_CUDA: "CUDA launch error",
-             CF_ERR_TIMEOUT: "timeout", CF_ERR_UNSUPPORTED: "unsupported"}
+             CF_ERR_TIMEOUT: "timeout", CF_ERR_UNSUPPORTED: "unsupported",
+             CF_ERR_TOO_LARGE: "size exceeds the static scratch capacity"}
     raise DeviceError(f"{what}: {names.get(rc, rc)}")
 
 

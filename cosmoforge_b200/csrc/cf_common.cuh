@@ -8,6 +8,7 @@
 #define CF_ERR_CUDA -2
 #define CF_ERR_TIMEOUT -3
 #define CF_ERR_UNSUPPORTED -4
+#define CF_ERR_TOO_LARGE -5
 
 #define CF_PI 3.14159265358979323846
 

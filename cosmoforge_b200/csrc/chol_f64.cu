@@ -11,6 +11,8 @@
 // LAPACK: 0 = success, k > 0 = the leading minor of order k is not positive.
 #include "cf_common.cuh"
 
+#include <mutex>
+
 extern "C" int cf_dgemm(int transa, int transb, int M, int N, int K, double alpha, const double* A,
                         long lda, long strideA, const double* B, long ldb, long strideB, double beta,
                         double* C, long ldc, long strideC, double* CT, long ldct, long strideCT,
@@ -269,4 +271,61 @@ extern "C" int cf_spd_inverse(int n, double* A, long lda, long strideA, int batc
     k_unscale_mirror<<<g2, b2, 0, st>>>(A, lda, strideA, n, d, n);
     CF_CHECK_LAUNCH();
     return CF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of cf_spd_inverse for callers that cannot allocate
+// device memory: code running inside a host callback or a custom allocator's
+// own hooks, plugins whose host forbids cudaMalloc after start-up, or
+// integrations that must not fragment a pool they do not own.  Its workspace
+// (L^-1 and the Jacobi scale factors) lives in this file-scope array, which
+// every GPU that loads the library holds until the process exits:
+// (1024^2 + 1024) doubles = 8.4 MB per device.
+#define CF_SPD_STATIC_MAX_N 1024
+static __device__ __align__(256) double g_spd_static_scratch[(size_t)CF_SPD_STATIC_MAX_N * CF_SPD_STATIC_MAX_N +
+                                                             CF_SPD_STATIC_MAX_N];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mu;
+double* g_static_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array for the current device.  In host code
+// the array's name is only a host-side stand-in, so the address is looked up
+// once per device with that device current and cached.
+int static_scratch(double** out)
+{
+    int dev = -1;
+    CF_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return CF_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (g_static_ptr[dev] == nullptr) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_spd_static_scratch);
+        if (e != cudaSuccess || p == nullptr) return CF_ERR_CUDA;
+        g_static_ptr[dev] = static_cast<double*>(p);
+    }
+    *out = g_static_ptr[dev];
+    return CF_OK;
+}
+}  // namespace
+
+extern "C" int cf_spd_inverse_static_max_n(void) { return CF_SPD_STATIC_MAX_N; }
+
+// Same result as cf_spd_inverse(n, A, lda, n*n, 1, work, info, stream) with no
+// caller workspace and no allocation.  The first call on a device looks up the
+// scratch address (make it before any stream capture).  All calls share one
+// scratch array: calls whose work overlaps on the GPU (different streams or
+// host threads on the same device) race.  Every scratch element the routine
+// reads is written by it first, so stale contents from a previous call do not
+// matter; *info is set to 0 on the stream before the factorisation.
+extern "C" int cf_spd_inverse_static(int n, double* A, long lda, int* info, void* stream)
+{
+    if (n <= 0 || !A || !info || lda < n) return CF_ERR_ARG;
+    if (n > CF_SPD_STATIC_MAX_N) return CF_ERR_TOO_LARGE;
+    double* work = nullptr;
+    int rc = static_scratch(&work);
+    if (rc) return rc;
+    CF_CHECK(cudaMemsetAsync(info, 0, sizeof(int), (cudaStream_t)stream));
+    return cf_spd_inverse(n, A, lda, (long)n * n, 1, work, info, stream);
 }

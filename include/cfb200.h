@@ -38,6 +38,7 @@ extern "C" {
 #define CF_ERR_CUDA -2        /* a kernel launch or CUDA runtime call failed */
 #define CF_ERR_TIMEOUT -3     /* a bounded device wait ran out */
 #define CF_ERR_UNSUPPORTED -4 /* valid but not implemented combination */
+#define CF_ERR_TOO_LARGE -5   /* size exceeds a static capacity of the library */
 
 /* Block kinds of cf_build_block (which field pair a block of S couples). */
 #define CF_KIND_00_AUTO 0  /* spin-0 field with itself */
@@ -116,6 +117,24 @@ size_t cf_spd_inverse_workspace(int n, int batch);
  */
 int cf_spd_inverse(int n, double* A, long lda, long strideA, int batch, void* work, int* info,
                    void* stream);
+
+/*
+ * Allocation-free SPD inverse: cf_spd_inverse for one n x n matrix with its
+ * workspace taken from a scratch array compiled into the library (a
+ * file-scope __device__ array of (1024^2 + 1024) doubles, 8.4 MB held by every
+ * GPU that loads the library until exit), for callers that cannot call
+ * cudaMalloc (host callbacks, allocator hooks, plugins whose host owns the
+ * memory pool).  Allocates nothing.  n > cf_spd_inverse_static_max_n()
+ * returns CF_ERR_TOO_LARGE.  The first call on a device looks up the
+ * scratch address (cudaGetSymbolAddress), so make it before any stream
+ * capture.  All calls share the one array: calls that overlap on the GPU
+ * race.  *info is zeroed on `stream` by the call.
+ * No counterpart in the reference (an addition of this library).
+ */
+int cf_spd_inverse_static(int n, double* A, long lda, int* info, void* stream);
+
+/* Largest n accepted by cf_spd_inverse_static. */
+int cf_spd_inverse_static_max_n(void);
 
 /*
  * Fisher trace contraction, split-K on the DMMA pipe:
