@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--scheme", choices=["bf16x3", "bf16x6"], default="bf16x6",
+                    help="split-product scheme of the mixed path")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--lmax", type=int, default=None,
@@ -238,7 +240,7 @@ def main():
         if args.precision == "mixed":
             from cosmoforge_b200 import engine_mixed
 
-            F, bias, q = engine_mixed.fisher_qml(E, C, N, X)
+            F, bias, q = engine_mixed.fisher_qml(E, C, N, X, scheme=args.scheme)
         else:
             F, bias, q = E.fisher_qml(C, N, X)
         Finv = E.spd_inverse(F.clone())
@@ -272,8 +274,10 @@ def main():
     clocks = clk.summary()
     tags = E.probe
     E.probe = None
-    dom = "a_gemm"
+    dom = "a_gemm" if args.precision == "fp64" else "a_gemm_mixed"
     recs = tags.get(dom, [])
+    stage_ms = {k: round(sum(a.elapsed_time(b) for a, b, _ in v) / max(args.steps, 1), 2)
+                for k, v in tags.items()}
     k_time = sum(a.elapsed_time(b) for a, b, _ in recs) / 1e3
     k_work = sum(w for _, _, w in recs)
     n_launch = max(len(recs), 1)
@@ -336,7 +340,7 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else "bf16x3/f32+f64",
+            "dtype": "f64" if args.precision == "fp64" else f"{args.scheme} split products, f32 tensor accumulation, f64 promotion/reductions",
             "data": "synthetic (seeded): config-1 TQU problem, x ~ N(0, C) drawn on device",
             "config": {"workload": WORKLOAD, "n_pixels": L.n, "n_params": L.n_params, "nsims": 1,
                        "lmax_signal": L.lmax_signal, "precision": args.precision,
@@ -344,6 +348,7 @@ def main():
                        "A_b slabs 56 GB)"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
+            "stage_ms_per_step": stage_ms,
             "roofline": {"bound": "tensor", "kernel": dom, "achieved": achieved, "peak": peak,
                          "peak_source": peak_src, "unit": "TFLOP/s", "frac": achieved / peak,
                          "traffic": traffic, "launches_timed": n_launch,

@@ -18,6 +18,8 @@
 // multiply-add), because the angle of nearly collinear pairs is an ill-
 // conditioned function of these products; the recurrences themselves are
 // well conditioned and use FMA.
+#include <cuda_bf16.h>
+
 #include "cf_common.cuh"
 
 namespace {
@@ -42,6 +44,8 @@ struct BuildArgs {
     long ldT, rowT_off, colT_off, binT_stride;
     long tstride;   // batch stride of the l tables
     long ostride;   // batch stride of out and outT
+    int planes;     // 0: FP64 output; 1..3: BF16 split planes of the FP64 value
+    long plane_stride, planeT_stride;
 };
 
 __device__ __forceinline__ void rotation_angle(double r1x, double r1y, double r1z, double r2x,
@@ -92,8 +96,22 @@ struct Emitter {
     __device__ Emitter(const BuildArgs& args, long b) : a(args), base(b) {}
     __device__ __forceinline__ void put(long r, long c, int bin, double v, bool mirror) const
     {
-        a.out[base + (a.row_off + r) * a.ld + a.col_off + bin * a.bin_stride + c] = v;
-        if (mirror) a.outT[base + (a.rowT_off + c) * a.ldT + a.colT_off + bin * a.binT_stride + r] = v;
+        const long i = base + (a.row_off + r) * a.ld + a.col_off + bin * a.bin_stride + c;
+        const long iT = base + (a.rowT_off + c) * a.ldT + a.colT_off + bin * a.binT_stride + r;
+        if (a.planes == 0) {
+            a.out[i] = v;
+            if (mirror) a.outT[iT] = v;
+            return;
+        }
+        __nv_bfloat16* o = reinterpret_cast<__nv_bfloat16*>(a.out);
+        __nv_bfloat16* oT = reinterpret_cast<__nv_bfloat16*>(a.outT);
+        double x = v;
+        for (int p = 0; p < a.planes; ++p) {
+            const __nv_bfloat16 h = __double2bfloat16(x);
+            o[p * a.plane_stride + i] = h;
+            if (mirror) oT[p * a.planeT_stride + iT] = h;
+            x -= (double)__bfloat162float(h);
+        }
     }
 };
 
@@ -289,19 +307,43 @@ __global__ void __launch_bounds__(BX* BY) k_build(BuildArgs a)
 
 }  // namespace
 
+extern "C" int cf_build_block_planes(int kind, int mode, int na, const double* va, int nb, const double* vb,
+                                     int lmax, const double* t0, const double* t1, const double* t2,
+                                     const int* bin_of, void* out, long ld, long row_off, long col_off,
+                                     long bin_stride, void* outT, long ldT, long rowT_off, long colT_off,
+                                     long binT_stride, int batch, long tstride, long ostride, int planes,
+                                     long plane_stride, long planeT_stride, void* stream);
+
 extern "C" int cf_build_block(int kind, int mode, int na, const double* va, int nb, const double* vb,
                               int lmax, const double* t0, const double* t1, const double* t2,
                               const int* bin_of, double* out, long ld, long row_off, long col_off,
                               long bin_stride, double* outT, long ldT, long rowT_off, long colT_off,
                               long binT_stride, int batch, long tstride, long ostride, void* stream)
 {
+    return cf_build_block_planes(kind, mode, na, va, nb, vb, lmax, t0, t1, t2, bin_of, out, ld, row_off, col_off,
+                                 bin_stride, outT, ldT, rowT_off, colT_off, binT_stride, batch, tstride, ostride,
+                                 0, 0, 0, stream);
+}
+
+// As cf_build_block, with `planes` >= 1 writing BF16 split planes (out/outT
+// are then __nv_bfloat16 arrays, planes `plane_stride` / `planeT_stride`
+// elements apart) instead of FP64.
+extern "C" int cf_build_block_planes(int kind, int mode, int na, const double* va, int nb, const double* vb,
+                                     int lmax, const double* t0, const double* t1, const double* t2,
+                                     const int* bin_of, void* out, long ld, long row_off, long col_off,
+                                     long bin_stride, void* outT, long ldT, long rowT_off, long colT_off,
+                                     long binT_stride, int batch, long tstride, long ostride, int planes,
+                                     long plane_stride, long planeT_stride, void* stream)
+{
     if (kind < K00A || kind > K02 || na <= 0 || nb <= 0 || lmax < 0 || lmax > MAXL || !va || !vb ||
         !out || !outT || !t0)
         return CF_ERR_ARG;
     if ((kind == K00A || kind == K22A) && (na != nb || va != vb)) return CF_ERR_ARG;
     if (batch < 1) return CF_ERR_ARG;
-    BuildArgs a{kind, mode, na, nb, va, vb, lmax, t0, t1, t2, bin_of, out, ld, row_off, col_off,
-                bin_stride, outT, ldT, rowT_off, colT_off, binT_stride, tstride, ostride};
+    if (planes < 0 || planes > 3) return CF_ERR_ARG;
+    BuildArgs a{kind, mode, na, nb, va, vb, lmax, t0, t1, t2, bin_of, (double*)out, ld, row_off, col_off,
+                bin_stride, (double*)outT, ldT, rowT_off, colT_off, binT_stride, tstride, ostride, planes,
+                plane_stride, planeT_stride};
     dim3 block(BX, BY);
     dim3 grid(cf_cdiv(na, BX), cf_cdiv(nb, BY), batch);
     k_build<<<grid, block, 0, (cudaStream_t)stream>>>(a);

@@ -1,0 +1,636 @@
+// Split-precision GEMM on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+//   C[M, N] = sum_t A_{a(t)}[M, K] . B_{b(t)}[N, K]^T        (FP32 accumulation in TMEM)
+//
+// A_s / B_s are BF16 "split planes" of FP64 operands: x = x_0 + x_1 (+ x_2)
+// with x_0 = bf16(x), x_1 = bf16(x - x_0), ...  The product list selects
+// which plane pairs are multiplied: BF16x3 = {(0,0), (0,1), (1,0)} keeps ~16
+// significant bits, BF16x6 adds {(0,2), (1,1), (2,0)} for ~24.  Both operands
+// are K-major (row-major with K contiguous).
+//
+// Structure (one 128 x BN output tile per CTA, 6 warps):
+//   warp 0   TMA producer: 128B-swizzled boxes of A and B into a STAGES-deep
+//            shared-memory ring, completion counted on per-stage mbarriers;
+//   warp 1   allocates the TMEM accumulator and issues tcgen05.mma from one
+//            thread; tcgen05.commit releases each stage and finally signals
+//            the epilogue;
+//   warps 2-5  epilogue: tcgen05.ld of the accumulator (one TMEM lane per
+//            output row), then either BF16 split planes of the result (row-
+//            major and/or transposed) or FP32.
+// Every wait on an mbarrier is bounded; on timeout the CTA records an error,
+// drains, frees its TMEM and returns.
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include <type_traits>
+
+#include "cf_common.cuh"
+
+namespace {
+
+constexpr int BM = 128, BK = 64, NTHREADS = 320;  // producer, MMA, 8 epilogue warps
+constexpr int EPI_WARPS = 8;
+constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s bound on any single wait
+constexpr int MAX_TERMS = 6;
+
+struct Terms {
+    int n;
+    int a[MAX_TERMS];
+    int b[MAX_TERMS];
+};
+
+// Trace mode: the K index runs over the (k, l) plane, k < K1, l < K2, and
+// the CTA's share of it is blockIdx.z of gridDim.z; the result is scaled and
+// added into an FP64 matrix F at (p_off + row, q_off + col) (and its mirror).
+struct TraceArgs {
+    int K1, K2;
+    double* F;
+    long ldF, p_off, q_off;
+    int sym;
+    double scale;
+    const int* row_map;  // optional: F row of output row p (instead of p_off + p)
+    const int* col_map;  // optional: F column of output column q
+};
+
+struct EpiArgs {
+    __nv_bfloat16* X;   // [planes][M][ldx]
+    long ldx, x_plane;
+    int x_planes;
+    __nv_bfloat16* XT;  // [planes][N][ldxt]
+    long ldxt, xt_plane;
+    float* Cf;          // [M][ldc] fp32
+    long ldc;
+    int M, N;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(200000u)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ unsigned long long now_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Wait bounded in time; false (and the abort flag raised) when it runs out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag)
+{
+    const unsigned long long t0 = now_ns();
+    for (unsigned i = 0;; ++i) {
+        if (mbar_try(bar, parity)) return true;
+        if (*abort_flag) return false;
+        if ((i & 255) == 255 && now_ns() - t0 > WAIT_NS) break;
+    }
+    *abort_flag = 1;
+    return false;
+}
+
+// Wait bounded in time that ignores the abort flag: drains work already issued.
+__device__ __forceinline__ void mbar_drain(uint64_t* bar, uint32_t parity)
+{
+    const unsigned long long t0 = now_ns();
+    for (unsigned i = 0;; ++i) {
+        if (mbar_try(bar, parity)) return;
+        if ((i & 255) == 255 && now_ns() - t0 > WAIT_NS) return;
+    }
+}
+
+__device__ __forceinline__ void tma_load_3d(const CUtensorMap* map, uint64_t* bar, void* dst, int c0, int c1, int c2)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];\n"
+        ::"r"(smem_u32(dst)), "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_4d(const CUtensorMap* map, uint64_t* bar, void* dst, int c0, int c1, int c2,
+                                            int c3)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], [%2];\n"
+        ::"r"(smem_u32(dst)), "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+        : "memory");
+}
+
+// Shared-memory matrix descriptor: K-major, 128B swizzle, 8-row atoms 1024 B apart.
+__device__ __forceinline__ uint64_t smem_desc(const void* tile)
+{
+    const uint64_t addr = smem_u32(tile);
+    uint64_t d = 0;
+    d |= (addr >> 4) & 0x3FFFull;          // start address
+    d |= (uint64_t)(16 >> 4) << 16;        // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;      // stride byte offset: 8 rows x 128 B
+    d |= (uint64_t)1 << 46;                // descriptor version (sm100)
+    d |= (uint64_t)2 << 61;                // SWIZZLE_128B
+    return d;
+}
+
+template <int BN>
+__device__ __forceinline__ uint32_t instr_desc()
+{
+    // D = F32, A = B = BF16, both K-major, M = 128, N = BN.
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate)
+{
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+        ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+          "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+          "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+          "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+template <int BN, int STAGES, bool TRACE, int KC>
+__global__ void __launch_bounds__(NTHREADS, 1)
+    k_umma_gemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int K,
+                int n_split, Terms terms, EpiArgs epi, TraceArgs tr, int* err)
+{
+    // Persistent: each CTA walks output tiles blockIdx.x, +gridDim.x, ...; the
+    // shared-memory ring, TMEM and all mbarrier phases carry over between
+    // tiles, so the epilogue of one tile overlaps the MMAs of the next.
+    // Partial sums are promoted out of TMEM every KC k-tiles: the MMA thread
+    // alternates between two TMEM accumulators while the epilogue warps add the
+    // finished one into registers (FP32 for GEMM outputs, FP64 for the Fisher
+    // traces), so no FP32 tensor-core accumulator sees more than 4 KC steps.
+    // Two epilogue warps share each TMEM lane quadrant, each owning half of the
+    // BN columns.
+    using AccT = typename std::conditional<TRACE, double, float>::type;
+    constexpr int HALF = BN / 2;
+    constexpr uint32_t A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2;
+    constexpr uint32_t TMEM_COLS = 2 * BN <= 64 ? 64 : (2 * BN <= 128 ? 128 : (2 * BN <= 256 ? 256 : 512));
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* sA = smem;
+    uint8_t* sB = smem + STAGES * A_BYTES;
+    uint64_t* full = (uint64_t*)(sB + STAGES * B_BYTES);
+    uint64_t* empty = full + STAGES;
+    uint64_t* accf = empty + STAGES;  // [2] accumulator ready
+    uint64_t* acce = accf + 2;        // [2] accumulator drained
+    uint64_t* dbar = acce + 2;        // MMA drain on abort
+    uint32_t* tmem_slot = (uint32_t*)(dbar + 1);
+    volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int n_mt = (epi.M + BM - 1) / BM, n_nt = (epi.N + BN - 1) / BN;
+    const long n_tiles = (long)n_mt * n_nt * n_split;
+    const int nl = TRACE ? (tr.K2 + BK - 1) / BK : 1;
+    const long kt_total = TRACE ? (long)tr.K1 * nl : (long)((K + BK - 1) / BK);
+    auto coords = [&](long tile, int& m0, int& n0, long& t_lo, int& kt) {
+        const int mt = (int)(tile % n_mt);
+        const long rest = tile / n_mt;
+        const int nt = (int)(rest % n_nt), z = (int)(rest / n_nt);
+        m0 = mt * BM;
+        n0 = nt * BN;
+        t_lo = kt_total * z / n_split;
+        kt = (int)(kt_total * (z + 1) / n_split - t_lo);
+    };
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&accf[0], 1);
+        mbar_init(&accf[1], 1);
+        mbar_init(&acce[0], EPI_WARPS);
+        mbar_init(&acce[1], EPI_WARPS);
+        mbar_init(dbar, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            long g = 0;
+            bool stop = false;
+            for (long tile = blockIdx.x; tile < n_tiles && !stop; tile += gridDim.x) {
+                int m0, n0, kt;
+                long t_lo;
+                coords(tile, m0, n0, t_lo, kt);
+                const int iters = terms.n * kt;
+                for (int it = 0; it < iters; ++it, ++g) {
+                    const int s = (int)(g % STAGES);
+                    const long r = g / STAGES;
+                    if (r > 0 && !mbar_wait(&empty[s], (uint32_t)((r - 1) & 1), abort_flag)) {
+                        stop = true;
+                        break;
+                    }
+                    const int t = it / kt;
+                    const long ktile = t_lo + it % kt;
+                    mbar_expect_tx(&full[s], A_BYTES + B_BYTES);
+                    if (TRACE) {
+                        const int k = (int)(ktile / nl), l0 = (int)(ktile % nl) * BK;
+                        tma_load_4d(&mapA, &full[s], sA + s * A_BYTES, l0, k, m0, terms.a[t]);
+                        tma_load_4d(&mapB, &full[s], sB + s * B_BYTES, l0, k, n0, terms.b[t]);
+                    } else {
+                        const int kk = (int)ktile * BK;
+                        tma_load_3d(&mapA, &full[s], sA + s * A_BYTES, kk, m0, terms.a[t]);
+                        tma_load_3d(&mapB, &full[s], sB + s * B_BYTES, kk, n0, terms.b[t]);
+                    }
+                }
+            }
+            // drain: every issued copy lands before the CTA may exit
+            for (long q = (g > STAGES ? g - STAGES : 0); q < g; ++q)
+                mbar_drain(&full[q % STAGES], (uint32_t)((q / STAGES) & 1));
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = instr_desc<BN>();
+            bool aborted = false;
+            long g = 0, gc = 0;
+            for (long tile = blockIdx.x; tile < n_tiles && !aborted; tile += gridDim.x) {
+                int m0, n0, kt;
+                long t_lo;
+                coords(tile, m0, n0, t_lo, kt);
+                const int iters = terms.n * kt;
+                int buf = 0;
+                for (int it = 0; it < iters; ++it, ++g) {
+                    const bool first = (it % KC) == 0;
+                    if (first) {
+                        buf = (int)(gc & 1);
+                        const long u = gc >> 1;
+                        if (u >= 1 && !mbar_wait(&acce[buf], (uint32_t)((u - 1) & 1), abort_flag)) {
+                            aborted = true;
+                            break;
+                        }
+                    }
+                    const int s = (int)(g % STAGES);
+                    if (!mbar_wait(&full[s], (uint32_t)((g / STAGES) & 1), abort_flag)) {
+                        aborted = true;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                    const uint64_t ad = smem_desc(sA + s * A_BYTES), bd = smem_desc(sB + s * B_BYTES);
+                    const uint32_t dst = tmem + (uint32_t)(buf * BN);
+#pragma unroll
+                    for (int k = 0; k < BK / 16; ++k)  // 16 BF16 = 32 B per MMA; advance the start address
+                        umma_bf16(dst, ad + (uint64_t)((k * 32) >> 4), bd + (uint64_t)((k * 32) >> 4), idesc,
+                                  (first && k == 0) ? 0u : 1u);
+                    umma_commit(&empty[s]);
+                    if ((it % KC) == KC - 1 || it == iters - 1) {
+                        umma_commit(&accf[buf]);
+                        ++gc;
+                    }
+                }
+            }
+            if (aborted) {  // MMAs already issued finish before TMEM is freed
+                umma_commit(dbar);
+                mbar_drain(dbar, 0);
+            }
+        }
+    } else {
+        // epilogue warps 2..9: TMEM lanes 32 * (warp % 4) .. + 31 (one output row
+        // per thread), columns [half * BN/2, half * BN/2 + BN/2)
+        const int quad = warp & 3, half = (warp - 2) >> 2;
+        const uint32_t lane_addr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(half * HALF);
+        long gc = 0;
+        bool ok = true;
+        for (long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
+            int m0, n0, kt;
+            long t_lo;
+            coords(tile, m0, n0, t_lo, kt);
+            const int iters = terms.n * kt;
+            const int nchunks = (iters + KC - 1) / KC;
+            AccT acc[HALF];
+#pragma unroll
+            for (int j = 0; j < HALF; ++j) acc[j] = AccT(0);
+            for (int c = 0; c < nchunks; ++c, ++gc) {
+                const int buf = (int)(gc & 1);
+                if (!mbar_wait(&accf[buf], (uint32_t)((gc >> 1) & 1), abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+#pragma unroll
+                for (int gi = 0; gi < HALF / 32; ++gi) {
+                    uint32_t v[32];
+                    tmem_ld32(lane_addr + (uint32_t)(buf * BN + gi * 32), v);
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) acc[gi * 32 + j] += (AccT)__uint_as_float(v[j]);
+                }
+                asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+                __syncwarp();
+                if (lane == 0)
+                    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(&acce[buf])) : "memory");
+            }
+            const int row = m0 + quad * 32 + lane;
+            if (!ok || *abort_flag || iters == 0 || row >= epi.M) continue;
+            if (TRACE) {
+#pragma unroll
+                for (int j = 0; j < HALF; ++j) {
+                    const int col = n0 + half * HALF + j;
+                    if (col < epi.N) {
+                        const double val = tr.scale * (double)acc[j];
+                        const long fr = tr.row_map ? (long)tr.row_map[row] : tr.p_off + row;
+                        const long fc = tr.col_map ? (long)tr.col_map[col] : tr.q_off + col;
+                        atomicAdd(tr.F + fr * tr.ldF + fc, val);
+                        if (tr.sym) atomicAdd(tr.F + fc * tr.ldF + fr, val);
+                    }
+                }
+            } else {
+                // Row-major planes in 16-byte stores of 8 columns; the transposed
+                // planes column by column (32 lanes = 32 consecutive rows).
+                const int cbase = n0 + half * HALF;
+#pragma unroll
+                for (int j0 = 0; j0 < HALF; j0 += 8) {
+                    float x[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) x[u] = (float)acc[j0 + u];
+                    if (epi.Cf) {
+#pragma unroll
+                        for (int u = 0; u < 8; ++u)
+                            if (cbase + j0 + u < epi.N) epi.Cf[(long)row * epi.ldc + cbase + j0 + u] = x[u];
+                    }
+                    for (int p = 0; p < epi.x_planes && (epi.X || epi.XT); ++p) {
+                        __nv_bfloat16 h[8];
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) {
+                            h[u] = __float2bfloat16_rn(x[u]);
+                            x[u] -= __bfloat162float(h[u]);
+                        }
+                        if (epi.X) {
+                            __nv_bfloat16* dst = epi.X + p * epi.x_plane + (long)row * epi.ldx + cbase + j0;
+                            if (cbase + j0 + 8 <= epi.N) {
+                                uint4 w;
+                                w.x = (uint32_t)__bfloat16_as_ushort(h[0]) | ((uint32_t)__bfloat16_as_ushort(h[1]) << 16);
+                                w.y = (uint32_t)__bfloat16_as_ushort(h[2]) | ((uint32_t)__bfloat16_as_ushort(h[3]) << 16);
+                                w.z = (uint32_t)__bfloat16_as_ushort(h[4]) | ((uint32_t)__bfloat16_as_ushort(h[5]) << 16);
+                                w.w = (uint32_t)__bfloat16_as_ushort(h[6]) | ((uint32_t)__bfloat16_as_ushort(h[7]) << 16);
+                                *reinterpret_cast<uint4*>(dst) = w;
+                            } else {
+                                for (int u = 0; u < 8; ++u)
+                                    if (cbase + j0 + u < epi.N) dst[u] = h[u];
+                            }
+                        }
+                        if (epi.XT) {
+#pragma unroll
+                            for (int u = 0; u < 8; ++u)
+                                if (cbase + j0 + u < epi.N)
+                                    epi.XT[p * epi.xt_plane + (long)(cbase + j0 + u) * epi.ldxt + row] = h[u];
+                        }
+                    }
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 1) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TMEM_COLS));
+    }
+    if (threadIdx.x == 0 && *abort_flag && err) atomicExch(err, 1);
+}
+
+// --- host: tensor maps through the driver entry point (no link-time libcuda) ---
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+// 3D bf16 map: dims (K, rows, planes), row stride ld elements, plane stride ps elements;
+// box (64, box_rows, 1) with 128B swizzle.
+int make_map(CUtensorMap* map, const void* base, long K, long rows, long ld, int planes, long ps, int box_rows)
+{
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return CF_ERR_CUDA;
+    if (((uintptr_t)base & 15) || (ld * 2) % 16 || (ps * 2) % 16) return CF_ERR_ARG;
+    cuuint64_t dims[3] = {(cuuint64_t)K, (cuuint64_t)rows, (cuuint64_t)planes};
+    cuuint64_t strides[2] = {(cuuint64_t)ld * 2, (cuuint64_t)(ps > 0 ? ps : ld * rows) * 2};
+    cuuint32_t box[3] = {(cuuint32_t)BK, (cuuint32_t)box_rows, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? CF_OK : CF_ERR_ARG;
+}
+
+// 4D bf16 map for the trace mode: dims (l: K2, k: K1, row: rows, plane), strides
+// ldk (between k), ldr (between rows), ps (between planes), box (64, 1, box_rows, 1).
+int make_map4(CUtensorMap* map, const void* base, long K2, long K1, long rows, int planes, long ldk, long ldr,
+              long ps, int box_rows)
+{
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return CF_ERR_CUDA;
+    if (((uintptr_t)base & 15) || (ldk * 2) % 16 || (ldr * 2) % 16 || (ps * 2) % 16) return CF_ERR_ARG;
+    cuuint64_t dims[4] = {(cuuint64_t)K2, (cuuint64_t)K1, (cuuint64_t)rows, (cuuint64_t)planes};
+    cuuint64_t strides[3] = {(cuuint64_t)ldk * 2, (cuuint64_t)ldr * 2, (cuuint64_t)(ps > 0 ? ps : 16) * 2};
+    cuuint32_t box[4] = {(cuuint32_t)BK, 1, (cuuint32_t)box_rows, 1};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? CF_OK : CF_ERR_ARG;
+}
+
+template <int BN, int STAGES, bool TRACE, int KC>
+int launch_gemm_kc(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, int K, const Terms& t,
+                   const EpiArgs& e, const TraceArgs& tr, int splits, int* err, cudaStream_t st)
+{
+    const size_t smem = 1024 + (size_t)STAGES * (BM * BK * 2 + BN * BK * 2) + 256;
+    static bool attr = false;
+    if (!attr) {
+        CF_CHECK(cudaFuncSetAttribute(k_umma_gemm<BN, STAGES, TRACE, KC>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr = true;
+    }
+    int dev = 0, sms = 0;
+    CF_CHECK(cudaGetDevice(&dev));
+    CF_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const long tiles = (long)cf_cdiv(M, BM) * cf_cdiv(N, BN) * splits;
+    const int grid = (int)(tiles < sms ? tiles : sms);
+    k_umma_gemm<BN, STAGES, TRACE, KC><<<grid, NTHREADS, smem, st>>>(ma, mb, K, splits, t, e, tr, err);
+    CF_CHECK_LAUNCH();
+    return CF_OK;
+}
+
+// Promotion interval (k-tiles of 64 per FP32 accumulator): 1, 2, 4, 8 or 16.
+int g_promote_kc = 16;
+
+template <int BN, int STAGES, bool TRACE>
+int launch_gemm(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, int K, const Terms& t,
+                const EpiArgs& e, const TraceArgs& tr, int splits, int* err, cudaStream_t st)
+{
+    switch (g_promote_kc) {
+        case 1: return launch_gemm_kc<BN, STAGES, TRACE, 1>(ma, mb, M, N, K, t, e, tr, splits, err, st);
+        case 2: return launch_gemm_kc<BN, STAGES, TRACE, 2>(ma, mb, M, N, K, t, e, tr, splits, err, st);
+        case 8: return launch_gemm_kc<BN, STAGES, TRACE, 8>(ma, mb, M, N, K, t, e, tr, splits, err, st);
+        case 16: return launch_gemm_kc<BN, STAGES, TRACE, 16>(ma, mb, M, N, K, t, e, tr, splits, err, st);
+        default: return launch_gemm_kc<BN, STAGES, TRACE, 4>(ma, mb, M, N, K, t, e, tr, splits, err, st);
+    }
+}
+
+}  // namespace
+
+int cf_umma_trace_impl(int P1, int P2, int K1, int K2, int nterms, const int* ta, const int* tb, const void* X,
+                       long sXp, long ldX, long x_ps, int x_planes, const void* Y, long sYq, long ldY, long y_ps,
+                       int y_planes, double scale, double* F, long ldF, long p_off, long q_off, int sym,
+                       const int* row_map, const int* col_map, int splits, int* err, void* stream);
+
+// Set the promotion interval of the tensor-core kernels (k-tiles of 64 summed
+// in one FP32 TMEM accumulator before the partial is promoted): 1, 2, 4,
+// 8 or 16 (default).  Returns the previous value.
+extern "C" int cf_umma_set_promotion(int kc)
+{
+    const int prev = g_promote_kc;
+    if (kc == 1 || kc == 2 || kc == 4 || kc == 8 || kc == 16) g_promote_kc = kc;
+    return prev;
+}
+
+// C = sum_t A_{ta[t]} B_{tb[t]}^T with BF16 split planes, FP32 accumulation.
+//   A: planes of M x K (row stride lda, plane stride a_ps), B: planes of N x K.
+//   Outputs (any may be NULL): X = C as x_planes BF16 split planes (M x N,
+//   ldx, plane stride x_ps); XT = C^T likewise (N x M, ldxt, xt_ps);
+//   Cf = C in FP32 (M x N, ldc).  err: device int set to 1 if a wait ran out.
+extern "C" int cf_umma_gemm_bf16(int M, int N, int K, int nterms, const int* ta, const int* tb, const void* A,
+                                 long lda, long a_ps, int a_planes, const void* B, long ldb, long b_ps,
+                                 int b_planes, void* X, long ldx, long x_ps, int x_planes, void* XT, long ldxt,
+                                 long xt_ps, float* Cf, long ldc, int* err, void* stream)
+{
+    if (M <= 0 || N <= 0 || K <= 0 || nterms < 1 || nterms > MAX_TERMS || !A || !B) return CF_ERR_ARG;
+    if ((X || XT) && (x_planes < 1 || x_planes > 3)) return CF_ERR_ARG;
+    Terms t{};
+    t.n = nterms;
+    for (int i = 0; i < nterms; ++i) {
+        if (ta[i] < 0 || ta[i] >= a_planes || tb[i] < 0 || tb[i] >= b_planes) return CF_ERR_ARG;
+        t.a[i] = ta[i];
+        t.b[i] = tb[i];
+    }
+    CUtensorMap ma, mb;
+    int rc = make_map(&ma, A, K, M, lda, a_planes, a_ps, BM);
+    if (rc) return rc;
+    rc = make_map(&mb, B, K, N, ldb, b_planes, b_ps, 256);
+    if (rc) return rc;
+    EpiArgs e{(__nv_bfloat16*)X, ldx, x_ps, x_planes, (__nv_bfloat16*)XT, ldxt, xt_ps, Cf, ldc, M, N};
+    TraceArgs tr{};
+    cudaStream_t st = (cudaStream_t)stream;
+    return launch_gemm<256, 4, false>(ma, mb, M, N, K, t, e, tr, 1, err, st);
+}
+
+// Fisher contraction on the tensor cores:
+//   F[(p_off+p) ldF + q_off+q] += scale sum_t sum_{k<K1, l<K2} X_{ta[t]}[p, k, l] Y_{tb[t]}[q, k, l]
+// X_s[p, k, l] = X[s*x_ps + p*sXp + k*ldX + l] (BF16 planes), Y likewise; the
+// mirror entry too when sym.  F (FP64) accumulates partial sums of `splits`
+// CTAs per output tile with atomics; zero it first.
+extern "C" int cf_umma_trace_bf16_mapped(int P1, int P2, int K1, int K2, int nterms, const int* ta,
+                                         const int* tb, const void* X, long sXp, long ldX, long x_ps, int x_planes,
+                                         const void* Y, long sYq, long ldY, long y_ps, int y_planes, double scale,
+                                         double* F, long ldF, const int* row_map, const int* col_map, int splits,
+                                         int* err, void* stream);
+
+extern "C" int cf_umma_trace_bf16(int P1, int P2, int K1, int K2, int nterms, const int* ta, const int* tb,
+                                  const void* X, long sXp, long ldX, long x_ps, int x_planes, const void* Y,
+                                  long sYq, long ldY, long y_ps, int y_planes, double scale, double* F, long ldF,
+                                  long p_off, long q_off, int sym, int splits, int* err, void* stream)
+{
+    return cf_umma_trace_impl(P1, P2, K1, K2, nterms, ta, tb, X, sXp, ldX, x_ps, x_planes, Y, sYq, ldY, y_ps,
+                              y_planes, scale, F, ldF, p_off, q_off, sym, nullptr, nullptr, splits, err, stream);
+}
+
+// As cf_umma_trace_bf16, with output row p going to F row row_map[p] and column
+// q to F column col_map[q] (device int arrays); no mirror entry.
+extern "C" int cf_umma_trace_bf16_mapped(int P1, int P2, int K1, int K2, int nterms, const int* ta,
+                                         const int* tb, const void* X, long sXp, long ldX, long x_ps, int x_planes,
+                                         const void* Y, long sYq, long ldY, long y_ps, int y_planes, double scale,
+                                         double* F, long ldF, const int* row_map, const int* col_map, int splits,
+                                         int* err, void* stream)
+{
+    if (!row_map || !col_map) return CF_ERR_ARG;
+    return cf_umma_trace_impl(P1, P2, K1, K2, nterms, ta, tb, X, sXp, ldX, x_ps, x_planes, Y, sYq, ldY, y_ps,
+                              y_planes, scale, F, ldF, 0, 0, 0, row_map, col_map, splits, err, stream);
+}
+
+int cf_umma_trace_impl(int P1, int P2, int K1, int K2, int nterms, const int* ta, const int* tb, const void* X,
+                       long sXp, long ldX, long x_ps, int x_planes, const void* Y, long sYq, long ldY, long y_ps,
+                       int y_planes, double scale, double* F, long ldF, long p_off, long q_off, int sym,
+                       const int* row_map, const int* col_map, int splits, int* err, void* stream)
+{
+    if (P1 <= 0 || P2 <= 0 || K1 <= 0 || K2 <= 0 || nterms < 1 || nterms > MAX_TERMS || !X || !Y || !F)
+        return CF_ERR_ARG;
+    Terms t{};
+    t.n = nterms;
+    for (int i = 0; i < nterms; ++i) {
+        if (ta[i] < 0 || ta[i] >= x_planes || tb[i] < 0 || tb[i] >= y_planes) return CF_ERR_ARG;
+        t.a[i] = ta[i];
+        t.b[i] = tb[i];
+    }
+    CUtensorMap ma, mb;
+    int rc = make_map4(&ma, X, K2, K1, P1, x_planes, ldX, sXp, x_ps, BM);
+    if (rc) return rc;
+    const bool narrow = P2 <= 64;
+    rc = make_map4(&mb, Y, K2, K1, P2, y_planes, ldY, sYq, y_ps, narrow ? 64 : 128);
+    if (rc) return rc;
+    const long tiles = (long)K1 * ((K2 + BK - 1) / BK);
+    const int out_tiles = cf_cdiv(P1, BM) * cf_cdiv(P2, narrow ? 64 : 128);
+    if (splits <= 0) splits = (148 * 2 + out_tiles - 1) / out_tiles;
+    if (splits > tiles) splits = (int)tiles;
+    EpiArgs e{};
+    e.M = P1;
+    e.N = P2;
+    TraceArgs tr{K1, K2, F, ldF, p_off, q_off, sym, scale, row_map, col_map};
+    cudaStream_t st = (cudaStream_t)stream;
+    if (narrow) return launch_gemm<64, 8, true>(ma, mb, P1, P2, 0, t, e, tr, splits, err, st);
+    return launch_gemm<128, 6, true>(ma, mb, P1, P2, 0, t, e, tr, splits, err, st);
+}

@@ -60,3 +60,39 @@ unsigned long long g_cf_launch_count = 0;
 extern "C" unsigned long long cf_launch_count(void) { return g_cf_launch_count; }
 
 extern "C" int cf_version(void) { return 1; }
+
+#include <cuda_bf16.h>
+
+namespace {
+
+// out[p][r][c] = p-th BF16 split plane of X[r][c]: x_0 = bf16(x), x_1 = bf16(x - x_0), ...
+__global__ void k_split_bf16(int R, int C, const double* X, long ldx, int planes, __nv_bfloat16* out, long ldo,
+                             long plane_stride)
+{
+    const long total = (long)R * C;
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+        const long r = e / C, c = e % C;
+        double x = X[r * ldx + c];
+        for (int p = 0; p < planes; ++p) {
+            __nv_bfloat16 h = __double2bfloat16(x);
+            out[p * plane_stride + r * ldo + c] = h;
+            x -= (double)__bfloat162float(h);
+        }
+    }
+}
+
+}  // namespace
+
+// BF16 split planes of an R x C FP64 matrix (row stride ldx) into `planes`
+// planes of row stride ldo, `plane_stride` elements apart.
+extern "C" int cf_split_bf16(int R, int C, const double* X, long ldx, int planes, void* out, long ldo,
+                             long plane_stride, void* stream)
+{
+    if (R <= 0 || C <= 0 || !X || !out || planes < 1 || planes > 3) return CF_ERR_ARG;
+    long blocks = ((long)R * C + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_split_bf16<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(R, C, X, ldx, planes, (__nv_bfloat16*)out,
+                                                                     ldo, plane_stride);
+    CF_CHECK_LAUNCH();
+    return CF_OK;
+}

@@ -117,8 +117,10 @@ class Engine:
         ws = self.lib.cf_spd_inverse_workspace(n, B)
         work = torch.empty(ws // 8 + 1, dtype=F64, device=A.device)
         info = torch.zeros(B, dtype=torch.int32, device=A.device)
+        ev = self._probe_begin("spd_inverse")
         check(self.lib.cf_spd_inverse(n, A.data_ptr(), n, n * n, B, work.data_ptr(), info.data_ptr(),
                                       stream()), "cf_spd_inverse")
+        self._probe_end("spd_inverse", ev, 0)
         bad = info.cpu()
         if int(bad.abs().max()) != 0:
             raise ValueError(f"dpotrf failed with info={int(bad[bad != 0][0])}")

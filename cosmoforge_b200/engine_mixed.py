@@ -1,0 +1,216 @@
+"""Mixed-precision Fisher on the tensor cores (tcgen05 BF16 split products).
+
+Same algebra as ``engine.Engine.fisher_qml`` (``qube/fisher.py:501-607``), with
+the two O(P n^3) / O(P^2 n^2) stages moved to the 5th-generation tensor
+cores:
+
+* C^-1 (FP64, from the Jacobi-scaled Cholesky inverse) is split into BF16
+  planes c = c_0 + c_1 (+ c_2); the derivative blocks of one spectrum are
+  emitted by the pair builder directly as BF16 planes (FP64 recurrences,
+  split at the store);
+* A_b = C^-1 dC_b runs as the split-product GEMM ``cf_umma_gemm_bf16``
+  (FP32 accumulation in TMEM) whose epilogue writes A_b, and A_b^T, as BF16
+  planes again;
+* the traces F_pq = 1/2 sum_{k,l} A_p[k,l] A_q[l,k] run as the tensor-core
+  contraction ``cf_umma_trace_bf16`` over the flattened (k, l) plane, partial
+  sums added into an FP64 F.
+
+Schemes: ``bf16x3`` = planes {(0,0), (0,1), (1,0)} (~16 bits per product),
+``bf16x6`` adds {(0,2), (1,1), (2,0)} (~24 bits).  The quadratic forms q and
+the noise bias stay FP64 (one FP64 derivative pass per spectrum): they carry
+the q - b cancellation and cost little.
+
+Field segments are placed at 8-element-aligned offsets of a padded index
+space (zero rows / columns in the gaps) so every TMA box starts 16-byte
+aligned whatever the pixel counts.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import layout as lay
+from ._lib import check, stream
+from .engine import Engine, _off
+
+BF16 = torch.bfloat16
+SCHEMES = {
+    "bf16x3": (2, (0, 0, 1), (0, 1, 0)),
+    "bf16x6": (3, (0, 0, 1, 0, 1, 2), (0, 1, 0, 2, 1, 0)),
+}
+
+
+def _r8(x: int) -> int:
+    return (int(x) + 7) // 8 * 8
+
+
+class MixedPlan:
+    """Padded segment layout and plane buffers for one layout and scheme."""
+
+    def __init__(self, E: Engine, scheme: str):
+        if scheme not in SCHEMES:
+            raise ValueError(f"unknown scheme {scheme!r}; expected one of {list(SCHEMES)}")
+        self.E = E
+        self.planes, ta, tb = SCHEMES[scheme]
+        self.nterms = len(ta)
+        self._ta = (ctypes.c_int * len(ta))(*ta)
+        self._tb = (ctypes.c_int * len(tb))(*tb)
+        L = E.L
+        self.po = []  # padded offset of each field segment
+        off = 0
+        for f in L.fields:
+            self.po.append(off)
+            off = _r8(off + f.nrows)
+        self.n_pad = off
+        self.err = torch.zeros(1, dtype=torch.int32, device=E.dev)
+
+    @property
+    def ta(self):
+        return ctypes.cast(self._ta, ctypes.c_void_p)
+
+    @property
+    def tb(self):
+        return ctypes.cast(self._tb, ctypes.c_void_p)
+
+    def split_cinv(self, Cinv: torch.Tensor) -> torch.Tensor:
+        L, E = self.E.L, self.E
+        npd = self.n_pad
+        Cp = torch.zeros((self.planes, npd, npd), dtype=BF16, device=E.dev)
+        for fi, f in enumerate(L.fields):
+            for gi, g in enumerate(L.fields):
+                src = _off(Cinv, f.offset * L.n + g.offset)
+                dst = _off(Cp, self.po[fi] * npd + self.po[gi])
+                check(E.lib.cf_split_bf16(f.nrows, g.nrows, src, L.n, self.planes, dst, npd, npd * npd,
+                                          stream()), "cf_split_bf16")
+        return Cp
+
+
+def _build_planes(plan: MixedPlan, s: int):
+    """BF16 planes of the derivative blocks of spectrum s as GEMM B operands.
+
+    Returns {segment: (B planes tensor, K, k_seg)}: B rows are (bin, j) for
+    output columns j in `segment` (each bin padded to a multiple of 8 rows,
+    the padding rows zero), the K index runs over segment `k_seg`.
+    """
+    E, L = plan.E, plan.E.L
+    blk = L.blocks[E.block_of_spec[s]]
+    fa, fb = L.fields[blk.fa], L.fields[blk.fb]
+    nb, Lp = L.nbins, L.lmax_signal + 1
+    mode = L.spectra[s].mode
+    t0 = _off(E.deriv_tab, s * Lp)
+    bins = _off(E.deriv_bin, s * Lp)
+    P = plan.planes
+    va, vb = E.vec[blk.fa], E.vec[blk.fb]
+    def alloc(rows_per_bin, rows_pad, ld):
+        mk = torch.empty if rows_pad == rows_per_bin else torch.zeros
+        return mk((P, nb * rows_pad, ld), dtype=BF16, device=E.dev)
+
+    if blk.kind in (lay.KIND_00_AUTO, lay.KIND_22_AUTO):
+        m = fa.nrows
+        mp = ldm = _r8(m)
+        D = alloc(m, mp, ldm)
+        ps = nb * mp * ldm
+        check(E.lib.cf_build_block_planes(
+            blk.kind, mode, fa.npix, va.data_ptr(), fb.npix, vb.data_ptr(), L.lmax_signal, t0, None, None,
+            bins, D.data_ptr(), ldm, 0, 0, mp * ldm, D.data_ptr(), ldm, 0, 0, mp * ldm, 1, 0, 0, P, ps, ps,
+            stream()), "cf_build_block_planes")
+        return blk, {blk.fa: (D, m, blk.fa)}
+    R, Cc = fb.nrows, fa.nrows
+    Rp = ldR = _r8(R)
+    Cp_ = ldC = _r8(Cc)
+    Dba = alloc(R, Rp, ldC)  # [b][r in fb (padded)][c in fa]
+    Dab = alloc(Cc, Cp_, ldR)  # [b][c in fa (padded)][r in fb]
+    check(E.lib.cf_build_block_planes(
+        blk.kind, mode, fa.npix, va.data_ptr(), fb.npix, vb.data_ptr(), L.lmax_signal, t0, None, None,
+        bins, Dba.data_ptr(), ldC, 0, 0, Rp * ldC, Dab.data_ptr(), ldR, 0, 0, Cp_ * ldR, 1, 0, 0, P,
+        nb * Rp * ldC, nb * Cp_ * ldR, stream()), "cf_build_block_planes")
+    # output columns in fa: K over fb with B[b][j in fa][k in fb] = Dab;
+    # output columns in fb: K over fa with B[b][j in fb][k in fa] = Dba
+    return blk, {blk.fa: (Dab, R, blk.fb), blk.fb: (Dba, Cc, blk.fa)}
+
+
+def fisher(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6") -> torch.Tensor:
+    """F (P x P, FP64) with the A_b GEMMs and traces on the tensor cores.
+
+    A_b is kept for every parameter in one buffer per column segment (field):
+    ``X[f]`` holds, for every spectrum whose derivative touches columns of
+    field f, its bins' column slabs side by side (n_pad x sum nb * m_f), and
+    ``XT[f]`` their transposes.  After all spectra, each ordered segment pair
+    (s, t) is one tensor-core contraction of all parameters touching s against
+    all parameters touching t, scattered into F through parameter-index maps.
+    """
+    plan = MixedPlan(E, scheme)
+    L = E.L
+    nb, P = L.nbins, L.n_params
+    npd = plan.n_pad
+    Pl = plan.planes
+    ev = E._probe_begin("split_cinv")
+    Cp = plan.split_cinv(Cinv)
+    E._probe_end("split_cinv", ev, 0)
+    segrows = {i: f.nrows for i, f in enumerate(L.fields)}
+    segpad = {i: _r8(f.nrows) for i, f in enumerate(L.fields)}
+    cols_of = {}
+    for s in range(L.nspectra):
+        blk = L.blocks[E.block_of_spec[s]]
+        cols_of[s] = [blk.fa] if blk.fa == blk.fb else [blk.fa, blk.fb]
+    seg_specs = {f: [s for s in range(L.nspectra) if f in cols_of[s]] for f in range(len(L.fields))}
+    X, XT, pmap, ldseg = {}, {}, {}, {}
+    for f, specs in seg_specs.items():
+        if not specs:
+            continue
+        ncols = len(specs) * nb * segpad[f]
+        ldseg[f] = _r8(ncols)
+        X[f] = torch.empty((Pl, npd, ldseg[f]), dtype=BF16, device=E.dev)
+        XT[f] = torch.empty((Pl, ncols, npd), dtype=BF16, device=E.dev)
+        pmap[f] = torch.tensor([s * nb + b for s in specs for b in range(nb)], dtype=torch.int32,
+                               device=E.dev)
+    for s in range(L.nspectra):
+        ev = E._probe_begin("build_planes")
+        blk, ops = _build_planes(plan, s)
+        E._probe_end("build_planes", ev, 0)
+        for seg, (B, K, kseg) in ops.items():
+            N = nb * segpad[seg]
+            col0 = seg_specs[seg].index(s) * N
+            Xs, XTs = X[seg], XT[seg]
+            ev = E._probe_begin("a_gemm_mixed")
+            torch.cuda.nvtx.range_push("a_gemm_mixed")
+            check(E.lib.cf_umma_gemm_bf16(
+                npd, N, K, plan.nterms, plan.ta, plan.tb, _off(Cp, plan.po[kseg]), npd, npd * npd, Pl,
+                B.data_ptr(), B.shape[2], B.shape[1] * B.shape[2], Pl,
+                _off(Xs, col0), ldseg[seg], npd * ldseg[seg], Pl,
+                _off(XTs, col0 * npd), npd, XTs.shape[1] * npd, None, 0,
+                plan.err.data_ptr(), stream()), "cf_umma_gemm_bf16")
+            torch.cuda.nvtx.range_pop()
+            E._probe_end("a_gemm_mixed", ev, 2.0 * npd * N * K * plan.nterms)
+        del ops
+    F = torch.zeros((P, P), dtype=torch.float64, device=E.dev)
+    for ss in X:
+        for tt in X:
+            P1, P2 = pmap[ss].numel(), pmap[tt].numel()
+            m_s, m_t = segrows[ss], segrows[tt]
+            ev = E._probe_begin("trace_mixed")
+            torch.cuda.nvtx.range_push("trace_mixed")
+            check(E.lib.cf_umma_trace_bf16_mapped(
+                P1, P2, m_t, m_s, plan.nterms, plan.ta, plan.tb,
+                _off(X[ss], plan.po[tt] * ldseg[ss]), segpad[ss], ldseg[ss], npd * ldseg[ss], Pl,
+                _off(XT[tt], plan.po[ss]), segpad[tt] * npd, npd, XT[tt].shape[1] * npd, Pl,
+                0.5, F.data_ptr(), P, pmap[ss].data_ptr(), pmap[tt].data_ptr(), 0,
+                plan.err.data_ptr(), stream()), "cf_umma_trace_bf16_mapped")
+            torch.cuda.nvtx.range_pop()
+            E._probe_end("trace_mixed", ev, 2.0 * P1 * P2 * m_t * m_s * plan.nterms)
+    del X, XT
+    if int(plan.err.item()) != 0:
+        raise RuntimeError("tensor-core kernel reported a timed-out wait")
+    return F
+
+
+def fisher_qml(E: Engine, Cinv: torch.Tensor, N: torch.Tensor | None = None,
+               maps: torch.Tensor | None = None, scheme: str = "bf16x6"):
+    """Mixed F, FP64 bias and q (same return convention as Engine.fisher_qml)."""
+    F = fisher(E, Cinv, scheme)
+    ev = E._probe_begin("qml_fp64")
+    _, bias, q = E.fisher_qml(Cinv, N, maps, want_fisher=False)
+    E._probe_end("qml_fp64", ev, 0)
+    return F, bias, q
