@@ -323,8 +323,10 @@ def main():
             peak = fp64_peak_tflops(torch)
             peak_src = "measured cuBLAS DGEMM 8192^3 in this run (FP64 tensor)"
         else:
-            peak = peaks.get("bf16_tflops", 1590.0)
-            peak_src = "MEASURED_PEAKS.json bf16_tflops" if peaks else "fallback 1.59 PFLOP/s"
+            # the GEMM runs inside a long step under the power cap: sustained figure
+            peak = peaks.get("bf16_tflops_sustained", 1400.0)
+            peak_src = ("MEASURED_PEAKS.json bf16_tflops_sustained (kernel timed inside a long step)"
+                        if peaks else "fallback 1.4 PFLOP/s sustained")
         achieved = k_work / k_time / 1e12 if k_time > 0 else 0.0
         traffic = None
         tf = ROOT / "profiles" / "traffic.json"

@@ -28,7 +28,7 @@ SIGNATURES = {
     "cf_build_block": (_i, [_i, _i, _i, _p, _i, _p, _i, _p, _p, _p, _p, _p, _l, _l, _l, _l, _p, _l,
                             _l, _l, _l, _i, _l, _l, _p]),
     "cf_build_block_planes": (_i, [_i, _i, _i, _p, _i, _p, _i, _p, _p, _p, _p, _p, _l, _l, _l, _l, _p,
-                                   _l, _l, _l, _l, _i, _l, _l, _i, _l, _l, _p]),
+                                   _l, _l, _l, _l, _i, _l, _l, _i, _l, _l, _i, _p]),
     "cf_dgemm": (_i, [_i, _i, _i, _i, _i, _d, _p, _l, _l, _p, _l, _l, _d, _p, _l, _l, _p, _l, _l,
                       _i, _i, _p]),
     "cf_potrf": (_i, [_i, _p, _l, _l, _i, _p, _p]),
@@ -49,6 +49,7 @@ SIGNATURES = {
     "cf_umma_set_promotion": (_i, [_i]),
     "cf_umma_trace_bf16_mapped": (_i, [_i, _i, _i, _i, _i, _p, _p, _p, _l, _l, _l, _i, _p, _l, _l, _l, _i,
                                        _d, _p, _l, _p, _p, _i, _p, _p]),
+    "cf_outer_planes": (_i, [_i, _i, _p, _p, _l, _i, _p, _l, _l, _l, _p]),
     "cf_split_bf16": (_i, [_i, _i, _p, _l, _i, _p, _l, _l, _p]),
     "cf_umma_gemm_bf16": (_i, [_i, _i, _i, _i, _p, _p, _p, _l, _l, _i, _p, _l, _l, _i, _p, _l, _l, _i,
                                _p, _l, _l, _p, _l, _p, _p]),

@@ -46,6 +46,8 @@ struct BuildArgs {
     long ostride;   // batch stride of out and outT
     int planes;     // 0: FP64 output; 1..3: BF16 split planes of the FP64 value
     long plane_stride, planeT_stride;
+    int full;       // compute every pair of an auto block (no mirror writes)
+    int trans;      // threads walk (col pixel, row pixel) and write only the transposed entry
 };
 
 __device__ __forceinline__ void rotation_angle(double r1x, double r1y, double r1z, double r2x,
@@ -98,8 +100,10 @@ struct Emitter {
     {
         const long i = base + (a.row_off + r) * a.ld + a.col_off + bin * a.bin_stride + c;
         const long iT = base + (a.rowT_off + c) * a.ldT + a.colT_off + bin * a.binT_stride + r;
+        const bool prim = !a.trans;
+        mirror = a.trans || (mirror && !a.full);
         if (a.planes == 0) {
-            a.out[i] = v;
+            if (prim) a.out[i] = v;
             if (mirror) a.outT[iT] = v;
             return;
         }
@@ -108,7 +112,7 @@ struct Emitter {
         double x = v;
         for (int p = 0; p < a.planes; ++p) {
             const __nv_bfloat16 h = __double2bfloat16(x);
-            o[p * a.plane_stride + i] = h;
+            if (prim) o[p * a.plane_stride + i] = h;
             if (mirror) oT[p * a.planeT_stride + iT] = h;
             x -= (double)__bfloat162float(h);
         }
@@ -184,11 +188,13 @@ __global__ void __launch_bounds__(BX* BY) k_build(BuildArgs a)
     }
     __syncthreads();
 
-    const int i = blockIdx.x * BX + threadIdx.x;  // column pixel (field a)
-    const int j = blockIdx.y * BY + threadIdx.y;  // row pixel (field b)
+    // column pixel i (field a), row pixel j (field b); the transposed launch
+    // walks j along threadIdx.x so that its (transposed) writes coalesce
+    const int i = a.trans ? blockIdx.y * BY + threadIdx.y : blockIdx.x * BX + threadIdx.x;
+    const int j = a.trans ? blockIdx.x * BX + threadIdx.x : blockIdx.y * BY + threadIdx.y;
     const bool autob = (a.kind == K00A || a.kind == K22A);
     if (i >= a.na || j >= a.nb) return;
-    if (autob && j < i) return;
+    if (autob && !a.full && j < i) return;
 
     const double r2x = a.va[i], r2y = a.va[a.na + i], r2z = a.va[2 * a.na + i];
     const double r1x = a.vb[j], r1y = a.vb[a.nb + j], r1z = a.vb[2 * a.nb + j];
@@ -266,6 +272,12 @@ __global__ void __launch_bounds__(BX* BY) k_build(BuildArgs a)
                     em.put(j, i, b, qq, false);
                     em.put(j + n, i + n, b, uu, false);
                     em.put(j + n, i, b, qu, true);
+                    if (a.full) em.put(j, i + n, b, qu, false);
+                } else if (a.full) {  // this pair owns its entries in rows j and j + n
+                    em.put(j, i, b, vqq, false);
+                    em.put(j + n, i + n, b, vuu, false);
+                    em.put(j + n, i, b, vuq, false);
+                    em.put(j, i + n, b, vqu, false);
                 } else {
                     em.put(j, i, b, vqq, true);
                     em.put(j + n, i + n, b, vuu, true);
@@ -312,7 +324,7 @@ extern "C" int cf_build_block_planes(int kind, int mode, int na, const double* v
                                      const int* bin_of, void* out, long ld, long row_off, long col_off,
                                      long bin_stride, void* outT, long ldT, long rowT_off, long colT_off,
                                      long binT_stride, int batch, long tstride, long ostride, int planes,
-                                     long plane_stride, long planeT_stride, void* stream);
+                                     long plane_stride, long planeT_stride, int flags, void* stream);
 
 extern "C" int cf_build_block(int kind, int mode, int na, const double* va, int nb, const double* vb,
                               int lmax, const double* t0, const double* t1, const double* t2,
@@ -322,18 +334,22 @@ extern "C" int cf_build_block(int kind, int mode, int na, const double* va, int 
 {
     return cf_build_block_planes(kind, mode, na, va, nb, vb, lmax, t0, t1, t2, bin_of, out, ld, row_off, col_off,
                                  bin_stride, outT, ldT, rowT_off, colT_off, binT_stride, batch, tstride, ostride,
-                                 0, 0, 0, stream);
+                                 0, 0, 0, 0, stream);
 }
 
 // As cf_build_block, with `planes` >= 1 writing BF16 split planes (out/outT
 // are then __nv_bfloat16 arrays, planes `plane_stride` / `planeT_stride`
-// elements apart) instead of FP64.
+// elements apart) instead of FP64.  flags bit 0 (auto blocks): every entry
+// of the block is computed from its own pixel pair and written once, no
+// mirror writes (symmetric entries then agree to rounding, not bit for bit);
+// bit 1 (cross blocks): write only the transposed block outT, threads
+// walking the row field fastest so the writes coalesce.
 extern "C" int cf_build_block_planes(int kind, int mode, int na, const double* va, int nb, const double* vb,
                                      int lmax, const double* t0, const double* t1, const double* t2,
                                      const int* bin_of, void* out, long ld, long row_off, long col_off,
                                      long bin_stride, void* outT, long ldT, long rowT_off, long colT_off,
                                      long binT_stride, int batch, long tstride, long ostride, int planes,
-                                     long plane_stride, long planeT_stride, void* stream)
+                                     long plane_stride, long planeT_stride, int flags, void* stream)
 {
     if (kind < K00A || kind > K02 || na <= 0 || nb <= 0 || lmax < 0 || lmax > MAXL || !va || !vb ||
         !out || !outT || !t0)
@@ -341,11 +357,13 @@ extern "C" int cf_build_block_planes(int kind, int mode, int na, const double* v
     if ((kind == K00A || kind == K22A) && (na != nb || va != vb)) return CF_ERR_ARG;
     if (batch < 1) return CF_ERR_ARG;
     if (planes < 0 || planes > 3) return CF_ERR_ARG;
+    const int full = flags & 1, trans = (flags >> 1) & 1;
+    if (trans && (kind == K00A || kind == K22A)) return CF_ERR_ARG;
     BuildArgs a{kind, mode, na, nb, va, vb, lmax, t0, t1, t2, bin_of, (double*)out, ld, row_off, col_off,
                 bin_stride, (double*)outT, ldT, rowT_off, colT_off, binT_stride, tstride, ostride, planes,
-                plane_stride, planeT_stride};
+                plane_stride, planeT_stride, full, trans};
     dim3 block(BX, BY);
-    dim3 grid(cf_cdiv(na, BX), cf_cdiv(nb, BY), batch);
+    dim3 grid(trans ? cf_cdiv(nb, BX) : cf_cdiv(na, BX), trans ? cf_cdiv(na, BY) : cf_cdiv(nb, BY), batch);
     k_build<<<grid, block, 0, (cudaStream_t)stream>>>(a);
     CF_CHECK_LAUNCH();
     return CF_OK;

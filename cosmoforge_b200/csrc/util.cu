@@ -96,3 +96,40 @@ extern "C" int cf_split_bf16(int R, int C, const double* X, long ldx, int planes
     CF_CHECK_LAUNCH();
     return CF_OK;
 }
+
+namespace {
+
+// out[p][q][i][j] = p-th BF16 split plane of x_q[i] * y_q[j]  (i, j < n)
+__global__ void k_outer_planes(int n, int nvec, const double* x, const double* y, long ldv, int planes,
+                               __nv_bfloat16* out, long ld, long q_stride, long plane_stride)
+{
+    const long total = (long)nvec * n * n;
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+        const long q = e / ((long)n * n), rem = e % ((long)n * n);
+        const long i = rem / n, j = rem % n;
+        double v = x[i * ldv + q] * y[j * ldv + q];
+        for (int p = 0; p < planes; ++p) {
+            __nv_bfloat16 h = __double2bfloat16(v);
+            out[p * plane_stride + q * q_stride + i * ld + j] = h;
+            v -= (double)__bfloat162float(h);
+        }
+    }
+}
+
+}  // namespace
+
+// BF16 split planes of the outer products x_q y_q^T, q < nvec (x, y: n x nvec
+// column-major-by-vector with row stride ldv), into out[p][q] (n x n, row
+// stride ld, q_stride / plane_stride elements apart).
+extern "C" int cf_outer_planes(int n, int nvec, const double* x, const double* y, long ldv, int planes, void* out,
+                               long ld, long q_stride, long plane_stride, void* stream)
+{
+    if (n <= 0 || nvec <= 0 || !x || !y || !out || planes < 1 || planes > 3) return CF_ERR_ARG;
+    long blocks = ((long)nvec * n * n + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_outer_planes<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(n, nvec, x, y, ldv, planes,
+                                                                       (__nv_bfloat16*)out, ld, q_stride,
+                                                                       plane_stride);
+    CF_CHECK_LAUNCH();
+    return CF_OK;
+}

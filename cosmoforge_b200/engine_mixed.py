@@ -16,9 +16,9 @@ cores:
   sums added into an FP64 F.
 
 Schemes: ``bf16x3`` = planes {(0,0), (0,1), (1,0)} (~16 bits per product),
-``bf16x6`` adds {(0,2), (1,1), (2,0)} (~24 bits).  The quadratic forms q and
-the noise bias stay FP64 (one FP64 derivative pass per spectrum): they carry
-the q - b cancellation and cost little.
+``bf16x6`` adds {(0,2), (1,1), (2,0)} (~24 bits).  The noise bias and the
+quadratic forms are contractions of the same resident A_b slabs against
+G = N C^-1 and x (C^-1 x)^T (``_qml_core``).
 
 Field segments are placed at 8-element-aligned offsets of a padded index
 space (zero rows / columns in the gaps) so every TMA box starts 16-byte
@@ -64,6 +64,7 @@ class MixedPlan:
             self.po.append(off)
             off = _r8(off + f.nrows)
         self.n_pad = off
+        self.segments = list(range(len(L.fields)))
         self.err = torch.zeros(1, dtype=torch.int32, device=E.dev)
 
     @property
@@ -75,6 +76,7 @@ class MixedPlan:
         return ctypes.cast(self._tb, ctypes.c_void_p)
 
     def split_cinv(self, Cinv: torch.Tensor) -> torch.Tensor:
+        """BF16 planes of an n x n FP64 matrix in the padded index space."""
         L, E = self.E.L, self.E
         npd = self.n_pad
         Cp = torch.zeros((self.planes, npd, npd), dtype=BF16, device=E.dev)
@@ -85,6 +87,14 @@ class MixedPlan:
                 check(E.lib.cf_split_bf16(f.nrows, g.nrows, src, L.n, self.planes, dst, npd, npd * npd,
                                           stream()), "cf_split_bf16")
         return Cp
+
+    def pad_rows(self, V: torch.Tensor) -> torch.Tensor:
+        """Rows of an n x k FP64 array moved to their padded positions (zeros in gaps)."""
+        L = self.E.L
+        out = torch.zeros((self.n_pad, V.shape[1]), dtype=V.dtype, device=V.device)
+        for fi, f in enumerate(L.fields):
+            out[self.po[fi]: self.po[fi] + f.nrows] = V[f.offset: f.offset + f.nrows]
+        return out
 
 
 def _build_planes(plan: MixedPlan, s: int):
@@ -115,23 +125,29 @@ def _build_planes(plan: MixedPlan, s: int):
         check(E.lib.cf_build_block_planes(
             blk.kind, mode, fa.npix, va.data_ptr(), fb.npix, vb.data_ptr(), L.lmax_signal, t0, None, None,
             bins, D.data_ptr(), ldm, 0, 0, mp * ldm, D.data_ptr(), ldm, 0, 0, mp * ldm, 1, 0, 0, P, ps, ps,
-            stream()), "cf_build_block_planes")
+            1, stream()), "cf_build_block_planes")
         return blk, {blk.fa: (D, m, blk.fa)}
     R, Cc = fb.nrows, fa.nrows
     Rp = ldR = _r8(R)
     Cp_ = ldC = _r8(Cc)
     Dba = alloc(R, Rp, ldC)  # [b][r in fb (padded)][c in fa]
     Dab = alloc(Cc, Cp_, ldR)  # [b][c in fa (padded)][r in fb]
-    check(E.lib.cf_build_block_planes(
-        blk.kind, mode, fa.npix, va.data_ptr(), fb.npix, vb.data_ptr(), L.lmax_signal, t0, None, None,
-        bins, Dba.data_ptr(), ldC, 0, 0, Rp * ldC, Dab.data_ptr(), ldR, 0, 0, Cp_ * ldR, 1, 0, 0, P,
-        nb * Rp * ldC, nb * Cp_ * ldR, stream()), "cf_build_block_planes")
+    for flags in (1, 2):  # Dba (coalesced rows of fb), then Dab by the transposed walk
+        check(E.lib.cf_build_block_planes(
+            blk.kind, mode, fa.npix, va.data_ptr(), fb.npix, vb.data_ptr(), L.lmax_signal, t0, None, None,
+            bins, Dba.data_ptr(), ldC, 0, 0, Rp * ldC, Dab.data_ptr(), ldR, 0, 0, Cp_ * ldR, 1, 0, 0, P,
+            nb * Rp * ldC, nb * Cp_ * ldR, flags, stream()), "cf_build_block_planes")
     # output columns in fa: K over fb with B[b][j in fa][k in fb] = Dab;
     # output columns in fb: K over fa with B[b][j in fb][k in fa] = Dba
     return blk, {blk.fa: (Dab, R, blk.fb), blk.fb: (Dba, Cc, blk.fa)}
 
 
 def fisher(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6") -> torch.Tensor:
+    """F (P x P, FP64) on the tensor cores (see _fisher_core)."""
+    return _fisher_core(E, Cinv, scheme)[0]
+
+
+def _fisher_core(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6", N=None, maps=None):
     """F (P x P, FP64) with the A_b GEMMs and traces on the tensor cores.
 
     A_b is kept for every parameter in one buffer per column segment (field):
@@ -171,19 +187,19 @@ def fisher(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6") -> torch.Tenso
         blk, ops = _build_planes(plan, s)
         E._probe_end("build_planes", ev, 0)
         for seg, (B, K, kseg) in ops.items():
-            N = nb * segpad[seg]
-            col0 = seg_specs[seg].index(s) * N
+            ncol = nb * segpad[seg]
+            col0 = seg_specs[seg].index(s) * ncol
             Xs, XTs = X[seg], XT[seg]
             ev = E._probe_begin("a_gemm_mixed")
             torch.cuda.nvtx.range_push("a_gemm_mixed")
             check(E.lib.cf_umma_gemm_bf16(
-                npd, N, K, plan.nterms, plan.ta, plan.tb, _off(Cp, plan.po[kseg]), npd, npd * npd, Pl,
+                npd, ncol, K, plan.nterms, plan.ta, plan.tb, _off(Cp, plan.po[kseg]), npd, npd * npd, Pl,
                 B.data_ptr(), B.shape[2], B.shape[1] * B.shape[2], Pl,
                 _off(Xs, col0), ldseg[seg], npd * ldseg[seg], Pl,
                 _off(XTs, col0 * npd), npd, XTs.shape[1] * npd, None, 0,
                 plan.err.data_ptr(), stream()), "cf_umma_gemm_bf16")
             torch.cuda.nvtx.range_pop()
-            E._probe_end("a_gemm_mixed", ev, 2.0 * npd * N * K * plan.nterms)
+            E._probe_end("a_gemm_mixed", ev, 2.0 * npd * ncol * K * plan.nterms)
         del ops
     F = torch.zeros((P, P), dtype=torch.float64, device=E.dev)
     for ss in X:
@@ -200,17 +216,71 @@ def fisher(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6") -> torch.Tenso
                 plan.err.data_ptr(), stream()), "cf_umma_trace_bf16_mapped")
             torch.cuda.nvtx.range_pop()
             E._probe_end("trace_mixed", ev, 2.0 * P1 * P2 * m_t * m_s * plan.nterms)
-    del X, XT
+    del XT
+    qml = None
+    if N is not None or maps is not None:
+        qml = _qml_core(plan, E, Cinv, Cp, N, maps, X, pmap, ldseg, segrows, segpad)
+    del X
     if int(plan.err.item()) != 0:
         raise RuntimeError("tensor-core kernel reported a timed-out wait")
-    return F
+    return F, qml
+
+
+def _qml_core(plan, E, Cinv, Cp, N, maps, X, pmap, ldseg, segrows, segpad):
+    """Noise bias and quadratic forms as contractions of the resident A_b slabs.
+
+    b_p = 1/2 Tr(C^-1 N C^-1 dC_p) = 1/2 sum_kl A_p[k,l] G[k,l], G = N C^-1;
+    q_p = 1/2 y^T dC_p y = 1/2 sum_kl A_p[k,l] x_k y_l, y = C^-1 x
+    (qube/spectra.py:1124-1186).  G comes from the split-product GEMM, the
+    outer products x y^T are split into planes, and one contraction per
+    segment pair reads every A_b slab once.
+    """
+    L = E.L
+    npd, Pl, P = plan.n_pad, plan.planes, L.n_params
+    nsims = 0 if maps is None else maps.shape[1]
+    Q = 1 + nsims
+    ev = E._probe_begin("qml_mixed")
+    stack = torch.empty((Pl, Q, npd, npd), dtype=BF16, device=E.dev)
+    if N is not None:
+        Np = plan.split_cinv(N)
+        check(E.lib.cf_umma_gemm_bf16(
+            npd, npd, npd, plan.nterms, plan.ta, plan.tb, Np.data_ptr(), npd, npd * npd, Pl,
+            Cp.data_ptr(), npd, npd * npd, Pl, stack.data_ptr(), npd, Q * npd * npd, Pl, None, 0, 0, None, 0,
+            plan.err.data_ptr(), stream()), "cf_umma_gemm_bf16")
+        del Np
+    else:
+        stack[:, 0].zero_()
+    bias = q = None
+    if nsims:
+        Xm = maps.to(E.dev, torch.float64).contiguous()
+        Ym = E.gemm(Cinv, Xm)
+        xp, yp = plan.pad_rows(Xm), plan.pad_rows(Ym)
+        check(E.lib.cf_outer_planes(npd, nsims, xp.data_ptr(), yp.data_ptr(), nsims, Pl,
+                                    _off(stack, npd * npd), npd, npd * npd, Q * npd * npd, stream()),
+              "cf_outer_planes")
+    R = torch.zeros((P, Q), dtype=torch.float64, device=E.dev)
+    cmap = torch.arange(Q, dtype=torch.int32, device=E.dev)
+    for ss in X:
+        for tt in plan.segments:
+            check(E.lib.cf_umma_trace_bf16_mapped(
+                pmap[ss].numel(), Q, segrows[tt], segrows[ss], plan.nterms, plan.ta, plan.tb,
+                _off(X[ss], plan.po[tt] * ldseg[ss]), segpad[ss], ldseg[ss], npd * ldseg[ss], Pl,
+                _off(stack, plan.po[tt] * npd + plan.po[ss]), npd * npd, npd, Q * npd * npd, Pl,
+                0.5, R.data_ptr(), Q, pmap[ss].data_ptr(), cmap.data_ptr(), 0,
+                plan.err.data_ptr(), stream()), "cf_umma_trace_bf16_mapped")
+    if N is not None:
+        bias = R[:, 0].contiguous()
+    if nsims:
+        q = R[:, 1:].T.contiguous()
+    E._probe_end("qml_mixed", ev, 0)
+    return bias, q
 
 
 def fisher_qml(E: Engine, Cinv: torch.Tensor, N: torch.Tensor | None = None,
                maps: torch.Tensor | None = None, scheme: str = "bf16x6"):
     """Mixed F, FP64 bias and q (same return convention as Engine.fisher_qml)."""
-    F = fisher(E, Cinv, scheme)
-    ev = E._probe_begin("qml_fp64")
-    _, bias, q = E.fisher_qml(Cinv, N, maps, want_fisher=False)
-    E._probe_end("qml_fp64", ev, 0)
+    F, qml = _fisher_core(E, Cinv, scheme, N, maps)
+    bias, q = qml if qml is not None else (None, None)
+    if q is not None and N is None:
+        bias = None
     return F, bias, q

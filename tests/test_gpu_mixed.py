@@ -65,4 +65,37 @@ def test_mixed_fisher_matches_fp64(name, drop, scheme):
     Finv_m = np.linalg.inv(Fm)
     sig = np.sqrt(np.diag(Finv))
     q = np.random.default_rng(0).standard_normal(F64.shape[0]) @ np.linalg.cholesky(F64).T
-    assert np.max(np.abs(q @ Finv_m - q @ Finv) / sig) < 1e-3
+    assert np.max(np.abs(q @ Finv_m - q @ Finv) / sig) < (1e-3 if scheme == "bf16x6" else 1e-2)
+
+
+# |dC_hat| / sigma bound per case.  The full-sky nside-4 TQU fixture is nearly
+# noiseless (N = 0.013 / 1.3e-4 muK^2) with an ill-conditioned Fisher matrix;
+# 24-bit products leave ~3e-2 sigma there, which is why the plain FP64 path
+# stays available for such problems.
+QML_SIGMA_TOL = {"tqu_cut_nside4": 1e-3, "config0_tt_nside8": 1e-3, "nside4_TQU": 5e-2}
+
+
+@pytest.mark.parametrize("name", sorted(QML_SIGMA_TOL))
+def test_mixed_qml_matches_fp64(name):
+    """Noise bias, raw q and C_hat of the BF16x6 path against plain FP64."""
+    from cosmoforge_b200 import engine, engine_mixed
+
+    d, p, mask, N, maps = _case(name)
+    L = build_layout(p, mask, d["beam"])
+    E = engine.Engine(L)
+    Nd = torch.from_numpy(N).cuda()
+    X = torch.from_numpy(maps).cuda()
+    S = E.signal(L.smoothed_cl_table(cls_of(d)))
+    Cinv = E.spd_inverse(S + Nd)
+    F64, b64, q64 = E.fisher_qml(Cinv, Nd, X)
+    Fm, bm, qm = engine_mixed.fisher_qml(E, Cinv, Nd, X, scheme="bf16x6")
+    F64, b64, q64 = F64.cpu().numpy(), b64.cpu().numpy(), q64.cpu().numpy()
+    Fm, bm, qm = Fm.cpu().numpy(), bm.cpu().numpy(), qm.cpu().numpy()
+    assert np.max(np.abs(bm - b64)) / np.max(np.abs(b64)) < 1e-5
+    assert np.max(np.abs(qm - q64)) / np.max(np.abs(q64)) < 1e-5
+    Finv = np.linalg.inv(F64)
+    sig = np.sqrt(np.diag(Finv))
+    c64 = (q64 - b64) @ Finv
+    cm = (qm - bm) @ np.linalg.inv(Fm)
+    print(f"{name}: |dC_hat|/sigma {np.max(np.abs(cm - c64) / sig):.2e}")
+    assert np.max(np.abs(cm - c64) / sig) < QML_SIGMA_TOL[name]
