@@ -181,7 +181,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 
-template <int BN, int STAGES, bool TRACE, int KC>
+template <int BN, int STAGES, bool TRACE, int KC, int PLS>
 __global__ void __launch_bounds__(NTHREADS, 1)
     k_umma_gemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int K,
                 int n_split, Terms terms, EpiArgs epi, TraceArgs tr, int* err)
@@ -195,15 +195,19 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     // traces), so no FP32 tensor-core accumulator sees more than 4 KC steps.
     // Two epilogue warps share each TMEM lane quadrant, each owning half of the
     // BN columns.
+    // PLS > 1: one pipeline stage holds planes 0..PLS-1 of both operands' k-tile
+    // and the MMA thread issues every product term from it (each plane is read
+    // from memory once); PLS == 1: terms are walked one after the other.
     using AccT = typename std::conditional<TRACE, double, float>::type;
     constexpr int HALF = BN / 2;
     constexpr uint32_t A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2;
+    constexpr uint32_t A_STAGE = PLS * A_BYTES, B_STAGE = PLS * B_BYTES;
     constexpr uint32_t TMEM_COLS = 2 * BN <= 64 ? 64 : (2 * BN <= 128 ? 128 : (2 * BN <= 256 ? 256 : 512));
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint8_t* sA = smem;
-    uint8_t* sB = smem + STAGES * A_BYTES;
-    uint64_t* full = (uint64_t*)(sB + STAGES * B_BYTES);
+    uint8_t* sB = smem + STAGES * A_STAGE;
+    uint64_t* full = (uint64_t*)(sB + STAGES * B_STAGE);
     uint64_t* empty = full + STAGES;
     uint64_t* accf = empty + STAGES;  // [2] accumulator ready
     uint64_t* acce = accf + 2;        // [2] accumulator drained
@@ -257,7 +261,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 int m0, n0, kt;
                 long t_lo;
                 coords(tile, m0, n0, t_lo, kt);
-                const int iters = terms.n * kt;
+                const int iters = PLS > 1 ? kt : terms.n * kt;
                 for (int it = 0; it < iters; ++it, ++g) {
                     const int s = (int)(g % STAGES);
                     const long r = g / STAGES;
@@ -265,17 +269,23 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         stop = true;
                         break;
                     }
-                    const int t = it / kt;
-                    const long ktile = t_lo + it % kt;
-                    mbar_expect_tx(&full[s], A_BYTES + B_BYTES);
-                    if (TRACE) {
-                        const int k = (int)(ktile / nl), l0 = (int)(ktile % nl) * BK;
-                        tma_load_4d(&mapA, &full[s], sA + s * A_BYTES, l0, k, m0, terms.a[t]);
-                        tma_load_4d(&mapB, &full[s], sB + s * B_BYTES, l0, k, n0, terms.b[t]);
-                    } else {
-                        const int kk = (int)ktile * BK;
-                        tma_load_3d(&mapA, &full[s], sA + s * A_BYTES, kk, m0, terms.a[t]);
-                        tma_load_3d(&mapB, &full[s], sB + s * B_BYTES, kk, n0, terms.b[t]);
+                    const int t = PLS > 1 ? 0 : it / kt;
+                    const long ktile = t_lo + (PLS > 1 ? it : it % kt);
+                    mbar_expect_tx(&full[s], A_STAGE + B_STAGE);
+#pragma unroll
+                    for (int pl = 0; pl < PLS; ++pl) {
+                        const int pa = PLS > 1 ? pl : terms.a[t], pb = PLS > 1 ? pl : terms.b[t];
+                        uint8_t* da = sA + s * A_STAGE + pl * A_BYTES;
+                        uint8_t* db = sB + s * B_STAGE + pl * B_BYTES;
+                        if (TRACE) {
+                            const int k = (int)(ktile / nl), l0 = (int)(ktile % nl) * BK;
+                            tma_load_4d(&mapA, &full[s], da, l0, k, m0, pa);
+                            tma_load_4d(&mapB, &full[s], db, l0, k, n0, pb);
+                        } else {
+                            const int kk = (int)ktile * BK;
+                            tma_load_3d(&mapA, &full[s], da, kk, m0, pa);
+                            tma_load_3d(&mapB, &full[s], db, kk, n0, pb);
+                        }
                     }
                 }
             }
@@ -292,7 +302,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 int m0, n0, kt;
                 long t_lo;
                 coords(tile, m0, n0, t_lo, kt);
-                const int iters = terms.n * kt;
+                const int iters = PLS > 1 ? kt : terms.n * kt;
                 int buf = 0;
                 for (int it = 0; it < iters; ++it, ++g) {
                     const bool first = (it % KC) == 0;
@@ -310,12 +320,17 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         break;
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-                    const uint64_t ad = smem_desc(sA + s * A_BYTES), bd = smem_desc(sB + s * B_BYTES);
                     const uint32_t dst = tmem + (uint32_t)(buf * BN);
+                    const int nt = PLS > 1 ? terms.n : 1;
+                    for (int t = 0; t < nt; ++t) {
+                        const int pa = PLS > 1 ? terms.a[t] : 0, pb = PLS > 1 ? terms.b[t] : 0;
+                        const uint64_t ad = smem_desc(sA + s * A_STAGE + pa * A_BYTES);
+                        const uint64_t bd = smem_desc(sB + s * B_STAGE + pb * B_BYTES);
 #pragma unroll
-                    for (int k = 0; k < BK / 16; ++k)  // 16 BF16 = 32 B per MMA; advance the start address
-                        umma_bf16(dst, ad + (uint64_t)((k * 32) >> 4), bd + (uint64_t)((k * 32) >> 4), idesc,
-                                  (first && k == 0) ? 0u : 1u);
+                        for (int k = 0; k < BK / 16; ++k)  // 16 BF16 = 32 B per MMA; advance the start address
+                            umma_bf16(dst, ad + (uint64_t)((k * 32) >> 4), bd + (uint64_t)((k * 32) >> 4), idesc,
+                                      (first && t == 0 && k == 0) ? 0u : 1u);
+                    }
                     umma_commit(&empty[s]);
                     if ((it % KC) == KC - 1 || it == iters - 1) {
                         umma_commit(&accf[buf]);
@@ -339,7 +354,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             int m0, n0, kt;
             long t_lo;
             coords(tile, m0, n0, t_lo, kt);
-            const int iters = terms.n * kt;
+            const int iters = PLS > 1 ? kt : terms.n * kt;
             const int nchunks = (iters + KC - 1) / KC;
             AccT acc[HALF];
 #pragma unroll
@@ -485,14 +500,14 @@ int make_map4(CUtensorMap* map, const void* base, long K2, long K1, long rows, i
     return r == CUDA_SUCCESS ? CF_OK : CF_ERR_ARG;
 }
 
-template <int BN, int STAGES, bool TRACE, int KC>
+template <int BN, int STAGES, bool TRACE, int KC, int PLS = 1>
 int launch_gemm_kc(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, int K, const Terms& t,
                    const EpiArgs& e, const TraceArgs& tr, int splits, int* err, cudaStream_t st)
 {
-    const size_t smem = 1024 + (size_t)STAGES * (BM * BK * 2 + BN * BK * 2) + 256;
+    const size_t smem = 1024 + (size_t)STAGES * PLS * (BM * BK * 2 + BN * BK * 2) + 256;
     static bool attr = false;
     if (!attr) {
-        CF_CHECK(cudaFuncSetAttribute(k_umma_gemm<BN, STAGES, TRACE, KC>,
+        CF_CHECK(cudaFuncSetAttribute(k_umma_gemm<BN, STAGES, TRACE, KC, PLS>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
@@ -501,7 +516,7 @@ int launch_gemm_kc(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, i
     CF_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const long tiles = (long)cf_cdiv(M, BM) * cf_cdiv(N, BN) * splits;
     const int grid = (int)(tiles < sms ? tiles : sms);
-    k_umma_gemm<BN, STAGES, TRACE, KC><<<grid, NTHREADS, smem, st>>>(ma, mb, K, splits, t, e, tr, err);
+    k_umma_gemm<BN, STAGES, TRACE, KC, PLS><<<grid, NTHREADS, smem, st>>>(ma, mb, K, splits, t, e, tr, err);
     CF_CHECK_LAUNCH();
     return CF_OK;
 }
@@ -577,8 +592,8 @@ extern "C" int cf_umma_gemm_bf16(int M, int N, int K, int nterms, const int* ta,
 extern "C" int cf_umma_trace_bf16_mapped(int P1, int P2, int K1, int K2, int nterms, const int* ta,
                                          const int* tb, const void* X, long sXp, long ldX, long x_ps, int x_planes,
                                          const void* Y, long sYq, long ldY, long y_ps, int y_planes, double scale,
-                                         double* F, long ldF, const int* row_map, const int* col_map, int splits,
-                                         int* err, void* stream);
+                                         double* F, long ldF, const int* row_map, const int* col_map, int sym,
+                                         int splits, int* err, void* stream);
 
 extern "C" int cf_umma_trace_bf16(int P1, int P2, int K1, int K2, int nterms, const int* ta, const int* tb,
                                   const void* X, long sXp, long ldX, long x_ps, int x_planes, const void* Y,
@@ -590,16 +605,16 @@ extern "C" int cf_umma_trace_bf16(int P1, int P2, int K1, int K2, int nterms, co
 }
 
 // As cf_umma_trace_bf16, with output row p going to F row row_map[p] and column
-// q to F column col_map[q] (device int arrays); no mirror entry.
+// q to F column col_map[q] (device int arrays), and the mirror entry too when sym.
 extern "C" int cf_umma_trace_bf16_mapped(int P1, int P2, int K1, int K2, int nterms, const int* ta,
                                          const int* tb, const void* X, long sXp, long ldX, long x_ps, int x_planes,
                                          const void* Y, long sYq, long ldY, long y_ps, int y_planes, double scale,
-                                         double* F, long ldF, const int* row_map, const int* col_map, int splits,
-                                         int* err, void* stream)
+                                         double* F, long ldF, const int* row_map, const int* col_map, int sym,
+                                         int splits, int* err, void* stream)
 {
     if (!row_map || !col_map) return CF_ERR_ARG;
     return cf_umma_trace_impl(P1, P2, K1, K2, nterms, ta, tb, X, sXp, ldX, x_ps, x_planes, Y, sYq, ldY, y_ps,
-                              y_planes, scale, F, ldF, 0, 0, 0, row_map, col_map, splits, err, stream);
+                              y_planes, scale, F, ldF, 0, 0, sym, row_map, col_map, splits, err, stream);
 }
 
 int cf_umma_trace_impl(int P1, int P2, int K1, int K2, int nterms, const int* ta, const int* tb, const void* X,
@@ -631,6 +646,14 @@ int cf_umma_trace_impl(int P1, int P2, int K1, int K2, int nterms, const int* ta
     e.N = P2;
     TraceArgs tr{K1, K2, F, ldF, p_off, q_off, sym, scale, row_map, col_map};
     cudaStream_t st = (cudaStream_t)stream;
-    if (narrow) return launch_gemm<64, 8, true>(ma, mb, P1, P2, 0, t, e, tr, splits, err, st);
+    // every plane of a k-tile in one stage when both operands carry the same planes
+    const int pls = (x_planes == y_planes) ? x_planes : 1;
+    if (narrow) {
+        if (pls == 3) return launch_gemm_kc<64, 3, true, 4, 3>(ma, mb, P1, P2, 0, t, e, tr, splits, err, st);
+        if (pls == 2) return launch_gemm_kc<64, 4, true, 4, 2>(ma, mb, P1, P2, 0, t, e, tr, splits, err, st);
+        return launch_gemm<64, 8, true>(ma, mb, P1, P2, 0, t, e, tr, splits, err, st);
+    }
+    if (pls == 3) return launch_gemm_kc<128, 2, true, 4, 3>(ma, mb, P1, P2, 0, t, e, tr, splits, err, st);
+    if (pls == 2) return launch_gemm_kc<128, 3, true, 4, 2>(ma, mb, P1, P2, 0, t, e, tr, splits, err, st);
     return launch_gemm<128, 6, true>(ma, mb, P1, P2, 0, t, e, tr, splits, err, st);
 }

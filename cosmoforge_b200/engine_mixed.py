@@ -202,8 +202,10 @@ def _fisher_core(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6", N=None, 
             E._probe_end("a_gemm_mixed", ev, 2.0 * npd * ncol * K * plan.nterms)
         del ops
     F = torch.zeros((P, P), dtype=torch.float64, device=E.dev)
-    for ss in X:
-        for tt in X:
+    segs = list(X)
+    for a, ss in enumerate(segs):
+        # (s, t) and (t, s) give transposed blocks of F: compute s <= t, mirror s < t
+        for tt in segs[a:]:
             P1, P2 = pmap[ss].numel(), pmap[tt].numel()
             m_s, m_t = segrows[ss], segrows[tt]
             ev = E._probe_begin("trace_mixed")
@@ -212,7 +214,7 @@ def _fisher_core(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6", N=None, 
                 P1, P2, m_t, m_s, plan.nterms, plan.ta, plan.tb,
                 _off(X[ss], plan.po[tt] * ldseg[ss]), segpad[ss], ldseg[ss], npd * ldseg[ss], Pl,
                 _off(XT[tt], plan.po[ss]), segpad[tt] * npd, npd, XT[tt].shape[1] * npd, Pl,
-                0.5, F.data_ptr(), P, pmap[ss].data_ptr(), pmap[tt].data_ptr(), 0,
+                0.5, F.data_ptr(), P, pmap[ss].data_ptr(), pmap[tt].data_ptr(), int(ss != tt), 0,
                 plan.err.data_ptr(), stream()), "cf_umma_trace_bf16_mapped")
             torch.cuda.nvtx.range_pop()
             E._probe_end("trace_mixed", ev, 2.0 * P1 * P2 * m_t * m_s * plan.nterms)
@@ -266,7 +268,7 @@ def _qml_core(plan, E, Cinv, Cp, N, maps, X, pmap, ldseg, segrows, segpad):
                 pmap[ss].numel(), Q, segrows[tt], segrows[ss], plan.nterms, plan.ta, plan.tb,
                 _off(X[ss], plan.po[tt] * ldseg[ss]), segpad[ss], ldseg[ss], npd * ldseg[ss], Pl,
                 _off(stack, plan.po[tt] * npd + plan.po[ss]), npd * npd, npd, Q * npd * npd, Pl,
-                0.5, R.data_ptr(), Q, pmap[ss].data_ptr(), cmap.data_ptr(), 0,
+                0.5, R.data_ptr(), Q, pmap[ss].data_ptr(), cmap.data_ptr(), 0, 0,
                 plan.err.data_ptr(), stream()), "cf_umma_trace_bf16_mapped")
     if N is not None:
         bias = R[:, 0].contiguous()
