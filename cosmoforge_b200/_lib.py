@@ -31,8 +31,9 @@ SIGNATURES = {
                                    _l, _l, _l, _l, _i, _l, _l, _i, _l, _l, _i, _p]),
     "cf_dgemm": (_i, [_i, _i, _i, _i, _i, _d, _p, _l, _l, _p, _l, _l, _d, _p, _l, _l, _p, _l, _l,
                       _i, _i, _p]),
-    "cf_potrf": (_i, [_i, _p, _l, _l, _i, _p, _p]),
-    "cf_trtri_lower": (_i, [_i, _p, _l, _l, _p, _l, _l, _i, _p]),
+    "cf_potrf_workspace": (_sz, [_i, _i]),
+    "cf_potrf": (_i, [_i, _p, _l, _l, _i, _p, _p, _p]),
+    "cf_trtri_lower": (_i, [_i, _p, _l, _l, _p, _l, _l, _i, _p, _p]),
     "cf_spd_inverse_workspace": (_sz, [_i, _i]),
     "cf_spd_inverse": (_i, [_i, _p, _l, _l, _i, _p, _p, _p]),
     "cf_spd_inverse_static_max_n": (_i, []),

@@ -23,12 +23,20 @@ namespace {
 constexpr int NB = 64;
 constexpr int LDS = NB + 1;
 
-// Factor the kb x kb diagonal block at (k0, k0) of each batch matrix in place.
-__global__ void __launch_bounds__(256) k_potrf_diag(double* A, long lda, long sA, int k0, int kb, int* info)
+// Factor the kb x kb diagonal block at (k0, k0) of each batch matrix in place
+// (right-looking, one barrier per column: the scaling of column j is folded
+// into step j + 1) and write L11^-1 to Dinv (kb x kb, row-major, lower).
+__global__ void __launch_bounds__(256) k_potrf_diag_inv(double* A, long lda, long sA, int k0, int kb, double* Dinv,
+                                                        long sD, int* info)
 {
-    __shared__ double S[NB * LDS];
+    extern __shared__ double dsm[];
+    double* S = dsm;             // the block, then L11
+    double* Xs = dsm + NB * LDS;  // L11^-1
+    __shared__ double piv[NB];
     __shared__ int bad;
-    A += blockIdx.x * sA;
+    const int b = blockIdx.x;
+    A += b * sA;
+    Dinv += b * sD;
     const int tid = threadIdx.x;
     for (int e = tid; e < kb * kb; e += blockDim.x) {
         int r = e / kb, c = e % kb;
@@ -37,95 +45,63 @@ __global__ void __launch_bounds__(256) k_potrf_diag(double* A, long lda, long sA
     if (tid == 0) bad = 0;
     __syncthreads();
     for (int j = 0; j < kb; ++j) {
-        if (tid == 0) {
-            double d = S[j * LDS + j];
-            if (!(d > 0.0)) {  // also catches NaN
-                if (!bad) bad = k0 + j + 1;
-                d = 1.0;
-            }
-            S[j * LDS + j] = sqrt(d);
+        double d = S[j * LDS + j];
+        if (!(d > 0.0)) {  // also catches NaN
+            if (tid == 0 && !bad) bad = k0 + j + 1;
+            d = 1.0;
         }
-        __syncthreads();
-        const double piv = S[j * LDS + j];
-        for (int r = j + 1 + tid; r < kb; r += blockDim.x) S[r * LDS + j] /= piv;
-        __syncthreads();
+        if (tid == 0) piv[j] = sqrt(d);
+        const double inv_d = 1.0 / d;
+        // trailing update with the unscaled column j; column j - 1 gets its scaling now
         const int m = kb - j - 1;
-        for (int e = tid; e < m * m; e += blockDim.x) {
-            int r = j + 1 + e / m, c = j + 1 + e % m;
-            if (c <= r) S[r * LDS + c] -= S[r * LDS + j] * S[c * LDS + j];
+        for (int e = tid; e < m * (m + 1) / 2; e += blockDim.x) {
+            int r = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
+            while ((r + 1) * (r + 2) / 2 <= e) ++r;
+            while (r * (r + 1) / 2 > e) --r;
+            const int c = e - r * (r + 1) / 2;
+            const int rr = j + 1 + r, cc = j + 1 + c;
+            S[rr * LDS + cc] -= S[rr * LDS + j] * S[cc * LDS + j] * inv_d;
         }
+        if (j > 0)
+            for (int r = j + tid; r < kb; r += blockDim.x) S[r * LDS + j - 1] /= piv[j - 1];
         __syncthreads();
     }
+    for (int r = kb - 1 + tid; r < kb; r += blockDim.x) S[r * LDS + kb - 1] /= piv[kb - 1];
+    for (int r = tid; r < kb; r += blockDim.x) S[r * LDS + r] = piv[r];
+    __syncthreads();
     for (int e = tid; e < kb * kb; e += blockDim.x) {
         int r = e / kb, c = e % kb;
         A[(long)(k0 + r) * lda + k0 + c] = (c <= r) ? S[r * LDS + c] : 0.0;
     }
-    if (tid == 0 && bad && info && info[blockIdx.x] == 0) info[blockIdx.x] = bad;
-}
-
-// Panel below the diagonal block: A21 <- A21 L11^-T (one thread per row).
-__global__ void __launch_bounds__(NB) k_trsm_panel(double* A, long lda, long sA, int k0, int kb, int n)
-{
-    extern __shared__ double dsm[];
-    double* Ls = dsm;
-    double* Xs = dsm + NB * LDS;
-    A += blockIdx.y * sA;
-    const int tid = threadIdx.x;
-    const int r0 = k0 + kb + blockIdx.x * NB;
-    for (int e = tid; e < kb * kb; e += NB) {
-        int r = e / kb, c = e % kb;
-        Ls[r * LDS + c] = A[(long)(k0 + r) * lda + k0 + c];
-    }
-    for (int e = tid; e < NB * kb; e += NB) {
-        int r = e / kb, c = e % kb;
-        Xs[r * LDS + c] = (r0 + r < n) ? A[(long)(r0 + r) * lda + k0 + c] : 0.0;
-    }
-    __syncthreads();
-    if (r0 + tid < n) {
-        double* x = Xs + tid * LDS;
-        for (int c = 0; c < kb; ++c) {
-            double s = x[c];
-            for (int t = 0; t < c; ++t) s -= x[t] * Ls[c * LDS + t];
-            x[c] = s / Ls[c * LDS + c];
+    // L11^-1 by forward substitution in shared memory, one thread per column
+    if (tid < kb) {
+        const int c = tid;
+        for (int r = 0; r < kb; ++r) {
+            double x = 0.0;
+            if (r >= c) {
+                double acc = (r == c) ? 1.0 : 0.0;
+                for (int t = c; t < r; ++t) acc -= S[r * LDS + t] * Xs[t * LDS + c];
+                x = acc / S[r * LDS + r];
+            }
+            Xs[r * LDS + c] = x;
         }
     }
     __syncthreads();
-    for (int e = tid; e < NB * kb; e += NB) {
+    for (int e = tid; e < kb * kb; e += blockDim.x) {
         int r = e / kb, c = e % kb;
-        if (r0 + r < n) A[(long)(r0 + r) * lda + k0 + c] = Xs[r * LDS + c];
+        Dinv[r * kb + c] = Xs[r * LDS + c];
     }
+    if (tid == 0 && bad && info && info[b] == 0) info[b] = bad;
 }
 
-// In place Y[k0:k0+kb, 0:ncols] <- L11^-1 Y[k0:k0+kb, 0:ncols] (one thread per column).
-__global__ void __launch_bounds__(NB) k_trsm_left(const double* L, long lda, long sL, int k0, int kb,
-                                                  double* Y, long ldy, long sY, int ncols)
+// Batched 2D copy: dst[r * ldd + c] = src[r * lds + c], r < R, c < C.
+__global__ void k_copy2d(int R, int C, const double* src, long lds, long ss, double* dst, long ldd, long sd)
 {
-    extern __shared__ double dsm[];
-    double* Ls = dsm;
-    double* Xs = dsm + NB * LDS;
-    L += blockIdx.y * sL;
-    Y += blockIdx.y * sY;
-    const int tid = threadIdx.x;
-    const int c0 = blockIdx.x * NB;
-    for (int e = tid; e < kb * kb; e += NB) {
-        int r = e / kb, c = e % kb;
-        Ls[r * LDS + c] = L[(long)(k0 + r) * lda + k0 + c];
-    }
-    for (int e = tid; e < kb * NB; e += NB) {
-        int r = e / NB, c = e % NB;
-        Xs[r * LDS + c] = (c0 + c < ncols) ? Y[(long)(k0 + r) * ldy + c0 + c] : 0.0;
-    }
-    __syncthreads();
-    for (int r = 0; r < kb; ++r) {
-        double s = Xs[r * LDS + tid];
-        for (int t = 0; t < r; ++t) s -= Ls[r * LDS + t] * Xs[t * LDS + tid];
-        Xs[r * LDS + tid] = s / Ls[r * LDS + r];
-    }
-    __syncthreads();
-    for (int e = tid; e < kb * NB; e += NB) {
-        int r = e / NB, c = e % NB;
-        if (c0 + c < ncols) Y[(long)(k0 + r) * ldy + c0 + c] = Xs[r * LDS + c];
-    }
+    src += blockIdx.z * ss;
+    dst += blockIdx.z * sd;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y * blockDim.y + threadIdx.y;
+    if (r < R && c < C) dst[(long)r * ldd + c] = src[(long)r * lds + c];
 }
 
 __global__ void k_diag_scale(const double* A, long lda, long sA, int n, double* d, long sd)
@@ -174,64 +150,84 @@ __global__ void k_unscale_mirror(double* A, long lda, long sA, int n, const doub
     }
 }
 
-constexpr size_t TRSM_SMEM = 2 * NB * LDS * sizeof(double);
-
-int set_trsm_attrs()
-{
-    static bool done = false;
-    if (!done) {
-        CF_CHECK(cudaFuncSetAttribute(k_trsm_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRSM_SMEM));
-        CF_CHECK(cudaFuncSetAttribute(k_trsm_left, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRSM_SMEM));
-        done = true;
-    }
-    return CF_OK;
-}
-
 }  // namespace
 
-extern "C" int cf_potrf(int n, double* A, long lda, long strideA, int batch, int* info, void* stream)
+namespace {
+inline int nblocks(int n) { return (n + NB - 1) / NB; }
+// doubles of potrf workspace per problem: every diagonal-block inverse + one panel
+inline size_t potrf_ws(int n) { return (size_t)nblocks(n) * NB * NB + (size_t)n * NB; }
+}  // namespace
+
+extern "C" size_t cf_potrf_workspace(int n, int batch) { return potrf_ws(n) * sizeof(double) * (size_t)batch; }
+
+// Right-looking blocked Cholesky: per 64-wide panel, the diagonal block is
+// factored (and inverted) by one CTA, the panel below is L21 = A21 L11^-T
+// (DMMA GEMM against the inverted block) and the trailing matrix gets
+// A22 -= L21 L21^T (lower-only DMMA GEMM).  `work` holds
+// cf_potrf_workspace(n, batch) bytes and keeps every L11^-1 for cf_trtri_lower.
+extern "C" int cf_potrf(int n, double* A, long lda, long strideA, int batch, void* work, int* info, void* stream)
 {
-    if (n <= 0 || batch < 1 || !A) return CF_ERR_ARG;
+    if (n <= 0 || batch < 1 || !A || !work) return CF_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
-    if (int rc = set_trsm_attrs()) return rc;
-    for (int k0 = 0; k0 < n; k0 += NB) {
+    constexpr size_t DIAG_SMEM = 2 * NB * LDS * sizeof(double);
+    static bool attr = false;
+    if (!attr) {
+        CF_CHECK(cudaFuncSetAttribute(k_potrf_diag_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DIAG_SMEM));
+        attr = true;
+    }
+    const long ws = (long)potrf_ws(n);
+    double* Dinv = (double*)work;                   // [batch][nblocks][NB][NB]
+    double* T = Dinv + (long)nblocks(n) * NB * NB;  // [batch][n][NB] (same stride ws)
+    for (int k0 = 0, blk = 0; k0 < n; k0 += NB, ++blk) {
         const int kb = n - k0 < NB ? n - k0 : NB;
-        k_potrf_diag<<<batch, 256, 0, st>>>(A, lda, strideA, k0, kb, info);
+        double* Di = Dinv + (long)blk * NB * NB;
+        k_potrf_diag_inv<<<batch, 256, DIAG_SMEM, st>>>(A, lda, strideA, k0, kb, Di, ws, info);
         CF_CHECK_LAUNCH();
         const int rest = n - k0 - kb;
         if (rest > 0) {
-            k_trsm_panel<<<dim3(cf_cdiv(rest, NB), batch), NB, TRSM_SMEM, st>>>(A, lda, strideA, k0, kb, n);
-            CF_CHECK_LAUNCH();
             double* a21 = A + (long)(k0 + kb) * lda + k0;
-            int rc = cf_dgemm(0, 1, rest, rest, kb, -1.0, a21, lda, strideA, a21, lda, strideA, 1.0,
-                              a21 + kb, lda, strideA, nullptr, 0, 0, batch, 1, stream);
+            int rc = cf_dgemm(0, 1, rest, kb, kb, 1.0, a21, lda, strideA, Di, kb, ws, 0.0, T, kb, ws, nullptr, 0,
+                              0, batch, 0, stream);
             if (rc) return rc;
+            rc = cf_dgemm(0, 1, rest, rest, kb, -1.0, T, kb, ws, T, kb, ws, 1.0, a21 + kb, lda, strideA, nullptr, 0,
+                          0, batch, 1, stream);
+            if (rc) return rc;
+            k_copy2d<<<dim3(cf_cdiv(kb, 32), cf_cdiv(rest, 8), batch), dim3(32, 8), 0, st>>>(rest, kb, T, kb, ws, a21,
+                                                                                            lda, strideA);
+            CF_CHECK_LAUNCH();
         }
     }
     return CF_OK;
 }
 
-// Y = L^-1 for a lower factor L (both n x n, row-major).
-extern "C" int cf_trtri_lower(int n, const double* L, long lda, long strideL, double* Y, long ldy,
-                              long strideY, int batch, void* stream)
+// Y = L^-1 for the lower factor of cf_potrf, using the diagonal-block
+// inverses it left in `work`: block row i becomes L_ii^-1 Y_i (DMMA GEMM),
+// then the rows below take Y_below -= L_below,i Y_i.
+extern "C" int cf_trtri_lower(int n, const double* L, long lda, long strideL, double* Y, long ldy, long strideY,
+                              int batch, void* work, void* stream)
 {
-    if (n <= 0 || batch < 1 || !L || !Y) return CF_ERR_ARG;
+    if (n <= 0 || batch < 1 || !L || !Y || !work) return CF_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
-    if (int rc = set_trsm_attrs()) return rc;
+    const long ws = (long)potrf_ws(n);
+    double* Dinv = (double*)work;
+    double* T = Dinv + (long)nblocks(n) * NB * NB;
     dim3 b2(32, 8);
     k_set_identity<<<dim3(cf_cdiv(n, 32), cf_cdiv(n, 8), batch), b2, 0, st>>>(Y, ldy, strideY, n);
     CF_CHECK_LAUNCH();
-    for (int k0 = 0; k0 < n; k0 += NB) {
+    for (int k0 = 0, blk = 0; k0 < n; k0 += NB, ++blk) {
         const int kb = n - k0 < NB ? n - k0 : NB;
         const int ncols = k0 + kb;
-        k_trsm_left<<<dim3(cf_cdiv(ncols, NB), batch), NB, TRSM_SMEM, st>>>(L, lda, strideL, k0, kb, Y, ldy,
-                                                                    strideY, ncols);
+        double* Yi = Y + (long)k0 * ldy;
+        int rc = cf_dgemm(0, 0, kb, ncols, kb, 1.0, Dinv + (long)blk * NB * NB, kb, ws, Yi, ldy, strideY, 0.0, T,
+                          ncols, ws, nullptr, 0, 0, batch, 0, stream);
+        if (rc) return rc;
+        k_copy2d<<<dim3(cf_cdiv(ncols, 32), cf_cdiv(kb, 8), batch), b2, 0, st>>>(kb, ncols, T, ncols, ws, Yi, ldy,
+                                                                                strideY);
         CF_CHECK_LAUNCH();
         const int rest = n - k0 - kb;
         if (rest > 0) {
-            int rc = cf_dgemm(0, 0, rest, ncols, kb, -1.0, L + (long)(k0 + kb) * lda + k0, lda,
-                              strideL, Y + (long)k0 * ldy, ldy, strideY, 1.0,
-                              Y + (long)(k0 + kb) * ldy, ldy, strideY, nullptr, 0, 0, batch, 0, stream);
+            rc = cf_dgemm(0, 0, rest, ncols, kb, -1.0, L + (long)(k0 + kb) * lda + k0, lda, strideL, Yi, ldy,
+                          strideY, 1.0, Y + (long)(k0 + kb) * ldy, ldy, strideY, nullptr, 0, 0, batch, 0, stream);
             if (rc) return rc;
         }
     }
@@ -240,7 +236,7 @@ extern "C" int cf_trtri_lower(int n, const double* L, long lda, long strideL, do
 
 extern "C" size_t cf_spd_inverse_workspace(int n, int batch)
 {
-    return ((size_t)n * n + (size_t)n) * sizeof(double) * (size_t)batch;
+    return ((size_t)n * n + (size_t)n + potrf_ws(n)) * sizeof(double) * (size_t)batch;
 }
 
 // In place inverse of symmetric positive-definite matrices (row-major,
@@ -255,18 +251,19 @@ extern "C" int cf_spd_inverse(int n, double* A, long lda, long strideA, int batc
     double* Y = (double*)work;
     const long sY = (long)n * n;
     double* d = Y + sY * batch;
+    double* pw = d + (long)n * batch;
     dim3 b2(32, 8);
     dim3 g2(cf_cdiv(n, 32), cf_cdiv(n, 8), batch);
     k_diag_scale<<<dim3(cf_cdiv(n, 256), batch), 256, 0, st>>>(A, lda, strideA, n, d, n);
     CF_CHECK_LAUNCH();
     k_scale_sym<<<g2, b2, 0, st>>>(A, lda, strideA, n, d, n, 1);
     CF_CHECK_LAUNCH();
-    int rc = cf_potrf(n, A, lda, strideA, batch, info, stream);
+    int rc = cf_potrf(n, A, lda, strideA, batch, pw, info, stream);
     if (rc) return rc;
-    rc = cf_trtri_lower(n, A, lda, strideA, Y, n, sY, batch, stream);
+    rc = cf_trtri_lower(n, A, lda, strideA, Y, n, sY, batch, pw, stream);
     if (rc) return rc;
-    rc = cf_dgemm(1, 0, n, n, n, 1.0, Y, n, sY, Y, n, sY, 0.0, A, lda, strideA, nullptr, 0, 0, batch, 1,
-                  stream);
+    // C^-1 = Y^T Y; Y is lower triangular, so (Y^T Y)[r, c] sums k >= max(r, c)
+    rc = cf_dgemm(1, 0, n, n, n, 1.0, Y, n, sY, Y, n, sY, 0.0, A, lda, strideA, nullptr, 0, 0, batch, 3, stream);
     if (rc) return rc;
     k_unscale_mirror<<<g2, b2, 0, st>>>(A, lda, strideA, n, d, n);
     CF_CHECK_LAUNCH();
@@ -278,12 +275,14 @@ extern "C" int cf_spd_inverse(int n, double* A, long lda, long strideA, int batc
 // device memory: code running inside a host callback or a custom allocator's
 // own hooks, plugins whose host forbids cudaMalloc after start-up, or
 // integrations that must not fragment a pool they do not own.  Its workspace
-// (L^-1 and the Jacobi scale factors) lives in this file-scope array, which
-// every GPU that loads the library holds until the process exits:
-// (1024^2 + 1024) doubles = 8.4 MB per device.
+// (L^-1, the Jacobi scale factors, the diagonal-block inverses and one panel)
+// lives in this file-scope array, which every GPU that loads the library holds
+// until the process exits: 1.18 M doubles = 9.4 MB per device.
 #define CF_SPD_STATIC_MAX_N 1024
 static __device__ __align__(256) double g_spd_static_scratch[(size_t)CF_SPD_STATIC_MAX_N * CF_SPD_STATIC_MAX_N +
-                                                             CF_SPD_STATIC_MAX_N];
+                                                             CF_SPD_STATIC_MAX_N +
+                                                             (size_t)((CF_SPD_STATIC_MAX_N + NB - 1) / NB) * NB * NB +
+                                                             (size_t)CF_SPD_STATIC_MAX_N * NB];
 
 namespace {
 constexpr int kMaxDevices = 64;

@@ -110,6 +110,9 @@ __global__ void __launch_bounds__(NT) k_dgemm(int M, int N, int K, double alpha,
         for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
     const int KT = (K + BK - 1) / BK;
+    // lower_only bit 1: op(A) = Y^T with Y lower triangular (Y^T Y), so the
+    // K sum of a tile starts at its first row
+    const int kt0 = (lower_only & 2) ? tile_m / BK : 0;
     auto issue = [&](int kt, int st) {
         if (kt < KT) {
             load_tile<A_KMN>(sAbuf + st * SA, A, lda, tile_m, kt * BK, M, K, tid);
@@ -117,14 +120,14 @@ __global__ void __launch_bounds__(NT) k_dgemm(int M, int N, int K, double alpha,
         }
         cp_commit();
     };
-    for (int s = 0; s < STAGES - 1; ++s) issue(s, s);
+    for (int s = 0; s < STAGES - 1; ++s) issue(kt0 + s, s);
 
-    for (int kt = 0; kt < KT; ++kt) {
+    for (int kt = kt0; kt < KT; ++kt) {
         cp_wait<STAGES - 2>();
         __syncthreads();
-        issue(kt + STAGES - 1, (kt + STAGES - 1) % STAGES);
-        const double* a_s = sAbuf + (kt % STAGES) * SA;
-        const double* b_s = sBbuf + (kt % STAGES) * SB;
+        issue(kt + STAGES - 1, (kt - kt0 + STAGES - 1) % STAGES);
+        const double* a_s = sAbuf + ((kt - kt0) % STAGES) * SA;
+        const double* b_s = sBbuf + ((kt - kt0) % STAGES) * SB;
 #pragma unroll
         for (int ks = 0; ks < BK; ks += 4) {
             double af[8], bf[4];

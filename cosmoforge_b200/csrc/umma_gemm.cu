@@ -131,16 +131,19 @@ __device__ __forceinline__ void tma_load_4d(const CUtensorMap* map, uint64_t* ba
         : "memory");
 }
 
-// Shared-memory matrix descriptor: K-major, 128B swizzle, 8-row atoms 1024 B apart.
+// Shared-memory matrix descriptor, K-major rows of BKT BF16: BKT = 64 is the
+// 128B swizzle (8-row atoms 1024 B apart), BKT = 32 the 64B swizzle (512 B).
+template <int BKT>
 __device__ __forceinline__ uint64_t smem_desc(const void* tile)
 {
+    static_assert(BKT == 64 || BKT == 32, "k-tile of 64 or 32 BF16");
     const uint64_t addr = smem_u32(tile);
     uint64_t d = 0;
-    d |= (addr >> 4) & 0x3FFFull;          // start address
-    d |= (uint64_t)(16 >> 4) << 16;        // leading byte offset (unused for swizzled K-major)
-    d |= (uint64_t)(1024 >> 4) << 32;      // stride byte offset: 8 rows x 128 B
-    d |= (uint64_t)1 << 46;                // descriptor version (sm100)
-    d |= (uint64_t)2 << 61;                // SWIZZLE_128B
+    d |= (addr >> 4) & 0x3FFFull;                  // start address
+    d |= (uint64_t)(16 >> 4) << 16;                // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)((8 * BKT * 2) >> 4) << 32;     // stride byte offset: 8 rows
+    d |= (uint64_t)1 << 46;                        // descriptor version (sm100)
+    d |= (uint64_t)(BKT == 64 ? 2 : 4) << 61;      // SWIZZLE_128B / SWIZZLE_64B
     return d;
 }
 
@@ -181,7 +184,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 
-template <int BN, int STAGES, bool TRACE, int KC, int PLS>
+template <int BN, int STAGES, bool TRACE, int KC, int PLS, int BKT, bool SPLIT>
 __global__ void __launch_bounds__(NTHREADS, 1)
     k_umma_gemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int K,
                 int n_split, Terms terms, EpiArgs epi, TraceArgs tr, int* err)
@@ -198,9 +201,17 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     // PLS > 1: one pipeline stage holds planes 0..PLS-1 of both operands' k-tile
     // and the MMA thread issues every product term from it (each plane is read
     // from memory once); PLS == 1: terms are walked one after the other.
+    // SPLIT (with PLS > 1, term 0 the leading product of planes (0, 0)): the two
+    // TMEM accumulators hold term 0 and the sum of the correction terms of the
+    // same chunk instead of alternating, so the small corrections are not added
+    // into the large leading sum inside the tensor core; the MMA thread waits
+    // for the epilogue to read both before it starts the next chunk.
     using AccT = typename std::conditional<TRACE, double, float>::type;
     constexpr int HALF = BN / 2;
-    constexpr uint32_t A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2;
+    constexpr uint32_t A_BYTES = BM * BKT * 2, B_BYTES = BN * BKT * 2;
+    // stages per promotion chunk: KC k-tiles of 64
+    constexpr int CH = PLS > 1 ? KC * (64 / BKT) : KC;
+    static_assert(!SPLIT || PLS > 1, "split accumulators need all planes per stage");
     constexpr uint32_t A_STAGE = PLS * A_BYTES, B_STAGE = PLS * B_BYTES;
     constexpr uint32_t TMEM_COLS = 2 * BN <= 64 ? 64 : (2 * BN <= 128 ? 128 : (2 * BN <= 256 ? 256 : 512));
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -218,8 +229,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int n_mt = (epi.M + BM - 1) / BM, n_nt = (epi.N + BN - 1) / BN;
     const long n_tiles = (long)n_mt * n_nt * n_split;
-    const int nl = TRACE ? (tr.K2 + BK - 1) / BK : 1;
-    const long kt_total = TRACE ? (long)tr.K1 * nl : (long)((K + BK - 1) / BK);
+    const int nl = TRACE ? (tr.K2 + BKT - 1) / BKT : 1;
+    const long kt_total = TRACE ? (long)tr.K1 * nl : (long)((K + BKT - 1) / BKT);
     auto coords = [&](long tile, int& m0, int& n0, long& t_lo, int& kt) {
         const int mt = (int)(tile % n_mt);
         const long rest = tile / n_mt;
@@ -269,8 +280,17 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         stop = true;
                         break;
                     }
-                    const int t = PLS > 1 ? 0 : it / kt;
-                    const long ktile = t_lo + (PLS > 1 ? it : it % kt);
+                    // windows of KC k-tiles, term by term inside a window: every
+                    // accumulator chunk holds one product term, and all terms reuse the
+                    // window's planes from L2
+                    int t = 0;
+                    long ktile = t_lo + it;
+                    if (PLS == 1) {
+                        const int w = it / (KC * terms.n), rem = it % (KC * terms.n);
+                        const int wlen = min(KC, kt - w * KC);
+                        t = rem / wlen;
+                        ktile = t_lo + (long)w * KC + rem % wlen;
+                    }
                     mbar_expect_tx(&full[s], A_STAGE + B_STAGE);
 #pragma unroll
                     for (int pl = 0; pl < PLS; ++pl) {
@@ -278,11 +298,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         uint8_t* da = sA + s * A_STAGE + pl * A_BYTES;
                         uint8_t* db = sB + s * B_STAGE + pl * B_BYTES;
                         if (TRACE) {
-                            const int k = (int)(ktile / nl), l0 = (int)(ktile % nl) * BK;
+                            const int k = (int)(ktile / nl), l0 = (int)(ktile % nl) * BKT;
                             tma_load_4d(&mapA, &full[s], da, l0, k, m0, pa);
                             tma_load_4d(&mapB, &full[s], db, l0, k, n0, pb);
                         } else {
-                            const int kk = (int)ktile * BK;
+                            const int kk = (int)ktile * BKT;
                             tma_load_3d(&mapA, &full[s], da, kk, m0, pa);
                             tma_load_3d(&mapB, &full[s], db, kk, n0, pb);
                         }
@@ -305,13 +325,28 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 const int iters = PLS > 1 ? kt : terms.n * kt;
                 int buf = 0;
                 for (int it = 0; it < iters; ++it, ++g) {
-                    const bool first = (it % KC) == 0;
+                    // chunk boundaries: every KC iterations (PLS > 1), or at the end of
+                    // each (window, term) run of min(KC, k-tiles left) iterations
+                    int pos = it % CH, clen = CH;
+                    if (PLS == 1) {
+                        const int w = it / (KC * terms.n), rem = it % (KC * terms.n);
+                        clen = min(KC, kt - w * KC);
+                        pos = rem % clen;
+                    }
+                    const bool first = pos == 0;
                     if (first) {
-                        buf = (int)(gc & 1);
-                        const long u = gc >> 1;
-                        if (u >= 1 && !mbar_wait(&acce[buf], (uint32_t)((u - 1) & 1), abort_flag)) {
-                            aborted = true;
-                            break;
+                        if (SPLIT) {  // both accumulators drained by the epilogue
+                            if (gc >= 1 && !mbar_wait(&acce[0], (uint32_t)((gc - 1) & 1), abort_flag)) {
+                                aborted = true;
+                                break;
+                            }
+                        } else {
+                            buf = (int)(gc & 1);
+                            const long u = gc >> 1;
+                            if (u >= 1 && !mbar_wait(&acce[buf], (uint32_t)((u - 1) & 1), abort_flag)) {
+                                aborted = true;
+                                break;
+                            }
                         }
                     }
                     const int s = (int)(g % STAGES);
@@ -320,20 +355,22 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         break;
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-                    const uint32_t dst = tmem + (uint32_t)(buf * BN);
                     const int nt = PLS > 1 ? terms.n : 1;
                     for (int t = 0; t < nt; ++t) {
                         const int pa = PLS > 1 ? terms.a[t] : 0, pb = PLS > 1 ? terms.b[t] : 0;
-                        const uint64_t ad = smem_desc(sA + s * A_STAGE + pa * A_BYTES);
-                        const uint64_t bd = smem_desc(sB + s * B_STAGE + pb * B_BYTES);
+                        const uint64_t ad = smem_desc<BKT>(sA + s * A_STAGE + pa * A_BYTES);
+                        const uint64_t bd = smem_desc<BKT>(sB + s * B_STAGE + pb * B_BYTES);
+                        // SPLIT: term 0 into columns [0, BN), the others into [BN, 2 BN)
+                        const uint32_t dst = tmem + (uint32_t)((SPLIT ? (t > 0) : buf) * BN);
+                        const bool fresh = first && (SPLIT ? t <= 1 : t == 0);
 #pragma unroll
-                        for (int k = 0; k < BK / 16; ++k)  // 16 BF16 = 32 B per MMA; advance the start address
+                        for (int k = 0; k < BKT / 16; ++k)  // 16 BF16 = 32 B per MMA; advance the start address
                             umma_bf16(dst, ad + (uint64_t)((k * 32) >> 4), bd + (uint64_t)((k * 32) >> 4), idesc,
-                                      (first && t == 0 && k == 0) ? 0u : 1u);
+                                      (fresh && k == 0) ? 0u : 1u);
                     }
                     umma_commit(&empty[s]);
-                    if ((it % KC) == KC - 1 || it == iters - 1) {
-                        umma_commit(&accf[buf]);
+                    if (pos == clen - 1 || it == iters - 1) {
+                        umma_commit(&accf[SPLIT ? 0 : buf]);
                         ++gc;
                     }
                 }
@@ -355,13 +392,14 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             long t_lo;
             coords(tile, m0, n0, t_lo, kt);
             const int iters = PLS > 1 ? kt : terms.n * kt;
-            const int nchunks = (iters + KC - 1) / KC;
+            const int nchunks = PLS > 1 ? (iters + CH - 1) / CH : ((kt + KC - 1) / KC) * terms.n;
             AccT acc[HALF];
 #pragma unroll
             for (int j = 0; j < HALF; ++j) acc[j] = AccT(0);
             for (int c = 0; c < nchunks; ++c, ++gc) {
-                const int buf = (int)(gc & 1);
-                if (!mbar_wait(&accf[buf], (uint32_t)((gc >> 1) & 1), abort_flag)) {
+                const int buf = SPLIT ? 0 : (int)(gc & 1);
+                const uint32_t par = SPLIT ? (uint32_t)(gc & 1) : (uint32_t)((gc >> 1) & 1);
+                if (!mbar_wait(&accf[buf], par, abort_flag)) {
                     ok = false;
                     break;
                 }
@@ -372,6 +410,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     tmem_ld32(lane_addr + (uint32_t)(buf * BN + gi * 32), v);
 #pragma unroll
                     for (int j = 0; j < 32; ++j) acc[gi * 32 + j] += (AccT)__uint_as_float(v[j]);
+                    if (SPLIT && terms.n > 1) {  // the correction terms' partial sum
+                        tmem_ld32(lane_addr + (uint32_t)(BN + gi * 32), v);
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) acc[gi * 32 + j] += (AccT)__uint_as_float(v[j]);
+                    }
                 }
                 asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
                 __syncwarp();
@@ -466,18 +509,20 @@ EncodeTiledFn encode_fn()
 }
 
 // 3D bf16 map: dims (K, rows, planes), row stride ld elements, plane stride ps elements;
-// box (64, box_rows, 1) with 128B swizzle.
-int make_map(CUtensorMap* map, const void* base, long K, long rows, long ld, int planes, long ps, int box_rows)
+// box (bk, box_rows, 1): bk = 64 with 128B swizzle, bk = 32 with 64B swizzle.
+int make_map(CUtensorMap* map, const void* base, long K, long rows, long ld, int planes, long ps, int box_rows,
+             int bk = BK)
 {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return CF_ERR_CUDA;
     if (((uintptr_t)base & 15) || (ld * 2) % 16 || (ps * 2) % 16) return CF_ERR_ARG;
     cuuint64_t dims[3] = {(cuuint64_t)K, (cuuint64_t)rows, (cuuint64_t)planes};
     cuuint64_t strides[2] = {(cuuint64_t)ld * 2, (cuuint64_t)(ps > 0 ? ps : ld * rows) * 2};
-    cuuint32_t box[3] = {(cuuint32_t)BK, (cuuint32_t)box_rows, 1};
+    cuuint32_t box[3] = {(cuuint32_t)bk, (cuuint32_t)box_rows, 1};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides, box, estr,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, bk == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? CF_OK : CF_ERR_ARG;
 }
@@ -500,14 +545,16 @@ int make_map4(CUtensorMap* map, const void* base, long K2, long K1, long rows, i
     return r == CUDA_SUCCESS ? CF_OK : CF_ERR_ARG;
 }
 
-template <int BN, int STAGES, bool TRACE, int KC, int PLS = 1>
+template <int BN, int STAGES, bool TRACE, int KC, int PLS = 1, int BKT = BK, bool SPLIT = false>
 int launch_gemm_kc(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, int K, const Terms& t,
                    const EpiArgs& e, const TraceArgs& tr, int splits, int* err, cudaStream_t st)
 {
-    const size_t smem = 1024 + (size_t)STAGES * PLS * (BM * BK * 2 + BN * BK * 2) + 256;
+    const size_t smem = 1024 + (size_t)STAGES * PLS * (BM * BKT * 2 + BN * BKT * 2) + 256;
+    static_assert(1024 + (size_t)STAGES * PLS * (BM * BKT * 2 + BN * BKT * 2) + 256 <= 232448,
+                  "shared memory ring exceeds 227 KB");
     static bool attr = false;
     if (!attr) {
-        CF_CHECK(cudaFuncSetAttribute(k_umma_gemm<BN, STAGES, TRACE, KC, PLS>,
+        CF_CHECK(cudaFuncSetAttribute(k_umma_gemm<BN, STAGES, TRACE, KC, PLS, BKT, SPLIT>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
@@ -516,7 +563,8 @@ int launch_gemm_kc(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, i
     CF_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const long tiles = (long)cf_cdiv(M, BM) * cf_cdiv(N, BN) * splits;
     const int grid = (int)(tiles < sms ? tiles : sms);
-    k_umma_gemm<BN, STAGES, TRACE, KC, PLS><<<grid, NTHREADS, smem, st>>>(ma, mb, K, splits, t, e, tr, err);
+    k_umma_gemm<BN, STAGES, TRACE, KC, PLS, BKT, SPLIT><<<grid, NTHREADS, smem, st>>>(ma, mb, K, splits, t, e, tr,
+                                                                                     err);
     CF_CHECK_LAUNCH();
     return CF_OK;
 }
@@ -524,16 +572,17 @@ int launch_gemm_kc(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, i
 // Promotion interval (k-tiles of 64 per FP32 accumulator): 1, 2, 4, 8 or 16.
 int g_promote_kc = 16;
 
-template <int BN, int STAGES, bool TRACE>
+template <int BN, int STAGES, bool TRACE, int PLS = 1, int BKT = BK, bool SPLIT = false>
 int launch_gemm(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, int K, const Terms& t,
                 const EpiArgs& e, const TraceArgs& tr, int splits, int* err, cudaStream_t st)
 {
     switch (g_promote_kc) {
-        case 1: return launch_gemm_kc<BN, STAGES, TRACE, 1>(ma, mb, M, N, K, t, e, tr, splits, err, st);
-        case 2: return launch_gemm_kc<BN, STAGES, TRACE, 2>(ma, mb, M, N, K, t, e, tr, splits, err, st);
-        case 8: return launch_gemm_kc<BN, STAGES, TRACE, 8>(ma, mb, M, N, K, t, e, tr, splits, err, st);
-        case 16: return launch_gemm_kc<BN, STAGES, TRACE, 16>(ma, mb, M, N, K, t, e, tr, splits, err, st);
-        default: return launch_gemm_kc<BN, STAGES, TRACE, 4>(ma, mb, M, N, K, t, e, tr, splits, err, st);
+        case 1: return launch_gemm_kc<BN, STAGES, TRACE, 1, PLS, BKT, SPLIT>(ma, mb, M, N, K, t, e, tr, splits, err, st);
+        case 2: return launch_gemm_kc<BN, STAGES, TRACE, 2, PLS, BKT, SPLIT>(ma, mb, M, N, K, t, e, tr, splits, err, st);
+        case 8: return launch_gemm_kc<BN, STAGES, TRACE, 8, PLS, BKT, SPLIT>(ma, mb, M, N, K, t, e, tr, splits, err, st);
+        case 16:
+            return launch_gemm_kc<BN, STAGES, TRACE, 16, PLS, BKT, SPLIT>(ma, mb, M, N, K, t, e, tr, splits, err, st);
+        default: return launch_gemm_kc<BN, STAGES, TRACE, 4, PLS, BKT, SPLIT>(ma, mb, M, N, K, t, e, tr, splits, err, st);
     }
 }
 
@@ -573,14 +622,28 @@ extern "C" int cf_umma_gemm_bf16(int M, int N, int K, int nterms, const int* ta,
         t.a[i] = ta[i];
         t.b[i] = tb[i];
     }
+    EpiArgs e{(__nv_bfloat16*)X, ldx, x_ps, x_planes, (__nv_bfloat16*)XT, ldxt, xt_ps, Cf, ldc, M, N};
+    TraceArgs tr{};
+    cudaStream_t st = (cudaStream_t)stream;
     CUtensorMap ma, mb;
+    // All planes of a 32-wide k-slice in one stage (each plane read once per
+    // k-slice instead of once per term), the leading term (0, 0) accumulated
+    // apart from the corrections; otherwise 64-wide k-tiles walked term by term.
+    const int pls = a_planes == b_planes ? a_planes : 0;
+    bool all_planes = (pls == 2 || pls == 3) && t.a[0] == 0 && t.b[0] == 0;
+    for (int i = 1; i < nterms && all_planes; ++i) all_planes = !(t.a[i] == 0 && t.b[i] == 0);
+    if (all_planes) {
+        int rc = make_map(&ma, A, K, M, lda, a_planes, a_ps, BM, 32);
+        if (rc) return rc;
+        rc = make_map(&mb, B, K, N, ldb, b_planes, b_ps, 256, 32);
+        if (rc) return rc;
+        if (pls == 3) return launch_gemm<256, 3, false, 3, 32, true>(ma, mb, M, N, K, t, e, tr, 1, err, st);
+        return launch_gemm<256, 4, false, 2, 32, true>(ma, mb, M, N, K, t, e, tr, 1, err, st);
+    }
     int rc = make_map(&ma, A, K, M, lda, a_planes, a_ps, BM);
     if (rc) return rc;
     rc = make_map(&mb, B, K, N, ldb, b_planes, b_ps, 256);
     if (rc) return rc;
-    EpiArgs e{(__nv_bfloat16*)X, ldx, x_ps, x_planes, (__nv_bfloat16*)XT, ldxt, xt_ps, Cf, ldc, M, N};
-    TraceArgs tr{};
-    cudaStream_t st = (cudaStream_t)stream;
     return launch_gemm<256, 4, false>(ma, mb, M, N, K, t, e, tr, 1, err, st);
 }
 

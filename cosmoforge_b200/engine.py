@@ -285,7 +285,9 @@ class Engine:
         n = A.shape[-1]
         B = A.shape[0] if A.dim() == 3 else 1
         info = torch.zeros(B, dtype=torch.int32, device=A.device)
-        check(self.lib.cf_potrf(n, A.data_ptr(), n, n * n, B, info.data_ptr(), stream()), "cf_potrf")
+        work = torch.empty(self.lib.cf_potrf_workspace(n, B) // 8 + 1, dtype=F64, device=A.device)
+        check(self.lib.cf_potrf(n, A.data_ptr(), n, n * n, B, work.data_ptr(), info.data_ptr(), stream()),
+              "cf_potrf")
         return info
 
     def lnl(self, cl_tables, N: torch.Tensor, maps: torch.Tensor, noise_scale=None):

@@ -86,7 +86,8 @@ int cf_build_block(int kind, int mode, int na, const double* va, int nb, const d
  * FP64 GEMM on the DMMA tensor pipe: C = alpha op(A) op(B) + beta C, with an
  * optional transposed copy CT = C^T (NULL to skip) and a batch dimension.
  * transa / transb: 0 = A is M x K / B is K x N; 1 = A given as K x M / B as N x K.
- * lower_only: skip output tiles strictly above the diagonal.
+ * lower_only: bit 0 skips output tiles strictly above the diagonal; bit 1 (with
+ * transa) starts each tile's K sum at its first row (op(A) = Y^T, Y lower).
  * Replaces: cosmocore/basics/linalg.py:18-32 (matrix_mult, np.matmul).
  */
 int cf_dgemm(int transa, int transb, int M, int N, int K, double alpha, const double* A, long lda,
@@ -94,17 +95,23 @@ int cf_dgemm(int transa, int transb, int M, int N, int K, double alpha, const do
              long strideC, double* CT, long ldct, long strideCT, int batch, int lower_only,
              void* stream);
 
+/* Bytes of workspace cf_potrf needs for `batch` problems of order n. */
+size_t cf_potrf_workspace(int n, int batch);
+
 /*
- * Blocked lower Cholesky factorisation in place (batch of n x n matrices).
- * info: int[batch], zeroed by the caller.
+ * Blocked lower Cholesky factorisation in place (batch of n x n matrices):
+ * 64-wide panels, diagonal block factored and inverted by one CTA, panel and
+ * trailing updates as DMMA GEMMs.  work: cf_potrf_workspace(n, batch) bytes
+ * (keeps the diagonal-block inverses for cf_trtri_lower).  info: int[batch],
+ * zeroed by the caller.
  * Replaces: cosmocore/basics/linalg.py:362-406 (cholesky_factor, LAPACK dpotrf).
  */
-int cf_potrf(int n, double* A, long lda, long strideA, int batch, int* info, void* stream);
+int cf_potrf(int n, double* A, long lda, long strideA, int batch, void* work, int* info, void* stream);
 
-/* Y = L^-1 for lower-triangular L (batch).  Replaces the dpotri half of
- * cosmocore/basics/linalg.py:152-219. */
+/* Y = L^-1 for the lower factor L of a preceding cf_potrf with the same `work`
+ * (batch).  Replaces the dpotri half of cosmocore/basics/linalg.py:152-219. */
 int cf_trtri_lower(int n, const double* L, long lda, long strideL, double* Y, long ldy, long strideY,
-                   int batch, void* stream);
+                   int batch, void* work, void* stream);
 
 /* Bytes of workspace cf_spd_inverse needs for `batch` problems of order n. */
 size_t cf_spd_inverse_workspace(int n, int batch);
@@ -121,7 +128,7 @@ int cf_spd_inverse(int n, double* A, long lda, long strideA, int batch, void* wo
 /*
  * Allocation-free SPD inverse: cf_spd_inverse for one n x n matrix with its
  * workspace taken from a scratch array compiled into the library (a
- * file-scope __device__ array of (1024^2 + 1024) doubles, 8.4 MB held by every
+ * file-scope __device__ array of 1.18 M doubles, 9.4 MB held by every
  * GPU that loads the library until exit), for callers that cannot call
  * cudaMalloc (host callbacks, allocator hooks, plugins whose host owns the
  * memory pool).  Allocates nothing.  n > cf_spd_inverse_static_max_n()

@@ -69,13 +69,18 @@ def test_umma_single_product_matches_rounded_inputs(M, N, K):
     assert err < 1e-5, float(err)
 
 
-@pytest.mark.parametrize("terms,planes,tol", [(X3, 2, 2e-4), (X6, 3, 2e-6)])
-def test_umma_split_products(terms, planes, tol):
+# (M, N, K): one tile; ragged sizes with a partial 32-wide k-slice; several
+# promotion chunks per tile and more tiles than SMs (persistent CTAs walk 2).
+SHAPES = [(384, 640, 512), (200, 300, 100), (2048, 4352, 2112)]
+
+
+@pytest.mark.parametrize("M,N,K", SHAPES)
+@pytest.mark.parametrize("terms,planes,tol", [(X3, 2, 2e-4), (X6, 3, 2e-6), (X3, 3, 2e-4)])
+def test_umma_split_products(terms, planes, tol, M, N, K):
     from cosmoforge_b200 import _lib
 
     lib = _lib.lib()
-    g = torch.Generator(device="cuda").manual_seed(7)
-    M, N, K = 384, 640, 512
+    g = torch.Generator(device="cuda").manual_seed(7 + M + K)
     A = torch.randn((M, K), dtype=torch.float64, device="cuda", generator=g)
     B = torch.randn((N, K), dtype=torch.float64, device="cuda", generator=g)
     Cf, _, _, _, _ = _gemm(lib, A, B, terms, planes)
