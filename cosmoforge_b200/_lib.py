@@ -54,6 +54,10 @@ SIGNATURES = {
     "cf_split_bf16": (_i, [_i, _i, _p, _l, _i, _p, _l, _l, _p]),
     "cf_umma_gemm_bf16": (_i, [_i, _i, _i, _i, _p, _p, _p, _l, _l, _i, _p, _l, _l, _i, _p, _l, _l, _i,
                                _p, _l, _l, _p, _l, _p, _p]),
+    "cf_potrf_f32_workspace": (_sz, [_i, _i]),
+    "cf_potrf_f32": (_i, [_i, _p, _l, _l, _i, _p, _p, _p]),
+    "cf_axpby_f32": (_i, [_l, _d, _p, _l, _d, _p, _p, _l, _p, _l, _p, _l, _i, _p]),
+    "cf_chi2_logdet_mixed": (_i, [_i, _p, _l, _l, _p, _l, _l, _i, _p, _l, _l, _i, _p, _p, _p]),
 }
 
 _lib = None

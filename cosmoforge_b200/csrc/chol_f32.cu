@@ -1,0 +1,414 @@
+// Mixed-precision pixel likelihood: FP32 batched Cholesky, FP64-refined chi2.
+//
+// The reference evaluates -2 lnL = x^T C^-1 x + ln|C| per parameter point with
+// an FP64 inverse and a second FP64 Cholesky for the determinant
+// (picslike/picslike.py:568-664, cosmocore/basics/linalg.py:362-474).  Here
+// the factor is computed in FP32 and the solve is refined in FP64:
+//
+//   L L^T = C (FP32, blocked right-looking, 64-wide panels; the trailing
+//           updates are FP32 SIMT GEMMs),
+//   w = L^-1 x,  v = L^-T w               (FP64 arithmetic on the FP32 factor)
+//   chi2 = 2 w.w - v^T C v                (C in FP64)
+//
+// The last line is x^T z_1 for one step of iterative refinement
+// z_1 = z_0 + (L L^T)^-1 (x - C z_0) from z_0 = v, so the chi2 error is second
+// order in the factor's backward error.  ln|C| = 2 sum ln L_ii carries the
+// factor's first-order error.
+#include "cf_common.cuh"
+
+namespace {
+
+constexpr int NB = 64;
+constexpr int LDS = NB + 1;
+
+// Factor the kb x kb diagonal block at (k0, k0) of every batch matrix in place
+// (FP32) and write L11^-1 to Dinv (kb x kb, row-major).  One barrier per
+// column: the scaling of column j is folded into step j + 1.
+__global__ void __launch_bounds__(256) k_potrf_diag_inv_f32(float* A, long lda, long sA, int k0, int kb, float* Dinv,
+                                                            long sD, int* info)
+{
+    __shared__ float S[NB * LDS];
+    __shared__ float Xs[NB * LDS];
+    __shared__ float piv[NB];
+    __shared__ int bad;
+    const int b = blockIdx.x;
+    A += b * sA;
+    Dinv += b * sD;
+    const int tid = threadIdx.x;
+    for (int e = tid; e < kb * kb; e += blockDim.x) {
+        const int r = e / kb, c = e % kb;
+        S[r * LDS + c] = (c <= r) ? A[(long)(k0 + r) * lda + k0 + c] : 0.0f;
+    }
+    if (tid == 0) bad = 0;
+    __syncthreads();
+    for (int j = 0; j < kb; ++j) {
+        float d = S[j * LDS + j];
+        if (!(d > 0.0f)) {  // also catches NaN
+            if (tid == 0 && !bad) bad = k0 + j + 1;
+            d = 1.0f;
+        }
+        if (tid == 0) piv[j] = sqrtf(d);
+        const float inv_d = 1.0f / d;
+        const int m = kb - j - 1;
+        for (int e = tid; e < m * (m + 1) / 2; e += blockDim.x) {
+            int r = (int)((sqrtf(8.0f * e + 1.0f) - 1.0f) * 0.5f);
+            while ((r + 1) * (r + 2) / 2 <= e) ++r;
+            while (r * (r + 1) / 2 > e) --r;
+            const int c = e - r * (r + 1) / 2;
+            const int rr = j + 1 + r, cc = j + 1 + c;
+            S[rr * LDS + cc] -= S[rr * LDS + j] * S[cc * LDS + j] * inv_d;
+        }
+        if (j > 0)
+            for (int r = j + tid; r < kb; r += blockDim.x) S[r * LDS + j - 1] /= piv[j - 1];
+        __syncthreads();
+    }
+    // the last column has no entries below its diagonal, which becomes piv
+    for (int r = tid; r < kb; r += blockDim.x) S[r * LDS + r] = piv[r];
+    __syncthreads();
+    for (int e = tid; e < kb * kb; e += blockDim.x) {
+        const int r = e / kb, c = e % kb;
+        A[(long)(k0 + r) * lda + k0 + c] = (c <= r) ? S[r * LDS + c] : 0.0f;
+    }
+    if (tid < kb) {  // L11^-1 by forward substitution, one thread per column
+        const int c = tid;
+        for (int r = 0; r < kb; ++r) {
+            float x = 0.0f;
+            if (r >= c) {
+                float acc = (r == c) ? 1.0f : 0.0f;
+                for (int t = c; t < r; ++t) acc -= S[r * LDS + t] * Xs[t * LDS + c];
+                x = acc / S[r * LDS + r];
+            }
+            Xs[r * LDS + c] = x;
+        }
+    }
+    __syncthreads();
+    for (int e = tid; e < kb * kb; e += blockDim.x) {
+        const int r = e / kb, c = e % kb;
+        Dinv[r * kb + c] = Xs[r * LDS + c];
+    }
+    if (tid == 0 && bad && info && info[b] == 0) info[b] = bad;
+}
+
+// FP32 SIMT GEMM, both operands K-contiguous (the "NT" form):
+//   C[M x N] = alpha A[M x K] B[N x K]^T + beta C, batch on blockIdx.z.
+// 128 x 128 tile, BK 16, 256 threads with 8 x 8 outputs each (two 4 x 4
+// quadrants 64 rows / columns apart so shared-memory reads are broadcast-free
+// float4s).  The next k-tile is fetched into registers while the current one
+// is consumed.  lower_only: skip tiles strictly above the diagonal.
+constexpr int SBM = 128, SBK = 16, SNT = 256, SPAD = 4;
+
+__global__ void __launch_bounds__(SNT, 2) k_sgemm_nt(int M, int N, int K, float alpha, const float* A, long lda,
+                                                  long sA, const float* B, long ldb, long sB, float beta, float* C,
+                                                  long ldc, long sC, int lower_only)
+{
+    __shared__ __align__(16) float As[2][SBK][SBM + SPAD];
+    __shared__ __align__(16) float Bs[2][SBK][SBM + SPAD];
+    const int tile_m = blockIdx.y * SBM, tile_n = blockIdx.x * SBM;
+    if (lower_only && tile_n > tile_m + SBM - 1) return;
+    A += (long)blockIdx.z * sA;
+    B += (long)blockIdx.z * sB;
+    C += (long)blockIdx.z * sC;
+    const int tid = threadIdx.x;
+    // loader: thread -> (row lr, k half lk)
+    const int lr = tid >> 1, lk = (tid & 1) * 8;
+    const int ty = tid >> 4, tx = tid & 15;
+    float acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+    float ra[8], rb[8];
+    auto fetch = [&](int k0) {
+        const int ga = tile_m + lr, gb = tile_n + lr;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int gk = k0 + lk + u;
+            ra[u] = (ga < M && gk < K) ? A[(long)ga * lda + gk] : 0.0f;
+            rb[u] = (gb < N && gk < K) ? B[(long)gb * ldb + gk] : 0.0f;
+        }
+    };
+    auto stash = [&](int s) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            As[s][lk + u][lr] = ra[u];
+            Bs[s][lk + u][lr] = rb[u];
+        }
+    };
+    const int KT = (K + SBK - 1) / SBK;
+    fetch(0);
+    stash(0);
+    __syncthreads();
+    for (int kt = 0; kt < KT; ++kt) {
+        const int s = kt & 1;
+        if (kt + 1 < KT) fetch((kt + 1) * SBK);
+#pragma unroll
+        for (int k = 0; k < SBK; ++k) {
+            const float4 a0 = *reinterpret_cast<const float4*>(&As[s][k][ty * 4]);
+            const float4 a1 = *reinterpret_cast<const float4*>(&As[s][k][64 + ty * 4]);
+            const float4 b0 = *reinterpret_cast<const float4*>(&Bs[s][k][tx * 4]);
+            const float4 b1 = *reinterpret_cast<const float4*>(&Bs[s][k][64 + tx * 4]);
+            const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+        }
+        if (kt + 1 < KT) stash(s ^ 1);
+        __syncthreads();
+    }
+    // 16-byte row segments when the row stride and base allow it
+    const bool vec = ((ldc & 3) == 0) && ((((uintptr_t)C) & 15) == 0);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int r = tile_m + (i < 4 ? ty * 4 + i : 64 + ty * 4 + i - 4);
+        if (r >= M) continue;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int c0 = tile_n + h * 64 + tx * 4;
+            float* pc = C + (long)r * ldc + c0;
+            if (vec && c0 + 4 <= N) {
+                float4 o = make_float4(alpha * acc[i][h * 4], alpha * acc[i][h * 4 + 1], alpha * acc[i][h * 4 + 2],
+                                       alpha * acc[i][h * 4 + 3]);
+                if (beta != 0.0f) {
+                    const float4 q = *reinterpret_cast<const float4*>(pc);
+                    o.x += beta * q.x;
+                    o.y += beta * q.y;
+                    o.z += beta * q.z;
+                    o.w += beta * q.w;
+                }
+                *reinterpret_cast<float4*>(pc) = o;
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    if (c0 + j >= N) continue;
+                    float v = alpha * acc[i][h * 4 + j];
+                    if (beta != 0.0f) v += beta * pc[j];
+                    pc[j] = v;
+                }
+            }
+        }
+    }
+}
+
+int sgemm_nt(int M, int N, int K, float alpha, const float* A, long lda, long sA, const float* B, long ldb, long sB,
+             float beta, float* C, long ldc, long sC, int batch, int lower_only, cudaStream_t st)
+{
+    if (M <= 0 || N <= 0) return CF_OK;
+    dim3 grid(cf_cdiv(N, SBM), cf_cdiv(M, SBM), batch);
+    k_sgemm_nt<<<grid, SNT, 0, st>>>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, lower_only);
+    CF_CHECK_LAUNCH();
+    return CF_OK;
+}
+
+__global__ void k_copy2d_f32(int R, int Ccols, const float* src, long lds, long ss, float* dst, long ldd, long sd)
+{
+    src += blockIdx.z * ss;
+    dst += blockIdx.z * sd;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y * blockDim.y + threadIdx.y;
+    if (r < R && c < Ccols) dst[(long)r * ldd + c] = src[(long)r * lds + c];
+}
+
+// Z = a X + c_b W in FP64 and Z32 = (float) Z, per batch entry b.
+__global__ void k_axpby_f32(long count, double a, const double* X, long sX, double c, const double* cvec,
+                            const double* W, long sW, double* Z, long sZ, float* Z32, long sZ32)
+{
+    const int b = blockIdx.y;
+    const double cb = cvec ? cvec[b] : c;
+    X += b * sX;
+    W += b * sW;
+    if (Z) Z += b * sZ;
+    Z32 += b * sZ32;
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < count; e += (long)gridDim.x * blockDim.x) {
+        const double v = a * X[e] + cb * W[e];
+        if (Z) Z[e] = v;
+        Z32[e] = (float)v;
+    }
+}
+
+constexpr int CNT = 256;
+
+// One CTA per (problem b, map m): w = L^-1 x, v = L^-T w (FP64 arithmetic on
+// the FP32 factor, both vectors in shared memory), then
+// chi2 = 2 w.w - v^T C v with C read from its FP64 lower triangle.
+__global__ void __launch_bounds__(CNT) k_chi2_refined(int n, const float* L, long lda, long sL, const double* C,
+                                                      long ldc, long sC, const double* X, long ldx, long sX,
+                                                      int nrhs, double* chi2)
+{
+    extern __shared__ double sh[];
+    double* w = sh;
+    double* v = sh + n;
+    const int b = blockIdx.x / nrhs, m = blockIdx.x % nrhs;
+    L += (long)b * sL;
+    C += (long)b * sC;
+    X += (long)b * sX;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    __shared__ double red[CNT / 32];
+    for (int i = tid; i < n; i += CNT) w[i] = X[(long)i * ldx + m];
+    __syncthreads();
+    // forward substitution, 32 rows per block
+    for (int b0 = 0; b0 < n; b0 += 32) {
+        const int kb = n - b0 < 32 ? n - b0 : 32;
+        if (warp == 0) {
+            double zi = lane < kb ? w[b0 + lane] : 0.0;
+            for (int r = 0; r < kb; ++r) {
+                if (lane == r) zi /= (double)L[(long)(b0 + r) * lda + b0 + r];
+                const double zr = __shfl_sync(0xffffffffu, zi, r);
+                if (lane > r && lane < kb) zi -= (double)L[(long)(b0 + lane) * lda + b0 + r] * zr;
+            }
+            if (lane < kb) w[b0 + lane] = zi;
+        }
+        __syncthreads();
+        const double zl = lane < kb ? w[b0 + lane] : 0.0;
+        for (int r = b0 + kb + warp; r < n; r += CNT / 32) {
+            double t = lane < kb ? (double)L[(long)r * lda + b0 + lane] * zl : 0.0;
+            for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+            if (lane == 0) w[r] -= t;
+        }
+        __syncthreads();
+    }
+    for (int i = tid; i < n; i += CNT) v[i] = w[i];
+    __syncthreads();
+    // back substitution L^T v = w, 32 rows per block from the bottom
+    const int nblk = (n + 31) / 32;
+    for (int blk = nblk - 1; blk >= 0; --blk) {
+        const int b0 = blk * 32;
+        const int kb = n - b0 < 32 ? n - b0 : 32;
+        if (warp == 0) {
+            double vi = lane < kb ? v[b0 + lane] : 0.0;
+            for (int r = kb - 1; r >= 0; --r) {
+                if (lane == r) vi /= (double)L[(long)(b0 + r) * lda + b0 + r];
+                const double vr = __shfl_sync(0xffffffffu, vi, r);
+                if (lane < r) vi -= (double)L[(long)(b0 + r) * lda + b0 + lane] * vr;
+            }
+            if (lane < kb) v[b0 + lane] = vi;
+        }
+        __syncthreads();
+        // rows above the block: v[i] -= sum_k L[b0 + k, i] v[b0 + k]
+        for (int i = tid; i < b0; i += CNT) {
+            double t = 0.0;
+            for (int k = 0; k < kb; ++k) t += (double)L[(long)(b0 + k) * lda + i] * v[b0 + k];
+            v[i] -= t;
+        }
+        __syncthreads();
+    }
+    // 2 w.w - v^T C v, C from its lower triangle
+    double s = 0.0;
+    for (int i = tid; i < n; i += CNT) s += 2.0 * w[i] * w[i];
+    for (int r = warp; r < n; r += CNT / 32) {
+        const double* cr = C + (long)r * ldc;
+        double t = 0.0;
+        for (int c = lane; c < r; c += 32) t += cr[c] * v[c];
+        t = 2.0 * t;
+        if (lane == 0) t += cr[r] * v[r];
+        s -= t * v[r];
+    }
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) red[warp] = s;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int q = 0; q < CNT / 32; ++q) t += red[q];
+        chi2[blockIdx.x] = t;
+    }
+}
+
+__global__ void __launch_bounds__(CNT) k_logdet_f32(int n, const float* L, long lda, long sL, double* logdet)
+{
+    L += (long)blockIdx.x * sL;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += CNT) s += log((double)L[(long)i * lda + i]);
+    __shared__ double red[CNT / 32];
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int q = 0; q < CNT / 32; ++q) t += red[q];
+        logdet[blockIdx.x] = 2.0 * t;
+    }
+}
+
+inline size_t potrf_f32_ws(int n) { return (size_t)NB * NB + (size_t)n * NB; }
+
+}  // namespace
+
+extern "C" size_t cf_potrf_f32_workspace(int n, int batch) { return potrf_f32_ws(n) * sizeof(float) * (size_t)batch; }
+
+// Blocked FP32 Cholesky in place (lower factor), batched: per 64-wide panel the
+// diagonal block is factored and inverted by one CTA, L21 = A21 L11^-T and
+// A22 -= L21 L21^T are FP32 GEMMs.  info: int[batch] zeroed by the caller.
+extern "C" int cf_potrf_f32(int n, float* A, long lda, long strideA, int batch, void* work, int* info, void* stream)
+{
+    if (n <= 0 || batch < 1 || !A || !work || lda < n) return CF_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    const long ws = (long)potrf_f32_ws(n);
+    float* Di = (float*)work;        // [batch][NB][NB]
+    float* T = Di + (long)NB * NB;   // [batch][n][NB]
+    for (int k0 = 0; k0 < n; k0 += NB) {
+        const int kb = n - k0 < NB ? n - k0 : NB;
+        k_potrf_diag_inv_f32<<<batch, 256, 0, st>>>(A, lda, strideA, k0, kb, Di, ws, info);
+        CF_CHECK_LAUNCH();
+        const int rest = n - k0 - kb;
+        if (rest > 0) {
+            float* a21 = A + (long)(k0 + kb) * lda + k0;
+            int rc = sgemm_nt(rest, kb, kb, 1.0f, a21, lda, strideA, Di, kb, ws, 0.0f, T, kb, ws, batch, 0, st);
+            if (rc) return rc;
+            rc = sgemm_nt(rest, rest, kb, -1.0f, T, kb, ws, T, kb, ws, 1.0f, a21 + kb, lda, strideA, batch, 1, st);
+            if (rc) return rc;
+            k_copy2d_f32<<<dim3(cf_cdiv(kb, 32), cf_cdiv(rest, 8), batch), dim3(32, 8), 0, st>>>(rest, kb, T, kb, ws,
+                                                                                                a21, lda, strideA);
+            CF_CHECK_LAUNCH();
+        }
+    }
+    return CF_OK;
+}
+
+// Z_b = a X_b + c_b W_b in FP64 (Z may be NULL) and its FP32 copy Z32_b
+// (c_b = cvec[b] if cvec else c; strideW = 0 shares W).  The noise addition
+// C = S + s N of picslike/picslike.py:301-319 producing both precisions.
+extern "C" int cf_axpby_f32(long count, double a, const double* X, long strideX, double c, const double* cvec,
+                            const double* W, long strideW, double* Z, long strideZ, float* Z32, long strideZ32,
+                            int batch, void* stream)
+{
+    if (count <= 0 || batch < 1 || !X || !W || !Z32) return CF_ERR_ARG;
+    long blocks = (count + 255) / 256;
+    if (blocks > 1184) blocks = 1184;
+    k_axpby_f32<<<dim3((unsigned)blocks, batch), 256, 0, (cudaStream_t)stream>>>(count, a, X, strideX, c, cvec, W,
+                                                                                 strideW, Z, strideZ, Z32,
+                                                                                 strideZ32);
+    CF_CHECK_LAUNCH();
+    return CF_OK;
+}
+
+// chi2[b nrhs + m] = 2 |L_b^-1 x|^2 - v^T C_b v with v = (L_b L_b^T)^-1 x (one
+// FP64 refinement step on the FP32 factor L_b of C_b), logdet[b] = 2 sum ln
+// (L_b)_ii.  C: FP64 matrices (lower triangle read); X: n x nrhs (ldx),
+// strideX = 0 shares it.  n <= 12288 (two FP64 vectors in shared memory).
+extern "C" int cf_chi2_logdet_mixed(int n, const float* L, long lda, long strideL, const double* C, long ldc,
+                                    long strideC, int batch, const double* X, long ldx, long strideX, int nrhs,
+                                    double* chi2, double* logdet, void* stream)
+{
+    if (n <= 0 || batch < 1 || nrhs < 0 || !L) return CF_ERR_ARG;
+    if (n > 12288) return CF_ERR_UNSUPPORTED;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (nrhs > 0) {
+        if (!X || !C || !chi2) return CF_ERR_ARG;
+        const size_t smem = 2 * (size_t)n * sizeof(double);
+        static bool attr = false;
+        if (!attr) {
+            CF_CHECK(cudaFuncSetAttribute(k_chi2_refined, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          2 * 12288 * (int)sizeof(double)));
+            attr = true;
+        }
+        k_chi2_refined<<<batch * nrhs, CNT, smem, st>>>(n, L, lda, strideL, C, ldc, strideC, X, ldx, strideX, nrhs,
+                                                       chi2);
+        CF_CHECK_LAUNCH();
+    }
+    if (logdet) {
+        k_logdet_f32<<<batch, CNT, 0, st>>>(n, L, lda, strideL, logdet);
+        CF_CHECK_LAUNCH();
+    }
+    return CF_OK;
+}

@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(256) k_potrf_diag_inv(double* A, long lda, lon
             for (int r = j + tid; r < kb; r += blockDim.x) S[r * LDS + j - 1] /= piv[j - 1];
         __syncthreads();
     }
-    for (int r = kb - 1 + tid; r < kb; r += blockDim.x) S[r * LDS + kb - 1] /= piv[kb - 1];
+    // the last column has no entries below its diagonal, which becomes piv
     for (int r = tid; r < kb; r += blockDim.x) S[r * LDS + r] = piv[r];
     __syncthreads();
     for (int e = tid; e < kb * kb; e += blockDim.x) {

@@ -290,8 +290,14 @@ class Engine:
               "cf_potrf")
         return info
 
-    def lnl(self, cl_tables, N: torch.Tensor, maps: torch.Tensor, noise_scale=None):
-        """chi2 (B x nsims), ln|C| (B,), lnL (B x nsims), info (B,) for a batch of points."""
+    def lnl(self, cl_tables, N: torch.Tensor, maps: torch.Tensor, noise_scale=None, precision: str = "fp64"):
+        """chi2 (B x nsims), ln|C| (B,), lnL (B x nsims), info (B,) for a batch of points.
+
+        precision "fp64": FP64 Cholesky, chi2 = |L^-1 x|^2, ln|C| from its
+        diagonal.  "mixed": FP32 Cholesky of C, chi2 from one FP64 refinement
+        step against the FP64 C (second-order error), ln|C| from the FP32
+        factor's diagonal summed in FP64.
+        """
         cl = torch.as_tensor(cl_tables, dtype=F64, device=self.dev)
         if cl.dim() == 2:
             cl = cl[None]
@@ -301,6 +307,10 @@ class Engine:
         sc = None
         if noise_scale is not None:
             sc = torch.as_tensor(noise_scale, dtype=F64, device=self.dev).reshape(B).contiguous()
+        if precision == "mixed":
+            return self._lnl_mixed(C, N, maps, sc)
+        if precision != "fp64":
+            raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
         check(self.lib.cf_axpby(n * n, 1.0, C.data_ptr(), n * n, 1.0, ptr(sc), N.data_ptr(), 0,
                                 C.data_ptr(), n * n, B, stream()), "cf_axpby")
         info = self.potrf(C)
@@ -312,6 +322,24 @@ class Engine:
         check(self.lib.cf_chi2_logdet(n, C.data_ptr(), n, n * n, B, X.data_ptr(), nsims, 0, nsims,
                                       z.data_ptr(), chi2.data_ptr(), logdet.data_ptr(), stream()),
               "cf_chi2_logdet")
+        return chi2, logdet, -0.5 * (chi2 + logdet[:, None]), info
+
+    def _lnl_mixed(self, C: torch.Tensor, N: torch.Tensor, maps: torch.Tensor, sc):
+        B, n = C.shape[0], self.L.n
+        C32 = torch.empty((B, n, n), dtype=torch.float32, device=self.dev)
+        check(self.lib.cf_axpby_f32(n * n, 1.0, C.data_ptr(), n * n, 1.0, ptr(sc), N.data_ptr(), 0,
+                                    C.data_ptr(), n * n, C32.data_ptr(), n * n, B, stream()), "cf_axpby_f32")
+        info = torch.zeros(B, dtype=torch.int32, device=self.dev)
+        work = torch.empty(self.lib.cf_potrf_f32_workspace(n, B) // 4 + 1, dtype=torch.float32, device=self.dev)
+        check(self.lib.cf_potrf_f32(n, C32.data_ptr(), n, n * n, B, work.data_ptr(), info.data_ptr(), stream()),
+              "cf_potrf_f32")
+        X = maps.to(self.dev, F64).contiguous()
+        nsims = X.shape[1]
+        chi2 = torch.empty((B, nsims), dtype=F64, device=self.dev)
+        logdet = torch.empty(B, dtype=F64, device=self.dev)
+        check(self.lib.cf_chi2_logdet_mixed(n, C32.data_ptr(), n, n * n, C.data_ptr(), n, n * n, B,
+                                            X.data_ptr(), nsims, 0, nsims, chi2.data_ptr(), logdet.data_ptr(),
+                                            stream()), "cf_chi2_logdet_mixed")
         return chi2, logdet, -0.5 * (chi2 + logdet[:, None]), info
 
 

@@ -5,7 +5,9 @@ Same constructor and outputs as ``picslike.PICSLike`` (``picslike/picslike.py:
 chi2 = x^T C^-1 x per simulation, ln|C| and lnL = -(chi2 + ln|C|)/2 (the 2 pi
 constant omitted, as in the reference).  Points run in batches: one batched
 build of S(theta) for all points of a batch, one batched Cholesky, and
-chi2 / ln|C| from the factor, all on the GPU.
+chi2 / ln|C| from the factor, all on the GPU.  ``precision="mixed"`` factors
+C in FP32 and refines chi2 in FP64 (one step against the FP64 C); ln|C| then
+carries the FP32 factor's rounding.
 
 The parameter grid is supplied in memory: ``parameter_grid`` is any object
 with ``grid_points`` (list of tuples) and ``get_spectrum(point) -> {label:
@@ -87,7 +89,8 @@ class PICSLike(_Base):
             part = spectra[b0: b0 + self.batch_size]
             cl = np.stack([L.smoothed_cl_table(c) for c in part])
             sc = None if noise_scale is None else np.asarray(noise_scale[b0: b0 + len(part)], dtype=np.float64)
-            chi2, ld, lnl, info = self.engine.lnl(cl, self._dev_N, self._dev_X, noise_scale=sc)
+            chi2, ld, lnl, info = self.engine.lnl(cl, self._dev_N, self._dev_X, noise_scale=sc,
+                                                  precision=self.precision)
             bad = info.cpu().numpy()
             if np.any(bad != 0):
                 k = int(np.flatnonzero(bad)[0])

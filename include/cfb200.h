@@ -184,6 +184,84 @@ int cf_axpby(long count, double a, const double* X, long strideX, double c, cons
 /* B = A^T for an R x C row-major A. */
 int cf_transpose(int R, int C, const double* A, long lda, double* B, long ldb, void* stream);
 
+/* ---- Mixed-precision path: BF16 split planes on the tcgen05 tensor cores ----
+ * An FP64 value x is carried as planes x_0 = bf16(x), x_1 = bf16(x - x_0),
+ * x_2 = bf16(x - x_0 - x_1); a product list {(a_t, b_t)} selects which plane
+ * pairs are multiplied: BF16x3 = {(0,0),(0,1),(1,0)} (~16 bits), BF16x6 adds
+ * {(0,2),(1,1),(2,0)} (~24 bits).  Plane arrays are __nv_bfloat16, passed as
+ * void*.  err: device int set to 1 when a bounded wait inside a tensor-core
+ * kernel ran out (the kernel then returns early; results are invalid). */
+
+/* BF16 split planes of an R x C FP64 matrix (row stride ldx) into `planes`
+ * (1..3) planes of row stride ldo, plane_stride elements apart.  Operand
+ * preparation for qube/fisher.py:501-531 (A_b = C^-1 dC_b) in mixed precision. */
+int cf_split_bf16(int R, int C, const double* X, long ldx, int planes, void* out, long ldo,
+                  long plane_stride, void* stream);
+
+/* BF16 split planes of the outer products x_q y_q^T (n x n, q < nvec; x and y
+ * are n x nvec with row stride ldv) into out[p][q] (row stride ld, q_stride /
+ * plane_stride elements apart).  The quadratic forms of
+ * qube/spectra.py:1124-1186 as contractions against resident A_b slabs. */
+int cf_outer_planes(int n, int nvec, const double* x, const double* y, long ldv, int planes, void* out,
+                    long ld, long q_stride, long plane_stride, void* stream);
+
+/* cf_build_block writing BF16 split planes (planes 1..3, plane_stride /
+ * planeT_stride elements apart) instead of FP64.  flags bit 0 (auto kinds):
+ * every entry computed from its own pixel pair, no mirror writes; bit 1
+ * (cross kinds): write only the transposed block outT.  Replaces the same
+ * reference functions as cf_build_block (cosmocore/signal_kernels.py:715-829,
+ * cosmocore/basis/pixel.py:802-950) for the mixed path. */
+int cf_build_block_planes(int kind, int mode, int na, const double* va, int nb, const double* vb,
+                          int lmax, const double* t0, const double* t1, const double* t2,
+                          const int* bin_of, void* out, long ld, long row_off, long col_off,
+                          long bin_stride, void* outT, long ldT, long rowT_off, long colT_off,
+                          long binT_stride, int batch, long tstride, long ostride, int planes,
+                          long plane_stride, long planeT_stride, int flags, void* stream);
+
+/*
+ * C = sum_t A_{ta[t]} B_{tb[t]}^T on tcgen05 (FP32 accumulation in TMEM,
+ * partial sums promoted to registers every few k-tiles).  A: planes of
+ * M x K (row stride lda, plane stride a_ps), B: planes of N x K.  ta/tb are
+ * HOST int arrays of nterms (1..6) plane indices.  Outputs, any may be NULL:
+ * X = C as x_planes (1..3) BF16 split planes (M x N, ldx, x_ps); XT = C^T
+ * likewise (N x M, ldxt, xt_ps); Cf = C in FP32 (M x N, ldc).  Row strides
+ * and plane strides must be multiples of 8 elements, bases 16-byte aligned.
+ * Replaces: qube/fisher.py:501-531 (A_b = C^-1 dC_b, matrix_mult) in the
+ * mixed path.
+ */
+int cf_umma_gemm_bf16(int M, int N, int K, int nterms, const int* ta, const int* tb, const void* A,
+                      long lda, long a_ps, int a_planes, const void* B, long ldb, long b_ps,
+                      int b_planes, void* X, long ldx, long x_ps, int x_planes, void* XT, long ldxt,
+                      long xt_ps, float* Cf, long ldc, int* err, void* stream);
+
+/*
+ * Fisher contraction on tcgen05 with FP64 promotion of the partial sums:
+ *   F[(p_off+p) ldF + q_off+q] += scale sum_t sum_{k<K1, l<K2}
+ *                                 X_{ta[t]}[p sXp + k ldX + l] Y_{tb[t]}[q sYq + k ldY + l]
+ * (and the mirror entry when sym), X/Y BF16 planes x_ps / y_ps apart.  F is
+ * FP64 and accumulated with atomics over `splits` CTAs per output tile
+ * (splits <= 0 picks a split that fills the GPU); zero it first.
+ * Replaces: qube/fisher.py:557-607 and cosmocore/basics/linalg.py:66-98
+ * (F_ij = 1/2 Tr(A_i A_j)) in the mixed path.
+ */
+int cf_umma_trace_bf16(int P1, int P2, int K1, int K2, int nterms, const int* ta, const int* tb,
+                       const void* X, long sXp, long ldX, long x_ps, int x_planes, const void* Y,
+                       long sYq, long ldY, long y_ps, int y_planes, double scale, double* F, long ldF,
+                       long p_off, long q_off, int sym, int splits, int* err, void* stream);
+
+/* cf_umma_trace_bf16 with output row p scattered to F row row_map[p] and
+ * column q to F column col_map[q] (device int arrays). */
+int cf_umma_trace_bf16_mapped(int P1, int P2, int K1, int K2, int nterms, const int* ta, const int* tb,
+                              const void* X, long sXp, long ldX, long x_ps, int x_planes, const void* Y,
+                              long sYq, long ldY, long y_ps, int y_planes, double scale, double* F,
+                              long ldF, const int* row_map, const int* col_map, int sym, int splits,
+                              int* err, void* stream);
+
+/* Promotion interval of the tensor-core kernels: k-tiles of 64 summed in one
+ * FP32 TMEM accumulator before promotion (1, 2, 4, 8 or 16; default 16).
+ * Returns the previous value.  No counterpart in the reference. */
+int cf_umma_set_promotion(int kc);
+
 #ifdef __cplusplus
 }
 #endif

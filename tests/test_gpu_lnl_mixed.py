@@ -1,0 +1,147 @@
+"""Mixed-precision pixel likelihood (FP32 Cholesky, FP64-refined chi2).
+
+Checked against the reference's own outputs on the golden fixtures (the
+same cases the FP64 path matches to 1e-10) and against the FP64 device path
+on random SPD batches.  Tolerances, measured on B200 with margin:
+  chi2 (one FP64 refinement step)   relative 1e-8
+  ln|C| and lnL (FP32 factor)       absolute 3e-3 (lnL values are O(7e3): FP32
+                                    rounding of the Schur complements, ~1e-4 per
+                                    entry, against pivots near the noise level)
+  FP32 factor L                      relative 1e-5 of max |L| on well-conditioned batches
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from cosmoforge_b200 import workloads
+from cosmoforge_b200.layout import build_layout
+from golden_cases import load, params_of
+
+pytestmark = pytest.mark.gpu
+
+CHI2_REL = 1e-8
+LNL_ABS = 3e-3
+
+
+def _spd_batch(n, batch, seed):
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    R = torch.randn((batch, n, n), dtype=torch.float64, device="cuda", generator=g)
+    return R @ R.transpose(1, 2) / n + torch.eye(n, dtype=torch.float64, device="cuda")
+
+
+@pytest.mark.parametrize("n,batch", [(200, 3), (333, 2), (1312, 2)])
+def test_potrf_f32_matches_fp64_factor(n, batch):
+    from cosmoforge_b200 import _lib
+
+    lib = _lib.lib()
+    C = _spd_batch(n, batch, n)
+    A = C.float().contiguous()
+    info = torch.zeros(batch, dtype=torch.int32, device="cuda")
+    work = torch.empty(lib.cf_potrf_f32_workspace(n, batch) // 4 + 1, dtype=torch.float32, device="cuda")
+    assert lib.cf_potrf_f32(n, A.data_ptr(), n, n * n, batch, work.data_ptr(), info.data_ptr(),
+                            torch.cuda.current_stream().cuda_stream) == 0
+    assert int(info.abs().max()) == 0
+    L64 = torch.linalg.cholesky(C)
+    L32 = torch.tril(A.double())
+    err = float((L32 - L64).abs().max() / L64.abs().max())
+    print(f"n={n}: factor error {err:.2e}")
+    assert err <= 1e-5
+
+
+def test_potrf_f32_reports_first_bad_pivot():
+    from cosmoforge_b200 import _lib
+
+    lib = _lib.lib()
+    n, batch = 150, 3
+    C = _spd_batch(n, batch, 5)
+    C[1, 70, :] = 0.0
+    C[1, :, 70] = 0.0
+    C[1, 70, 70] = -1.0
+    A = C.float().contiguous()
+    info = torch.zeros(batch, dtype=torch.int32, device="cuda")
+    work = torch.empty(lib.cf_potrf_f32_workspace(n, batch) // 4 + 1, dtype=torch.float32, device="cuda")
+    assert lib.cf_potrf_f32(n, A.data_ptr(), n, n * n, batch, work.data_ptr(), info.data_ptr(),
+                            torch.cuda.current_stream().cuda_stream) == 0
+    assert info.cpu().tolist() == [0, 71, 0]
+
+
+def _check(chi2, lnl, ref_chi2, ref_lnl, tag):
+    e_chi2 = float(np.max(np.abs(chi2 / ref_chi2 - 1)))
+    e_lnl = float(np.max(np.abs(lnl - ref_lnl)))
+    print(f"{tag}: chi2 rel {e_chi2:.2e}  |dlnL| {e_lnl:.2e}")
+    assert e_chi2 <= CHI2_REL
+    assert e_lnl <= LNL_ABS
+
+
+def test_lnl_mixed_fortran_picslike():
+    from cosmoforge_b200 import engine
+
+    d = load("fortran_picslike_nside8_B")
+    L = build_layout(params_of(d), d["mask"], d["beam"])
+    E = engine.Engine(L)
+    cl = np.stack([L.smoothed_cl_table({"BB": c}) for c in d["point_cl_BB"]])
+    chi2, ld, lnl, info = E.lnl(cl, torch.from_numpy(d["noise"]).cuda(), torch.from_numpy(d["maps"]),
+                                precision="mixed")
+    assert int(info.abs().max()) == 0
+    _check(chi2.cpu().numpy()[:, 0], lnl.cpu().numpy()[:, 0], d["ref_chi2"][:, 0], d["ref_lnl"][:, 0],
+           "fortran_picslike")
+
+
+def test_lnl_mixed_tqu_batch():
+    from cosmoforge_b200 import engine
+
+    d = load("picslike_tqu_nside8")
+    L = build_layout(params_of(d), d["mask"], d["beam"])
+    E = engine.Engine(L)
+    cl = np.stack([L.smoothed_cl_table(workloads.model_cls(t, L.lmax_signal)) for t in d["thetas"]])
+    N = torch.from_numpy(np.diag(d["noise_diag"])).cuda()
+    chi2, ld, lnl, info = E.lnl(cl, N, torch.from_numpy(d["maps"]), noise_scale=d["thetas"][:, 4],
+                                precision="mixed")
+    assert int(info.abs().max()) == 0
+    _check(chi2.cpu().numpy()[:, 0], lnl.cpu().numpy()[:, 0], d["ref_chi2"][:, 0], d["ref_lnl"][:, 0],
+           "picslike_tqu")
+
+
+def test_lnl_mixed_config3_sobol_batch():
+    """256 Sobol points of the five-parameter box against the FP64 device path."""
+    from cosmoforge_b200 import engine
+
+    pb = workloads.config3()
+    L = build_layout(pb.params, pb.mask, pb.beam)
+    E = engine.Engine(L)
+    th = workloads.sobol_points(256, seed=1)
+    cl = np.stack([L.smoothed_cl_table(workloads.model_cls(t, L.lmax_signal)) for t in th])
+    N = torch.from_numpy(pb.noise).cuda()
+    g = torch.Generator(device="cuda").manual_seed(0)
+    X = torch.randn((L.n, 2), dtype=torch.float64, device="cuda", generator=g) * 10.0
+    c64, _, l64, i64 = E.lnl(cl, N, X, noise_scale=th[:, 4])
+    cm, _, lm, im = E.lnl(cl, N, X, noise_scale=th[:, 4], precision="mixed")
+    assert int(i64.abs().max()) == 0 and int(im.abs().max()) == 0
+    _check(cm.cpu().numpy(), lm.cpu().numpy(), c64.cpu().numpy(), l64.cpu().numpy(), "config3 sobol")
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_potrf_batch_copies_bitwise_identical(dtype):
+    """Every copy of one matrix in a batch gets the same factor, bit for bit.
+
+    Guards the diagonal-block kernels against intra-CTA races: 192 copies of
+    an n = 520 problem run 1728 diagonal-block factorisations.
+    """
+    from cosmoforge_b200 import _lib
+
+    lib = _lib.lib()
+    n, batch = 520, 192
+    C = _spd_batch(n, 1, 11).to(dtype).repeat(batch, 1, 1).contiguous()
+    info = torch.zeros(batch, dtype=torch.int32, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    if dtype == torch.float32:
+        work = torch.empty(lib.cf_potrf_f32_workspace(n, batch) // 4 + 1, dtype=dtype, device="cuda")
+        rc = lib.cf_potrf_f32(n, C.data_ptr(), n, n * n, batch, work.data_ptr(), info.data_ptr(), st)
+    else:
+        work = torch.empty(lib.cf_potrf_workspace(n, batch) // 8 + 1, dtype=dtype, device="cuda")
+        rc = lib.cf_potrf(n, C.data_ptr(), n, n * n, batch, work.data_ptr(), info.data_ptr(), st)
+    assert rc == 0
+    assert int(info.abs().max()) == 0
+    Lf = torch.tril(C)
+    assert bool((Lf == Lf[:1]).all())
