@@ -21,6 +21,7 @@ CF_ERR_UNSUPPORTED = -4
 CF_ERR_TOO_LARGE = -5
 
 _i, _l, _d, _p, _sz = C.c_int, C.c_long, C.c_double, C.c_void_p, C.c_size_t
+_f = C.c_float
 
 SIGNATURES = {
     "cf_version": (_i, []),
@@ -58,6 +59,16 @@ SIGNATURES = {
     "cf_potrf_f32": (_i, [_i, _p, _l, _l, _i, _p, _p, _p]),
     "cf_axpby_f32": (_i, [_l, _d, _p, _l, _d, _p, _p, _l, _p, _l, _p, _l, _i, _p]),
     "cf_chi2_logdet_mixed": (_i, [_i, _p, _l, _l, _p, _l, _l, _i, _p, _l, _l, _i, _p, _p, _p]),
+    "cf_mlp_dense_fwd": (_i, [_i, _i, _i, _p, _l, _p, _p, _i, _p, _p, _l, _p]),
+    "cf_mlp_dense_bwd_data": (_i, [_i, _i, _i, _p, _p, _p, _p, _p]),
+    "cf_mlp_dense_bwd_weight": (_i, [_i, _i, _i, _p, _p, _l, _p, _p, _p]),
+    "cf_mlp_mse": (_i, [_i, _p, _p, _p, _p, _p, _p]),
+    "cf_mlp_adam": (_i, [_l, _p, _p, _p, _p, _f, _f, _f, _f, _p, _p, _p]),
+    "cf_to_bf16": (_i, [_l, _p, _p, _p]),
+    "cf_mcmc_propose": (_i, [_i, _i, _p, _p, _p, _i, _p, _p, _p, _p, _p, _p, _p, _p]),
+    "cf_mcmc_stage1": (_i, [_i, _i, _p, _p, _d, _d, _p, _p, _p, _p, _p, _p, _p, _i, _p, _p]),
+    "cf_mcmc_stage2": (_i, [_i, _i, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _i, _p, _p, _p]),
+    "cf_mcmc_mh_accept": (_i, [_i, _i, _p, _p, _p, _p, _p, _p, _p, _p, _i, _p, _p, _p]),
 }
 
 _lib = None

@@ -49,14 +49,10 @@ __global__ void __launch_bounds__(256) k_potrf_diag_inv_f32(float* A, long lda, 
         }
         if (tid == 0) piv[j] = sqrtf(d);
         const float inv_d = 1.0f / d;
-        const int m = kb - j - 1;
-        for (int e = tid; e < m * (m + 1) / 2; e += blockDim.x) {
-            int r = (int)((sqrtf(8.0f * e + 1.0f) - 1.0f) * 0.5f);
-            while ((r + 1) * (r + 2) / 2 <= e) ++r;
-            while (r * (r + 1) / 2 > e) --r;
-            const int c = e - r * (r + 1) / 2;
-            const int rr = j + 1 + r, cc = j + 1 + c;
-            S[rr * LDS + cc] -= S[rr * LDS + j] * S[cc * LDS + j] * inv_d;
+        // trailing lower triangle: one warp per row, lanes over columns
+        for (int rr = j + 1 + (tid >> 5); rr < kb; rr += blockDim.x >> 5) {
+            const float srj = S[rr * LDS + j] * inv_d;
+            for (int cc = j + 1 + (tid & 31); cc <= rr; cc += 32) S[rr * LDS + cc] -= srj * S[cc * LDS + j];
         }
         if (j > 0)
             for (int r = j + tid; r < kb; r += blockDim.x) S[r * LDS + j - 1] /= piv[j - 1];
@@ -157,8 +153,20 @@ __global__ void __launch_bounds__(SNT, 2) k_sgemm_nt(int M, int N, int K, float 
         if (kt + 1 < KT) stash(s ^ 1);
         __syncthreads();
     }
-    // 16-byte row segments when the row stride and base allow it
+    // reads of C first (independent loads, one latency), then 16-byte stores
+    // when the row stride and base allow it
     const bool vec = ((ldc & 3) == 0) && ((((uintptr_t)C) & 15) == 0);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int r = tile_m + (i < 4 ? ty * 4 + i : 64 + ty * 4 + i - 4);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int c = tile_n + (j < 4 ? tx * 4 + j : 64 + tx * 4 + j - 4);
+            float v = alpha * acc[i][j];
+            if (beta != 0.0f && r < M && c < N) v += beta * C[(long)r * ldc + c];
+            acc[i][j] = v;
+        }
+    }
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         const int r = tile_m + (i < 4 ? ty * 4 + i : 64 + ty * 4 + i - 4);
@@ -168,24 +176,12 @@ __global__ void __launch_bounds__(SNT, 2) k_sgemm_nt(int M, int N, int K, float 
             const int c0 = tile_n + h * 64 + tx * 4;
             float* pc = C + (long)r * ldc + c0;
             if (vec && c0 + 4 <= N) {
-                float4 o = make_float4(alpha * acc[i][h * 4], alpha * acc[i][h * 4 + 1], alpha * acc[i][h * 4 + 2],
-                                       alpha * acc[i][h * 4 + 3]);
-                if (beta != 0.0f) {
-                    const float4 q = *reinterpret_cast<const float4*>(pc);
-                    o.x += beta * q.x;
-                    o.y += beta * q.y;
-                    o.z += beta * q.z;
-                    o.w += beta * q.w;
-                }
-                *reinterpret_cast<float4*>(pc) = o;
+                *reinterpret_cast<float4*>(pc) =
+                    make_float4(acc[i][h * 4], acc[i][h * 4 + 1], acc[i][h * 4 + 2], acc[i][h * 4 + 3]);
             } else {
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    if (c0 + j >= N) continue;
-                    float v = alpha * acc[i][h * 4 + j];
-                    if (beta != 0.0f) v += beta * pc[j];
-                    pc[j] = v;
-                }
+                for (int j = 0; j < 4; ++j)
+                    if (c0 + j < N) pc[j] = acc[i][h * 4 + j];
             }
         }
     }
@@ -251,20 +247,36 @@ __global__ void __launch_bounds__(CNT) k_chi2_refined(int n, const float* L, lon
     for (int b0 = 0; b0 < n; b0 += 32) {
         const int kb = n - b0 < 32 ? n - b0 : 32;
         if (warp == 0) {
+            // lane i holds row b0 + i of the diagonal block (independent loads)
+            float lrow[32];
+#pragma unroll
+            for (int k = 0; k < 32; ++k) lrow[k] = (lane < kb && k < kb) ? L[(long)(b0 + lane) * lda + b0 + k] : 1.0f;
             double zi = lane < kb ? w[b0 + lane] : 0.0;
-            for (int r = 0; r < kb; ++r) {
-                if (lane == r) zi /= (double)L[(long)(b0 + r) * lda + b0 + r];
-                const double zr = __shfl_sync(0xffffffffu, zi, r);
-                if (lane > r && lane < kb) zi -= (double)L[(long)(b0 + lane) * lda + b0 + r] * zr;
+#pragma unroll
+            for (int r = 0; r < 32; ++r) {
+                if (r < kb) {
+                    if (lane == r) zi /= (double)lrow[r];
+                    const double zr = __shfl_sync(0xffffffffu, zi, r);
+                    if (lane > r) zi -= (double)lrow[r] * zr;
+                }
             }
             if (lane < kb) w[b0 + lane] = zi;
         }
         __syncthreads();
+        // rows below: 8 coalesced row loads in flight per warp, then the reductions
         const double zl = lane < kb ? w[b0 + lane] : 0.0;
-        for (int r = b0 + kb + warp; r < n; r += CNT / 32) {
-            double t = lane < kb ? (double)L[(long)r * lda + b0 + lane] * zl : 0.0;
-            for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-            if (lane == 0) w[r] -= t;
+        for (int r0 = b0 + kb + warp * 8; r0 < n; r0 += (CNT / 32) * 8) {
+            double t[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                t[i] = (r0 + i < n && lane < kb) ? (double)L[(long)(r0 + i) * lda + b0 + lane] * zl : 0.0;
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                for (int o = 16; o; o >>= 1) t[i] += __shfl_xor_sync(0xffffffffu, t[i], o);
+            if (lane == 0)
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+                    if (r0 + i < n) w[r0 + i] -= t[i];
         }
         __syncthreads();
     }

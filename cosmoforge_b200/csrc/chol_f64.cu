@@ -53,14 +53,10 @@ __global__ void __launch_bounds__(256) k_potrf_diag_inv(double* A, long lda, lon
         if (tid == 0) piv[j] = sqrt(d);
         const double inv_d = 1.0 / d;
         // trailing update with the unscaled column j; column j - 1 gets its scaling now
-        const int m = kb - j - 1;
-        for (int e = tid; e < m * (m + 1) / 2; e += blockDim.x) {
-            int r = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
-            while ((r + 1) * (r + 2) / 2 <= e) ++r;
-            while (r * (r + 1) / 2 > e) --r;
-            const int c = e - r * (r + 1) / 2;
-            const int rr = j + 1 + r, cc = j + 1 + c;
-            S[rr * LDS + cc] -= S[rr * LDS + j] * S[cc * LDS + j] * inv_d;
+        // trailing lower triangle: one warp per row, lanes over columns
+        for (int rr = j + 1 + (tid >> 5); rr < kb; rr += blockDim.x >> 5) {
+            const double srj = S[rr * LDS + j] * inv_d;
+            for (int cc = j + 1 + (tid & 31); cc <= rr; cc += 32) S[rr * LDS + cc] -= srj * S[cc * LDS + j];
         }
         if (j > 0)
             for (int r = j + tid; r < kb; r += blockDim.x) S[r * LDS + j - 1] /= piv[j - 1];

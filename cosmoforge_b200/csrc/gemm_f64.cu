@@ -144,6 +144,21 @@ __global__ void __launch_bounds__(NT) k_dgemm(int M, int N, int K, double alpha,
     }
     cp_wait<0>();
 
+    // All reads of C first (independent loads, one latency), then the stores.
+#pragma unroll
+    for (int mi = 0; mi < 8; ++mi) {
+        const int r = tile_m + wm + mi * 8 + (lane >> 2);
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int c = tile_n + wn + ni * 8 + (lane & 3) * 2 + h;
+                double v = alpha * acc[mi][ni][h];
+                if (beta != 0.0 && r < M && c < N) v += beta * C[(long)r * ldc + c];
+                acc[mi][ni][h] = v;
+            }
+        }
+    }
 #pragma unroll
     for (int mi = 0; mi < 8; ++mi) {
         const int r = tile_m + wm + mi * 8 + (lane >> 2);
@@ -154,10 +169,8 @@ __global__ void __launch_bounds__(NT) k_dgemm(int M, int N, int K, double alpha,
             for (int h = 0; h < 2; ++h) {
                 const int c = tile_n + wn + ni * 8 + (lane & 3) * 2 + h;
                 if (c >= N) continue;
-                double v = alpha * acc[mi][ni][h];
-                double* pc = C + (long)r * ldc + c;
-                if (beta != 0.0) v += beta * *pc;
-                *pc = v;
+                const double v = acc[mi][ni][h];
+                C[(long)r * ldc + c] = v;
                 if (CT) CT[(long)c * ldct + r] = v;
             }
         }

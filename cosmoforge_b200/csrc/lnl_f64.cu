@@ -28,20 +28,36 @@ __global__ void __launch_bounds__(NT) k_chi2(int n, const double* L, long lda, l
     for (int b0 = 0; b0 < n; b0 += 32) {
         const int kb = n - b0 < 32 ? n - b0 : 32;
         if (warp == 0) {
+            // lane i holds row b0 + i of the diagonal block (independent loads)
+            double lrow[32];
+#pragma unroll
+            for (int k = 0; k < 32; ++k) lrow[k] = (lane < kb && k < kb) ? L[(long)(b0 + lane) * lda + b0 + k] : 1.0;
             double zi = lane < kb ? z[b0 + lane] : 0.0;
-            for (int r = 0; r < kb; ++r) {
-                if (lane == r) zi /= L[(long)(b0 + r) * lda + b0 + r];
-                const double zr = __shfl_sync(0xffffffffu, zi, r);
-                if (lane > r && lane < kb) zi -= L[(long)(b0 + lane) * lda + b0 + r] * zr;
+#pragma unroll
+            for (int r = 0; r < 32; ++r) {
+                if (r < kb) {
+                    if (lane == r) zi /= lrow[r];
+                    const double zr = __shfl_sync(0xffffffffu, zi, r);
+                    if (lane > r) zi -= lrow[r] * zr;
+                }
             }
             if (lane < kb) z[b0 + lane] = zi;
         }
         __syncthreads();
+        // rows below: 8 coalesced row loads in flight per warp, then the reductions
         const double zl = lane < kb ? z[b0 + lane] : 0.0;
-        for (int r = b0 + kb + warp; r < n; r += NT / 32) {
-            double v = lane < kb ? L[(long)r * lda + b0 + lane] * zl : 0.0;
-            for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) z[r] -= v;
+        for (int r0 = b0 + kb + warp * 8; r0 < n; r0 += (NT / 32) * 8) {
+            double v[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                v[i] = (r0 + i < n && lane < kb) ? L[(long)(r0 + i) * lda + b0 + lane] * zl : 0.0;
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                for (int o = 16; o; o >>= 1) v[i] += __shfl_xor_sync(0xffffffffu, v[i], o);
+            if (lane == 0)
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+                    if (r0 + i < n) z[r0 + i] -= v[i];
         }
         __syncthreads();
     }

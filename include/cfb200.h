@@ -262,6 +262,82 @@ int cf_umma_trace_bf16_mapped(int P1, int P2, int K1, int K2, int nterms, const 
  * Returns the previous value.  No counterpart in the reference. */
 int cf_umma_set_promotion(int kc);
 
+/* ---- Mixed-precision pixel likelihood (FP32 factor, FP64-refined chi2) ---- */
+
+/* Bytes of workspace cf_potrf_f32 needs for `batch` problems of order n. */
+size_t cf_potrf_f32_workspace(int n, int batch);
+
+/* Blocked lower Cholesky in FP32, in place (batch), 64-wide panels with FP32
+ * GEMM updates; info as for cf_potrf.  The factor of the mixed likelihood:
+ * replaces cosmocore/basics/linalg.py:362-406 (cholesky_factor) at FP32. */
+int cf_potrf_f32(int n, float* A, long lda, long strideA, int batch, void* work, int* info, void* stream);
+
+/* Z_b = a X_b + c_b W_b in FP64 (Z may be NULL) plus its FP32 copy Z32_b;
+ * c_b = cvec[b] if cvec else c.  C = S + s N of picslike/picslike.py:301-319
+ * in both precisions. */
+int cf_axpby_f32(long count, double a, const double* X, long strideX, double c, const double* cvec,
+                 const double* W, long strideW, double* Z, long strideZ, float* Z32, long strideZ32,
+                 int batch, void* stream);
+
+/* chi2[b nrhs + m] = 2 |L_b^-1 x|^2 - v^T C_b v, v = (L_b L_b^T)^-1 x: one FP64
+ * refinement step on the FP32 factor L_b of the FP64 C_b (lower triangle
+ * read), second-order accurate; logdet[b] = 2 sum ln (L_b)_ii.  n <= 12288.
+ * Replaces picslike/picslike.py:643-664 and cosmocore/basics/linalg.py:430-474
+ * in the mixed likelihood. */
+int cf_chi2_logdet_mixed(int n, const float* L, long lda, long strideL, const double* C, long ldc,
+                         long strideC, int batch, const double* X, long ldx, long strideX, int nrhs,
+                         double* chi2, double* logdet, void* stream);
+
+/* ---- Emulator network (BF16 weights, FP32 accumulation) and sampler ----
+ * No counterpart in the reference: the MLP emulator of -2 Delta lnL and the
+ * delayed-acceptance Metropolis sampler built on the exact likelihood. */
+
+/* out = act(A W^T + b): A M x K FP32 (lda), W N x K BF16, b N FP32 (or NULL),
+ * act 1 = SiLU, 0 = linear; Z (pre-activation, may be NULL) and out M x N (ldo). */
+int cf_mlp_dense_fwd(int M, int N, int K, const float* A, long lda, const void* W, const float* b,
+                     int act, float* Z, float* out, long ldo, void* stream);
+
+/* dZ_prev = (dZ W) * silu'(Z_prev): dZ M x N, W N x K BF16, Z_prev / dZ_prev M x K. */
+int cf_mlp_dense_bwd_data(int M, int N, int K, const float* dZ, const void* W, const float* Zprev,
+                          float* dZprev, void* stream);
+
+/* dW = dZ^T A_prev (N x K) and db = column sums of dZ (may be NULL). */
+int cf_mlp_dense_bwd_weight(int M, int N, int K, const float* dZ, const float* Aprev, long lda, float* dW,
+                            float* db, void* stream);
+
+/* Weighted MSE sum w (y - t)^2 / sum w (w may be NULL), gradient dy, loss to *loss. */
+int cf_mlp_mse(int M, const float* y, const float* t, const float* w, float* dy, float* loss, void* stream);
+
+/* Adam step over `count` FP32 parameters; *step (device int) is incremented
+ * and sets the bias corrections; p16 (may be NULL) receives the BF16 copy. */
+int cf_mlp_adam(long count, float* p, const float* g, float* m, float* v, float lr, float b1, float b2,
+                float eps, int* step, void* p16, void* stream);
+
+/* y = bf16(x) for count values. */
+int cf_to_bf16(long count, const float* x, void* y, void* stream);
+
+/* Proposal theta_p = theta + Lp xi for chains neither pending nor finished;
+ * xin = theta_p mapped from [lo, hi] to [-1, 1]; active 0 idle / 1 inside /
+ * 2 outside the box. */
+int cf_mcmc_propose(int C, int D, const double* theta, const int* pending, const int* steps, int max_steps,
+                    const double* Lp, const double* xi, const double* lo, const double* hi, double* theta_p,
+                    float* xin, int* active, void* stream);
+
+/* Delayed-acceptance stage 1 (emulator: lnL~ = -(mu + sigma y) / 2). */
+int cf_mcmc_stage1(int C, int D, const int* active, const float* y, double mu, double sigma, const double* u,
+                   const double* theta, double* ltil, double* ltil_p, int* pending, int* steps,
+                   double* samples, int max_steps, int* n_stage1, void* stream);
+
+/* Delayed-acceptance stage 2 (exact lnL of the pending proposals). */
+int cf_mcmc_stage2(int C, int D, const double* lexact_p, double* lexact, double* ltil, const double* ltil_p,
+                   const double* u, double* theta, const double* theta_p, int* pending, int* steps,
+                   double* samples, int max_steps, int* n_exact, int* n_accept, void* stream);
+
+/* Plain exact-likelihood Metropolis acceptance. */
+int cf_mcmc_mh_accept(int C, int D, const int* active, const double* lexact_p, double* lexact, const double* u,
+                      double* theta, const double* theta_p, int* steps, double* samples, int max_steps,
+                      int* n_exact, int* n_accept, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
