@@ -68,6 +68,8 @@ SIGNATURES = {
     "cf_mcmc_propose": (_i, [_i, _i, _p, _p, _p, _i, _p, _p, _p, _p, _p, _p, _p, _p]),
     "cf_mcmc_stage1": (_i, [_i, _i, _p, _p, _d, _d, _p, _p, _p, _p, _p, _p, _p, _i, _p, _p]),
     "cf_mcmc_stage2": (_i, [_i, _i, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _i, _p, _p, _p]),
+    "cf_qform_reduce_f64": (_i, [_i, _i, _l, _p, _l, _p, _l, _l, _i, _d, _p, _l, _i, _p]),
+    "cf_qform_reduce_f32": (_i, [_i, _i, _l, _p, _l, _p, _l, _l, _i, _d, _p, _l, _i, _p]),
     "cf_mcmc_mh_accept": (_i, [_i, _i, _p, _p, _p, _p, _p, _p, _p, _p, _i, _p, _p, _p]),
 }
 

@@ -254,3 +254,32 @@ def patch_problems(n_patches: int = 48, seed: int = 0, nside: int = 16,
         m = (vec @ c > math.cos(radius)).astype(np.float64)
         out.append((m, sigma))
     return out
+
+
+def config2_patches(n_patches: int = 48, seed: int = 0, nside: int = 16, lmax: int = 47,
+                    lmax_signal: int = 64, delta_ell: int = 5) -> list:
+    """Config-2 part 2 as problem instances: TT on each cap of :func:`patch_problems`.
+
+    l = 2..lmax in bins of delta_ell multipoles, fiducial C_l as config 0,
+    Gaussian 4 deg beam (as config 1), white noise sigma^2 per patch.  At
+    nside 16 a cap of radius 10-40 deg holds about 23-360 pixels: too few to
+    separate single multipoles up to l = 47 (the Fisher matrix of 46
+    one-multipole bins is numerically singular on every cap), hence bins of
+    5 multipoles by default.
+    """
+    out = []
+    b = gaussian_beam(4.0, lmax_signal)
+    beam = np.stack([b, b, b])
+    for k, (m, sigma) in enumerate(patch_problems(n_patches, seed, nside, lmax, lmax_signal)):
+        n = int(m.sum())
+        diag = np.full(n, sigma * sigma)
+        out.append(SkyProblem(
+            name=f"config2_patch{k}",
+            params=_params(nside, [0], ["T"], 2, lmax, lmax_signal, 1, delta_ell=delta_ell),
+            mask=m[:, None],
+            cls={"TT": fiducial_tt(lmax_signal)},
+            beam=beam,
+            noise=np.diag(diag),
+            noise_diag=diag,
+        ))
+    return out

@@ -288,6 +288,17 @@ int cf_chi2_logdet_mixed(int n, const float* L, long lda, long strideL, const do
                          long strideC, int batch, const double* X, long ldx, long strideX, int nrhs,
                          double* chi2, double* logdet, void* stream);
 
+/* ---- Quadratic forms of many maps ----
+ * q[m ldq + p0 + b] += scale sum_{j<J} W[(b rows_per_bin + j) ldW + m] Y[(yoff + j) ldY + m]
+ * for b < nb, m < nmaps, with W = D^T Y from one GEMM against the stacked
+ * derivative blocks of a spectrum: q_b(m) = 1/2 y_m^T dC_b y_m for every map
+ * at once.  Replaces the per-bin loop of qube/spectra.py:1124-1186 for many
+ * simulations. */
+int cf_qform_reduce_f64(int nb, int J, long rows_per_bin, const double* W, long ldW, const double* Y, long ldY,
+                        long yoff, int nmaps, double scale, double* q, long ldq, int p0, void* stream);
+int cf_qform_reduce_f32(int nb, int J, long rows_per_bin, const float* W, long ldW, const double* Y, long ldY,
+                        long yoff, int nmaps, double scale, double* q, long ldq, int p0, void* stream);
+
 /* ---- Emulator network (BF16 weights, FP32 accumulation) and sampler ----
  * No counterpart in the reference: the MLP emulator of -2 Delta lnL and the
  * delayed-acceptance Metropolis sampler built on the exact likelihood. */
