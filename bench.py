@@ -4,8 +4,16 @@
 One step = one complete QML solve for one map: signal matrix S, C = S + N,
 C^-1, the 276 x 276 Fisher matrix, raw bandpowers q, noise bias, F^-1 and
 C_hat.  ``value`` is whole-job solves/s with every input already resident in
-HBM; ``e2e`` is the same metric through the drop-in ``Fisher`` / ``Spectra``
-API with host inputs (pinned) copied in and results copied out each step.
+HBM, for the mixed-precision path by default (BF16x6 split products on the
+tensor cores); the same step in plain FP64 is timed in the same run
+(``fp64``) together with the mixed path's error against it.  ``e2e`` is the
+metric through the drop-in ``Fisher`` / ``Spectra`` API with host inputs
+(pinned) copied in and results copied out each step.
+
+Secondary sections of the same line (skipped with ``--no-extra``): the
+batched pixel likelihood (1024 parameter points, FP64 and FP32+refinement),
+the emulator and delayed-acceptance sampler against exact Metropolis, the
+2048-map solves and the 48-patch batch.
 
 ``--impl reference`` times the CPU restatement of the reference algorithm
 (the oracle: C build with OpenMP, LAPACK/OpenBLAS linear algebra) on a
@@ -43,7 +51,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
+    ap.add_argument("--fp64-steps", type=int, default=2,
+                    help="timed FP64 steps beside a mixed headline (0: skip)")
+    ap.add_argument("--no-extra", action="store_true", help="headline only (no secondary sections)")
     ap.add_argument("--scheme", choices=["bf16x3", "bf16x6"], default="bf16x6",
                     help="split-product scheme of the mixed path")
     ap.add_argument("--e2e-steps", type=int, default=2)
@@ -198,6 +209,140 @@ def fp64_peak_tflops(torch):
     return 2 * 8192**3 / best / 1e12
 
 
+def _cuda_ms(torch, fn, reps):
+    """Mean ms of fn() over reps calls, CUDA events on the current stream (one untimed call first)."""
+    fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        out = fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps, out
+
+
+def secondary(args, dev):
+    """Config 3 (batched lnL), config 4 (emulator + delayed acceptance) and config 2 (batched QML)."""
+    import torch
+
+    from cosmoforge_b200 import batch, engine, qube, sampler, workloads
+    from cosmoforge_b200.emulator import MLPEmulator
+    from cosmoforge_b200.layout import build_layout
+
+    out = {}
+    # ---- config 3: pixel likelihood over 1024 Sobol points ----
+    pb = workloads.config3()
+    L = build_layout(pb.params, pb.mask, pb.beam)
+    E = engine.Engine(L, dev)
+    N = torch.from_numpy(pb.noise).to(dev)
+    X = qube.draw_maps(L, pb.cls, N, 1, seed=0, device=dev)
+    T = sampler.ModelTables(L, dev)
+    th = torch.as_tensor(workloads.sobol_points(1024), device=dev)
+    cl = T(th)
+    s = th[:, 4].contiguous()
+    res = {}
+    for prec in ("fp64", "mixed"):
+        ms, r = _cuda_ms(torch, lambda: E.lnl(cl, N, X, noise_scale=s, precision=prec), 3)
+        res[prec] = (ms, r)
+    d = (res["mixed"][1][2] - res["fp64"][1][2]).abs()
+    lnl = {"workload": "config3_tqu_nside8_lnl", "n_pixels": L.n, "points_per_batch": 1024,
+           "fp64_evals_per_s": 1024 / res["fp64"][0] * 1e3, "mixed_evals_per_s": 1024 / res["mixed"][0] * 1e3,
+           "mixed_max_abs_dlnL": float(d.max()), "mixed_form": "FP32 Cholesky, FP64-refined chi2"}
+    if int(os.environ.get("RANK", "0")) == 0 and not args.no_cpu_baseline:
+        from oracle import oracle as orc
+
+        thc = workloads.sobol_points(8, seed=5)
+        xh = X.cpu().numpy()
+        t0 = time.perf_counter()
+        for t in thc:
+            orc.lnl_point(L, workloads.model_cls(t, L.lmax_signal), pb.noise, xh, noise_scale=t[4])
+        dt = time.perf_counter() - t0
+        lnl["cpu_baseline"] = {"value": len(thc) / dt, "unit": "evals/s", "cores": cpu_threads(), "kind": "port",
+                               "sample": f"{len(thc)} points, oracle S build + Jacobi inverse + logdet"}
+    out["lnl"] = lnl
+
+    # ---- config 4: emulator trained on exact evaluations, delayed acceptance ----
+    t0 = time.perf_counter()
+    th_tr, m2 = sampler.training_set(E, T, N, X, 32768, seed=0)
+    torch.cuda.synchronize()
+    t_set = time.perf_counter() - t0
+    emu = MLPEmulator(workloads.THETA_LO, workloads.THETA_HI, seed=0, device=dev)
+    t0 = time.perf_counter()
+    hist = emu.fit(th_tr, m2, steps=3000, batch=1024, lr=1e-3)
+    torch.cuda.synchronize()
+    t_fit = time.perf_counter() - t0
+    F = sampler.fisher_theta(E, T, N, workloads.THETA_CENTRE)
+    prop = sampler.proposal_cov(F)
+    rng = np.random.default_rng(7)
+    pts = np.clip(rng.multivariate_normal(workloads.THETA_CENTRE, prop, 2048), workloads.THETA_LO,
+                  workloads.THETA_HI)
+    ex, _ = sampler.exact_m2lnl(E, T, N, X, pts)
+    em = emu.predict_m2lnl(pts)
+    dd = em - ex
+    rms = float(0.5 * (dd - dd.mean()).pow(2).mean().sqrt())
+    Xq = emu.normalise(pts[:64])
+    emu_ms, _ = _cuda_ms(torch, lambda: emu.predict_std(Xq), 20)
+    ex_ms, _ = _cuda_ms(torch, lambda: sampler.exact_m2lnl(E, T, N, X, pts[:64]), 3)
+    s_da = sampler.Sampler(E, N, X, emulator=emu, prop_cov=prop, seed=1)
+    ch_da, st_da = s_da.run_da(64, 400)
+    s_mh = sampler.Sampler(E, N, X, prop_cov=prop, seed=2)
+    ch_mh, st_mh = s_mh.run_exact_mh(64, 100)
+    ess_da = sampler.effective_sample_size(ch_da.samples.cpu().numpy(), burn=80)
+    ess_mh = sampler.effective_sample_size(ch_mh.samples.cpu().numpy(), burn=20)
+    out["emulator"] = {
+        "workload": "config4_mlp_delayed_acceptance", "chains": 64,
+        "training_points": 32768, "training_set_s": t_set, "fit_steps": 3000, "fit_s": t_fit,
+        "final_loss": hist[-1][1], "rms_dlnL_near_posterior": rms,
+        "emulated_evals_per_s": 64 / emu_ms * 1e3, "exact_evals_per_s_batch64": 64 / ex_ms * 1e3,
+        "da": {"steps": st_da["steps"], "seconds": st_da["seconds"], "steps_per_s": st_da["steps"] / st_da["seconds"],
+               "exact_evals_per_step": st_da["exact_evals"] / st_da["steps"],
+               "stage2_acceptance": st_da["accepted"] / max(st_da["exact_evals"], 1),
+               "min_ess_per_s": float(ess_da.min()) / st_da["seconds"]},
+        "exact_mh": {"steps": st_mh["steps"], "seconds": st_mh["seconds"],
+                     "steps_per_s": st_mh["steps"] / st_mh["seconds"],
+                     "exact_evals_per_step": st_mh["exact_evals"] / st_mh["steps"],
+                     "acceptance": st_mh["accepted"] / st_mh["steps"],
+                     "min_ess_per_s": float(ess_mh.min()) / st_mh["seconds"]},
+    }
+    out["emulator"]["da_over_exact_steps_per_s"] = (out["emulator"]["da"]["steps_per_s"]
+                                                    / out["emulator"]["exact_mh"]["steps_per_s"])
+    del E, ch_da, ch_mh
+
+    # ---- config 2: 2048 map-solves given C, and 48 sky patches ----
+    pb1 = workloads.config1()
+    L1 = build_layout(pb1.params, pb1.mask, pb1.beam)
+    E1 = engine.Engine(L1, dev)
+    N1 = torch.from_numpy(pb1.noise).to(dev)
+    X1 = qube.draw_maps(L1, pb1.cls, N1, 2048, seed=0, device=dev)
+    Cinv = E1.spd_inverse(E1.signal(L1.smoothed_cl_table(pb1.cls)) + N1)
+    part1 = {}
+    for prec in ("mixed", "fp64"):
+        ms, q = _cuda_ms(torch, lambda: batch.map_solves(E1, Cinv, X1, precision=prec), 1)
+        part1[prec] = (ms, q)
+    del Cinv, X1, E1
+    probs = []
+    for j, p in enumerate(workloads.config2_patches()):
+        Lp = build_layout(p.params, p.mask, p.beam)
+        Np = torch.from_numpy(p.noise).to(dev)
+        xp = qube.draw_maps(Lp, p.cls, Np, 1, seed=100 + j, device=dev)
+        probs.append(dict(params=p.params, mask=p.mask, beam=p.beam, cls=p.cls, noise=p.noise, maps=xp.cpu().numpy()))
+    pbat = batch.PatchBatch(probs, dev)
+    pbat.run()
+    ms2, _ = _cuda_ms(torch, pbat.run, 10)
+    qm, qd = part1["mixed"][1], part1["fp64"][1]
+    out["batched"] = {
+        "map_solves": {"workload": "config2_part1_2048_maps", "maps": 2048,
+                       "mixed_per_s": 2048 / part1["mixed"][0] * 1e3, "fp64_per_s": 2048 / part1["fp64"][0] * 1e3,
+                       "mixed_max_rel_dq": float((qm - qd).abs().max() / qd.abs().max())},
+        "patches": {"workload": "config2_part2_48_caps", "problems": 48, "pixels": [min(pbat.ns), max(pbat.ns)],
+                    "bins": pbat.nb, "solves_per_s": 48 / ms2 * 1e3, "ms_per_batch": ms2,
+                    "fisher_not_invertible": int((pbat.info_f != 0).sum()), "precision": "fp64",
+                    "launch": "one CUDA graph replay per batch"},
+    }
+    return out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -233,11 +378,11 @@ def main():
     cl_tab = torch.from_numpy(L.smoothed_cl_table(pb.cls)).to(dev)
     lib = _lib.lib()
 
-    def step():
+    def step(precision=args.precision, full=False):
         S = E.signal(cl_tab)
         C = S.add_(N)
         E.spd_inverse(C)
-        if args.precision == "mixed":
+        if precision == "mixed":
             from cosmoforge_b200 import engine_mixed
 
             F, bias, q = engine_mixed.fisher_qml(E, C, N, X, scheme=args.scheme)
@@ -246,7 +391,8 @@ def main():
         Finv = E.spd_inverse(F.clone())
         if L.remove_nb:
             q = q - bias[None, :]
-        return E.gemm(q, Finv)
+        clhat = E.gemm(q, Finv)
+        return (clhat, F, Finv) if full else clhat
 
     for _ in range(args.warmup):
         step()
@@ -282,6 +428,38 @@ def main():
     k_work = sum(w for _, _, w in recs)
     n_launch = max(len(recs), 1)
     assert bool(torch.isfinite(out).all())
+
+    # ---- the same step in plain FP64, and the mixed path's error against it ----
+    fp64_leg = None
+    if args.precision == "mixed" and args.fp64_steps > 0:
+        ch_m, F_m, _ = step("mixed", full=True)
+        ch_d, F_d, Finv_d = step("fp64", full=True)
+        torch.cuda.synchronize()
+        barrier()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record()
+        for _ in range(args.fp64_steps):
+            step("fp64")
+        s1.record()
+        torch.cuda.synchronize()
+        t64 = s0.elapsed_time(s1) / 1e3
+        tt64 = torch.tensor([t64], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(tt64, op=dist.ReduceOp.MAX)
+        t64 = float(tt64.item())
+        dF = (F_m - F_d).abs()
+        dg = torch.diagonal(F_d)
+        sig = torch.diagonal(Finv_d).sqrt()
+        fp64_leg = {
+            "value": world * args.fp64_steps / t64, "unit": UNIT, "ms_per_step": t64 / args.fp64_steps * 1e3,
+            "steps": args.fp64_steps, "mixed_over_fp64": (world * args.steps / elapsed) / (world * args.fp64_steps / t64),
+            "mixed_error": {
+                "fisher_max_rel_diag": float((torch.diagonal(dF) / dg).max()),
+                "fisher_max_corr_normalised": float((dF / torch.sqrt(torch.outer(dg, dg))).max()),
+                "clhat_max_shift_in_sigma": float(((ch_m - ch_d).abs() / sig[None, :]).max()),
+                "targets": "|dF|/F <= 1e-5, |dC_hat| <= 1e-3 sigma",
+            },
+        }
 
     # ---- end-to-end through the public API, host inputs and outputs ----
     Nh = torch.from_numpy(pb.noise).pin_memory()
@@ -358,7 +536,13 @@ def main():
             "cpu_baseline": cpu,
             "clocks": clocks,
             "gpu_launches": int(launches),
+            "fp64": fp64_leg,
         }
+    if not args.no_extra:
+        extra = secondary(args, dev)
+        if line is not None:
+            line["sections"] = extra
+    if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

@@ -569,8 +569,11 @@ int launch_gemm_kc(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, i
     return CF_OK;
 }
 
-// Promotion interval (k-tiles of 64 per FP32 accumulator): 1, 2, 4, 8 or 16.
+// Promotion interval (k-tiles of 64 per FP32 accumulator): 1, 2, 4, 8, 16 or 32.
 int g_promote_kc = 16;
+// GEMM mode: 1 = all planes of a 32-wide k-slice per stage with split
+// accumulators where the planes allow it, 0 = 64-wide k-tiles term by term.
+int g_all_planes = 1;
 
 template <int BN, int STAGES, bool TRACE, int PLS = 1, int BKT = BK, bool SPLIT = false>
 int launch_gemm(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, int K, const Terms& t,
@@ -582,6 +585,8 @@ int launch_gemm(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, int 
         case 8: return launch_gemm_kc<BN, STAGES, TRACE, 8, PLS, BKT, SPLIT>(ma, mb, M, N, K, t, e, tr, splits, err, st);
         case 16:
             return launch_gemm_kc<BN, STAGES, TRACE, 16, PLS, BKT, SPLIT>(ma, mb, M, N, K, t, e, tr, splits, err, st);
+        case 32:
+            return launch_gemm_kc<BN, STAGES, TRACE, 32, PLS, BKT, SPLIT>(ma, mb, M, N, K, t, e, tr, splits, err, st);
         default: return launch_gemm_kc<BN, STAGES, TRACE, 4, PLS, BKT, SPLIT>(ma, mb, M, N, K, t, e, tr, splits, err, st);
     }
 }
@@ -595,11 +600,19 @@ int cf_umma_trace_impl(int P1, int P2, int K1, int K2, int nterms, const int* ta
 
 // Set the promotion interval of the tensor-core kernels (k-tiles of 64 summed
 // in one FP32 TMEM accumulator before the partial is promoted): 1, 2, 4,
-// 8 or 16 (default).  Returns the previous value.
+// 8, 16 (default) or 32.  Returns the previous value.
 extern "C" int cf_umma_set_promotion(int kc)
 {
     const int prev = g_promote_kc;
-    if (kc == 1 || kc == 2 || kc == 4 || kc == 8 || kc == 16) g_promote_kc = kc;
+    if (kc == 1 || kc == 2 || kc == 4 || kc == 8 || kc == 16 || kc == 32) g_promote_kc = kc;
+    return prev;
+}
+
+// Select the GEMM form (1 = all planes per stage, 0 = term by term); returns the previous one.
+extern "C" int cf_umma_set_all_planes(int on)
+{
+    const int prev = g_all_planes;
+    g_all_planes = on ? 1 : 0;
     return prev;
 }
 
@@ -630,7 +643,7 @@ extern "C" int cf_umma_gemm_bf16(int M, int N, int K, int nterms, const int* ta,
     // k-slice instead of once per term), the leading term (0, 0) accumulated
     // apart from the corrections; otherwise 64-wide k-tiles walked term by term.
     const int pls = a_planes == b_planes ? a_planes : 0;
-    bool all_planes = (pls == 2 || pls == 3) && t.a[0] == 0 && t.b[0] == 0;
+    bool all_planes = g_all_planes && (pls == 2 || pls == 3) && t.a[0] == 0 && t.b[0] == 0;
     for (int i = 1; i < nterms && all_planes; ++i) all_planes = !(t.a[i] == 0 && t.b[i] == 0);
     if (all_planes) {
         int rc = make_map(&ma, A, K, M, lda, a_planes, a_ps, BM, 32);

@@ -142,12 +142,29 @@ def _build_planes(plan: MixedPlan, s: int):
     return blk, {blk.fa: (Dab, R, blk.fb), blk.fb: (Dba, Cc, blk.fa)}
 
 
-def fisher(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6") -> torch.Tensor:
+def default_gemm_forms(L) -> dict:
+    """Per-spectrum form of the A_b GEMM: {spectrum: (all_planes, promotion_kc)}.
+
+    The all-planes form (every plane of a k-slice per pipeline stage, the
+    leading product in its own TMEM accumulator, the five corrections sharing
+    a second one) is the faster one.  On blocks that involve a spin-0 field
+    its errors correlate with the transposed entries of A_b at the lowest
+    multipoles (measured on the TQU nside-16 problem: |dF_bb|/F_bb 1.2e-5 for
+    TT l=2 against 4e-6 term by term), so those spectra run term by term.
+    """
+    forms = {}
+    for s, sp in enumerate(L.spectra):
+        spin0 = any(L.fields[f].spin == 0 for f in (sp.fi, sp.fj))
+        forms[s] = (0, 16) if spin0 else (1, 16)
+    return forms
+
+
+def fisher(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6", forms: dict | None = None) -> torch.Tensor:
     """F (P x P, FP64) on the tensor cores (see _fisher_core)."""
-    return _fisher_core(E, Cinv, scheme)[0]
+    return _fisher_core(E, Cinv, scheme, forms=forms)[0]
 
 
-def _fisher_core(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6", N=None, maps=None):
+def _fisher_core(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6", N=None, maps=None, forms=None):
     """F (P x P, FP64) with the A_b GEMMs and traces on the tensor cores.
 
     A_b is kept for every parameter in one buffer per column segment (field):
@@ -182,7 +199,13 @@ def _fisher_core(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6", N=None, 
         XT[f] = torch.empty((Pl, ncols, npd), dtype=BF16, device=E.dev)
         pmap[f] = torch.tensor([s * nb + b for s in specs for b in range(nb)], dtype=torch.int32,
                                device=E.dev)
+    forms = default_gemm_forms(L) if forms is None else forms
+    prev_ap = E.lib.cf_umma_set_all_planes(1)
+    prev_kc = E.lib.cf_umma_set_promotion(16)
     for s in range(L.nspectra):
+        ap, kc = forms.get(s, (1, 16))
+        E.lib.cf_umma_set_all_planes(ap)
+        E.lib.cf_umma_set_promotion(kc)
         ev = E._probe_begin("build_planes")
         blk, ops = _build_planes(plan, s)
         E._probe_end("build_planes", ev, 0)
@@ -201,6 +224,8 @@ def _fisher_core(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6", N=None, 
             torch.cuda.nvtx.range_pop()
             E._probe_end("a_gemm_mixed", ev, 2.0 * npd * ncol * K * plan.nterms)
         del ops
+    E.lib.cf_umma_set_all_planes(prev_ap)
+    E.lib.cf_umma_set_promotion(prev_kc)
     F = torch.zeros((P, P), dtype=torch.float64, device=E.dev)
     segs = list(X)
     for a, ss in enumerate(segs):
@@ -279,9 +304,9 @@ def _qml_core(plan, E, Cinv, Cp, N, maps, X, pmap, ldseg, segrows, segpad):
 
 
 def fisher_qml(E: Engine, Cinv: torch.Tensor, N: torch.Tensor | None = None,
-               maps: torch.Tensor | None = None, scheme: str = "bf16x6"):
+               maps: torch.Tensor | None = None, scheme: str = "bf16x6", forms: dict | None = None):
     """Mixed F, FP64 bias and q (same return convention as Engine.fisher_qml)."""
-    F, qml = _fisher_core(E, Cinv, scheme, N, maps)
+    F, qml = _fisher_core(E, Cinv, scheme, N, maps, forms=forms)
     bias, q = qml if qml is not None else (None, None)
     if q is not None and N is None:
         bias = None

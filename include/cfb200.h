@@ -262,6 +262,13 @@ int cf_umma_trace_bf16_mapped(int P1, int P2, int K1, int K2, int nterms, const 
  * Returns the previous value.  No counterpart in the reference. */
 int cf_umma_set_promotion(int kc);
 
+/* Form of cf_umma_gemm_bf16: 1 (default) loads every plane of a 32-wide
+ * k-slice into one pipeline stage and keeps the leading product apart from
+ * the corrections in a second TMEM accumulator, when both operands carry the
+ * same 2 or 3 planes; 0 walks 64-wide k-tiles term by term.  Returns the
+ * previous setting.  No counterpart in the reference. */
+int cf_umma_set_all_planes(int on);
+
 /* ---- Mixed-precision pixel likelihood (FP32 factor, FP64-refined chi2) ---- */
 
 /* Bytes of workspace cf_potrf_f32 needs for `batch` problems of order n. */
