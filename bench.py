@@ -394,6 +394,20 @@ def main():
         clhat = E.gemm(q, Finv)
         return (clhat, F, Finv) if full else clhat
 
+    tune_report = None
+    if args.precision == "mixed":
+        # one-time tuning of the A_b GEMM forms on this problem (cached per shape)
+        from cosmoforge_b200 import autotune
+
+        S0 = E.signal(cl_tab)
+        C0 = S0.add_(N)
+        E.spd_inverse(C0)
+        t0 = time.perf_counter()
+        forms, rep = autotune.tune_fisher(E, C0, args.scheme, use_cache=False)
+        torch.cuda.synchronize()
+        tune_report = {"seconds": time.perf_counter() - t0,
+                       "forms": {L.spectra[k].label: {"all_planes": v[0], "kc": v[1]} for k, v in forms.items()}}
+        del S0, C0
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -537,6 +551,7 @@ def main():
             "clocks": clocks,
             "gpu_launches": int(launches),
             "fp64": fp64_leg,
+            "autotune": tune_report,
         }
     if not args.no_extra:
         extra = secondary(args, dev)

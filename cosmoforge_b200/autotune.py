@@ -1,0 +1,187 @@
+"""Autotuner for the mixed-precision Fisher's A_b = C^-1 dC_b products.
+
+For each spectrum it times the candidate forms of the split-product GEMM
+(``cf_umma_gemm_bf16``: all planes of a k-slice per stage with split
+accumulators, or 64-wide k-tiles term by term) and promotion intervals on the
+spectrum's own operands, checks every candidate's accuracy where it matters
+for the Fisher matrix, and keeps the fastest one within tolerance:
+
+* accuracy: for every bin of a small problem, or for the lowest multipoles
+  (where the cancellation in C^-1 dC_b is largest), one in the middle and
+  the last of a large one, the Fisher diagonal
+  F_bb = 1/2 Tr(A_b A_b) is formed in FP64 from the GEMM's output planes
+  (every output segment against the transposed others) and compared with
+  the same trace of an FP64 product;
+* speed: CUDA-event time of the spectrum's GEMMs (second of two runs);
+* choice: the fastest candidate whose error is below ``tol`` or within
+  ``slack`` of the most accurate candidate's (the split-product floor).
+
+Results are cached per (scheme, problem shape, device) in-process and in a
+JSON file (``CFB200_TUNE_CACHE``, default ``~/.cache/cosmoforge_b200/
+tuning.json``) so a problem shape is tuned once per machine.
+"""
+
+from __future__ import annotations
+
+import json
+import os
+from pathlib import Path
+
+import torch
+
+from ._lib import check, stream
+from .engine_mixed import MixedPlan, _build_planes, default_gemm_forms
+
+CANDIDATES = ((1, 16), (1, 8), (0, 16), (0, 32))
+_MEM = {}
+
+
+def _cache_path() -> Path:
+    p = os.environ.get("CFB200_TUNE_CACHE")
+    return Path(p) if p else Path.home() / ".cache" / "cosmoforge_b200" / "tuning.json"
+
+
+def _key(E, scheme: str, tol: float) -> str:
+    L = E.L
+    fields = ",".join(f"{f.spin}:{f.nrows}" for f in L.fields)
+    dev = torch.cuda.get_device_name(E.dev)
+    return f"{scheme}|n{L.n}|{fields}|nb{L.nbins}|L{L.lmax_signal}|tol{tol:g}|{dev}"
+
+
+def _load(key):
+    if key in _MEM:
+        return _MEM[key]
+    try:
+        d = json.loads(_cache_path().read_text())
+        if key in d:
+            _MEM[key] = {int(k): tuple(v) for k, v in d[key]["forms"].items()}
+            return _MEM[key]
+    except (OSError, ValueError, KeyError):
+        pass
+    return None
+
+
+def _store(key, forms, report):
+    _MEM[key] = forms
+    path = _cache_path()
+    try:
+        path.parent.mkdir(parents=True, exist_ok=True)
+        d = json.loads(path.read_text()) if path.exists() else {}
+        d[key] = {"forms": {str(k): list(v) for k, v in forms.items()}, "report": report}
+        path.write_text(json.dumps(d, indent=1))
+    except (OSError, ValueError):
+        pass
+
+
+def _trace_AA(cols, L):
+    """1/2 Tr(A A) from the column blocks {segment: A[:, segment] (n x m_seg, unpadded rows)}."""
+    t = 0.0
+    for s1, A1 in cols.items():
+        f1 = L.fields[s1]
+        for s2, A2 in cols.items():
+            f2 = L.fields[s2]
+            # sum_{k in s2, l in s1} A[k, l] A[l, k]
+            t += float((A1[f2.offset:f2.offset + f2.nrows] * A2[f1.offset:f1.offset + f1.nrows].T).sum())
+    return 0.5 * t
+
+
+def tune_fisher(E, Cinv: torch.Tensor, scheme: str = "bf16x6", tol: float = 6e-6, slack: float = 1.25,
+                candidates=CANDIDATES, probe_bins=None, use_cache: bool = True):
+    """Per-spectrum {s: (all_planes, kc)} for engine_mixed.fisher_qml, and a report."""
+    key = _key(E, scheme, tol)
+    if use_cache:
+        got = _load(key)
+        if got is not None:
+            return got, None
+    L = E.L
+    nb = L.nbins
+    if probe_bins is not None:
+        bins = list(probe_bins)
+    elif L.n <= 2048:  # FP64 references are cheap: check every bin
+        bins = list(range(nb))
+    else:
+        bins = sorted({0, min(1, nb - 1), min(2, nb - 1), nb // 2, nb - 1})
+    plan = MixedPlan(E, scheme)
+    Pl, npd = plan.planes, plan.n_pad
+    Cp = plan.split_cinv(Cinv)
+    lib = E.lib
+    prev_ap = lib.cf_umma_set_all_planes(1)
+    prev_kc = lib.cf_umma_set_promotion(16)
+    forms, report = {}, {}
+    try:
+        for s in range(L.nspectra):
+            blk, ops = _build_planes(plan, s)
+            _, D = E._deriv_blocks(s)
+            refs = {}
+            for b in bins:
+                cols = {}
+                for seg, (B, K, kseg) in ops.items():
+                    f, g = L.fields[seg], L.fields[kseg]
+                    m = f.nrows
+                    if "auto" in D:
+                        blkd = D["auto"][:, b * m:(b + 1) * m]
+                    elif seg == blk.fa:
+                        blkd = D["ba"][:, b * m:(b + 1) * m]
+                    else:
+                        blkd = D["ab"][:, b * m:(b + 1) * m]
+                    cols[seg] = E.gemm(Cinv[:, g.offset:g.offset + g.nrows].contiguous(), blkd.contiguous())
+                refs[b] = _trace_AA(cols, L)
+                del cols
+            del D
+            results = []
+            outs = {seg: (torch.empty((Pl, npd, B.shape[1]), dtype=torch.bfloat16, device=E.dev), B.shape[1] // nb)
+                    for seg, (B, K, kseg) in ops.items()}
+            for ap, kc in candidates:
+                lib.cf_umma_set_all_planes(ap)
+                lib.cf_umma_set_promotion(kc)
+                ms = 0.0
+                for rep in range(2):
+                    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    ev0.record()
+                    for seg, (B, K, kseg) in ops.items():
+                        M, ld = B.shape[1], B.shape[2]
+                        X = outs[seg][0]
+                        check(lib.cf_umma_gemm_bf16(npd, M, K, plan.nterms, plan.ta, plan.tb,
+                                                    Cp.data_ptr() + plan.po[kseg] * 2, npd, npd * npd, Pl,
+                                                    B.data_ptr(), ld, M * ld, Pl, X.data_ptr(), M, npd * M, Pl,
+                                                    None, 0, 0, None, 0, plan.err.data_ptr(), stream()),
+                              "cf_umma_gemm_bf16")
+                    ev1.record()
+                    torch.cuda.synchronize()
+                    ms = ev0.elapsed_time(ev1)
+                err = 0.0
+                for b, ref in refs.items():
+                    cols = {}
+                    for seg, (X, rpb) in outs.items():
+                        m = L.fields[seg].nrows
+                        Xb = sum(X[p, :, b * rpb:b * rpb + m].double() for p in range(Pl))
+                        cols[seg] = torch.cat([Xb[plan.po[fi]:plan.po[fi] + fl.nrows]
+                                               for fi, fl in enumerate(L.fields)])
+                    err = max(err, abs(_trace_AA(cols, L) / ref - 1.0))
+                results.append((ms, err, ap, kc))
+            del outs
+            if int(plan.err.item()) != 0:
+                raise RuntimeError("tensor-core kernel reported a timed-out wait while tuning")
+            floor = min(r[1] for r in results)
+            ok = [r for r in results if r[1] <= max(tol, slack * floor)]
+            best = min(ok)
+            forms[s] = (best[2], best[3])
+            report[L.spectra[s].label] = [{"all_planes": ap, "kc": kc, "ms": round(ms, 3), "err": err}
+                                          for ms, err, ap, kc in results]
+            del ops
+    finally:
+        lib.cf_umma_set_all_planes(prev_ap)
+        lib.cf_umma_set_promotion(prev_kc)
+    _store(key, forms, report)
+    return forms, report
+
+
+def forms_for(E, Cinv, scheme: str = "bf16x6", tune: bool = False, tol: float = 6e-6):
+    """Tuned forms when asked for (or already cached), else the fixed rule."""
+    key = _key(E, scheme, tol)
+    got = _load(key)
+    if got is not None:
+        return got
+    if tune:
+        return tune_fisher(E, Cinv, scheme, tol)[0]
+    return default_gemm_forms(E.L)

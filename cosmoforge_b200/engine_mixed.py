@@ -199,7 +199,10 @@ def _fisher_core(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6", N=None, 
         XT[f] = torch.empty((Pl, ncols, npd), dtype=BF16, device=E.dev)
         pmap[f] = torch.tensor([s * nb + b for s in specs for b in range(nb)], dtype=torch.int32,
                                device=E.dev)
-    forms = default_gemm_forms(L) if forms is None else forms
+    if forms is None:
+        from .autotune import forms_for
+
+        forms = forms_for(E, Cinv, scheme)
     prev_ap = E.lib.cf_umma_set_all_planes(1)
     prev_kc = E.lib.cf_umma_set_promotion(16)
     for s in range(L.nspectra):
