@@ -342,37 +342,57 @@ __global__ void __launch_bounds__(CNT) k_logdet_f32(int n, const float* L, long 
     }
 }
 
-inline size_t potrf_f32_ws(int n) { return (size_t)NB * NB + (size_t)n * NB; }
+inline size_t potrf_f32_ws(int n) { return (size_t)2 * NB * NB + (size_t)n * 2 * NB; }
 
 }  // namespace
 
 extern "C" size_t cf_potrf_f32_workspace(int n, int batch) { return potrf_f32_ws(n) * sizeof(float) * (size_t)batch; }
 
 // Blocked FP32 Cholesky in place (lower factor), batched: per 64-wide panel the
-// diagonal block is factored and inverted by one CTA, L21 = A21 L11^-T and
-// A22 -= L21 L21^T are FP32 GEMMs.  info: int[batch] zeroed by the caller.
+// diagonal block is factored and inverted by one CTA and L21 = A21 L11^-T is an
+// FP32 GEMM; panels go in pairs so the trailing update A22 -= L21 L21^T runs
+// once per 128 columns.  info: int[batch] zeroed by the caller.
 extern "C" int cf_potrf_f32(int n, float* A, long lda, long strideA, int batch, void* work, int* info, void* stream)
 {
     if (n <= 0 || batch < 1 || !A || !work || lda < n) return CF_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     const long ws = (long)potrf_f32_ws(n);
-    float* Di = (float*)work;        // [batch][NB][NB]
-    float* T = Di + (long)NB * NB;   // [batch][n][NB]
-    for (int k0 = 0; k0 < n; k0 += NB) {
-        const int kb = n - k0 < NB ? n - k0 : NB;
-        k_potrf_diag_inv_f32<<<batch, 256, 0, st>>>(A, lda, strideA, k0, kb, Di, ws, info);
+    float* D1 = (float*)work;             // [batch][NB][NB]
+    float* D2 = D1 + (long)NB * NB;       // [batch][NB][NB]
+    float* W = D2 + (long)NB * NB;        // [batch][n][2 NB]
+    constexpr int LDW = 2 * NB;
+    // Panels in pairs with a look-ahead (see cf_potrf): one K = 128 trailing
+    // update per 128 columns.
+    for (int k0 = 0; k0 < n; k0 += 2 * NB) {
+        const int kb1 = n - k0 < NB ? n - k0 : NB;
+        k_potrf_diag_inv_f32<<<batch, 256, 0, st>>>(A, lda, strideA, k0, kb1, D1, ws, info);
         CF_CHECK_LAUNCH();
-        const int rest = n - k0 - kb;
-        if (rest > 0) {
-            float* a21 = A + (long)(k0 + kb) * lda + k0;
-            int rc = sgemm_nt(rest, kb, kb, 1.0f, a21, lda, strideA, Di, kb, ws, 0.0f, T, kb, ws, batch, 0, st);
-            if (rc) return rc;
-            rc = sgemm_nt(rest, rest, kb, -1.0f, T, kb, ws, T, kb, ws, 1.0f, a21 + kb, lda, strideA, batch, 1, st);
-            if (rc) return rc;
-            k_copy2d_f32<<<dim3(cf_cdiv(kb, 32), cf_cdiv(rest, 8), batch), dim3(32, 8), 0, st>>>(rest, kb, T, kb, ws,
-                                                                                                a21, lda, strideA);
-            CF_CHECK_LAUNCH();
-        }
+        const int rest1 = n - k0 - kb1;
+        if (rest1 <= 0) break;
+        float* a21_1 = A + (long)(k0 + kb1) * lda + k0;
+        int rc = sgemm_nt(rest1, kb1, kb1, 1.0f, a21_1, lda, strideA, D1, kb1, ws, 0.0f, W, LDW, ws, batch, 0, st);
+        if (rc) return rc;
+        const int kb2 = rest1 < NB ? rest1 : NB;
+        rc = sgemm_nt(rest1, kb2, kb1, -1.0f, W, LDW, ws, W, LDW, ws, 1.0f, a21_1 + kb1, lda, strideA, batch, 0, st);
+        if (rc) return rc;
+        k_copy2d_f32<<<dim3(cf_cdiv(kb1, 32), cf_cdiv(rest1, 8), batch), dim3(32, 8), 0, st>>>(rest1, kb1, W, LDW, ws,
+                                                                                              a21_1, lda, strideA);
+        CF_CHECK_LAUNCH();
+        const int k1 = k0 + kb1;
+        k_potrf_diag_inv_f32<<<batch, 256, 0, st>>>(A, lda, strideA, k1, kb2, D2, ws, info);
+        CF_CHECK_LAUNCH();
+        const int rest2 = rest1 - kb2;
+        if (rest2 <= 0) break;
+        float* a21_2 = A + (long)(k1 + kb2) * lda + k1;
+        float* W2 = W + (long)kb2 * LDW;
+        rc = sgemm_nt(rest2, kb2, kb2, 1.0f, a21_2, lda, strideA, D2, kb2, ws, 0.0f, W2 + kb1, LDW, ws, batch, 0, st);
+        if (rc) return rc;
+        rc = sgemm_nt(rest2, rest2, kb1 + kb2, -1.0f, W2, LDW, ws, W2, LDW, ws, 1.0f, a21_2 + kb2, lda, strideA, batch,
+                      1, st);
+        if (rc) return rc;
+        k_copy2d_f32<<<dim3(cf_cdiv(kb2, 32), cf_cdiv(rest2, 8), batch), dim3(32, 8), 0, st>>>(
+            rest2, kb2, W2 + kb1, LDW, ws, a21_2, lda, strideA);
+        CF_CHECK_LAUNCH();
     }
     return CF_OK;
 }

@@ -150,17 +150,19 @@ __global__ void k_unscale_mirror(double* A, long lda, long sA, int n, const doub
 
 namespace {
 inline int nblocks(int n) { return (n + NB - 1) / NB; }
-// doubles of potrf workspace per problem: every diagonal-block inverse + one panel
-inline size_t potrf_ws(int n) { return (size_t)nblocks(n) * NB * NB + (size_t)n * NB; }
+// doubles of potrf workspace per problem: every diagonal-block inverse + one
+// double-width panel (two 64-column panels side by side)
+inline size_t potrf_ws(int n) { return (size_t)nblocks(n) * NB * NB + (size_t)n * 2 * NB; }
 }  // namespace
 
 extern "C" size_t cf_potrf_workspace(int n, int batch) { return potrf_ws(n) * sizeof(double) * (size_t)batch; }
 
 // Right-looking blocked Cholesky: per 64-wide panel, the diagonal block is
-// factored (and inverted) by one CTA, the panel below is L21 = A21 L11^-T
-// (DMMA GEMM against the inverted block) and the trailing matrix gets
-// A22 -= L21 L21^T (lower-only DMMA GEMM).  `work` holds
-// cf_potrf_workspace(n, batch) bytes and keeps every L11^-1 for cf_trtri_lower.
+// factored (and inverted) by one CTA and the panel below is L21 = A21 L11^-T
+// (DMMA GEMM against the inverted block); panels go in pairs with a
+// look-ahead so that the trailing update A22 -= L21 L21^T (lower-only DMMA
+// GEMM) runs once per 128 columns.  `work` holds cf_potrf_workspace(n, batch)
+// bytes and keeps every L11^-1 for cf_trtri_lower.
 extern "C" int cf_potrf(int n, double* A, long lda, long strideA, int batch, void* work, int* info, void* stream)
 {
     if (n <= 0 || batch < 1 || !A || !work) return CF_ERR_ARG;
@@ -173,25 +175,56 @@ extern "C" int cf_potrf(int n, double* A, long lda, long strideA, int batch, voi
     }
     const long ws = (long)potrf_ws(n);
     double* Dinv = (double*)work;                   // [batch][nblocks][NB][NB]
-    double* T = Dinv + (long)nblocks(n) * NB * NB;  // [batch][n][NB] (same stride ws)
-    for (int k0 = 0, blk = 0; k0 < n; k0 += NB, ++blk) {
-        const int kb = n - k0 < NB ? n - k0 : NB;
-        double* Di = Dinv + (long)blk * NB * NB;
-        k_potrf_diag_inv<<<batch, 256, DIAG_SMEM, st>>>(A, lda, strideA, k0, kb, Di, ws, info);
+    double* W = Dinv + (long)nblocks(n) * NB * NB;  // [batch][n][2 NB] (same stride ws)
+    constexpr int LDW = 2 * NB;
+    // Two 64-column panels per pass (look-ahead): factor panel 1, update only
+    // panel 2's columns with it, factor panel 2, then one trailing update of
+    // K = 128 with both, so the trailing matrix is read and written once per
+    // 128 columns.
+    int blk = 0;
+    for (int k0 = 0; k0 < n; k0 += 2 * NB) {
+        const int kb1 = n - k0 < NB ? n - k0 : NB;
+        k_potrf_diag_inv<<<batch, 256, DIAG_SMEM, st>>>(A, lda, strideA, k0, kb1, Dinv + (long)blk * NB * NB, ws,
+                                                        info);
         CF_CHECK_LAUNCH();
-        const int rest = n - k0 - kb;
-        if (rest > 0) {
-            double* a21 = A + (long)(k0 + kb) * lda + k0;
-            int rc = cf_dgemm(0, 1, rest, kb, kb, 1.0, a21, lda, strideA, Di, kb, ws, 0.0, T, kb, ws, nullptr, 0,
-                              0, batch, 0, stream);
-            if (rc) return rc;
-            rc = cf_dgemm(0, 1, rest, rest, kb, -1.0, T, kb, ws, T, kb, ws, 1.0, a21 + kb, lda, strideA, nullptr, 0,
-                          0, batch, 1, stream);
-            if (rc) return rc;
-            k_copy2d<<<dim3(cf_cdiv(kb, 32), cf_cdiv(rest, 8), batch), dim3(32, 8), 0, st>>>(rest, kb, T, kb, ws, a21,
-                                                                                            lda, strideA);
-            CF_CHECK_LAUNCH();
-        }
+        const double* D1 = Dinv + (long)blk * NB * NB;
+        ++blk;
+        const int rest1 = n - k0 - kb1;
+        if (rest1 <= 0) break;
+        double* a21_1 = A + (long)(k0 + kb1) * lda + k0;
+        // T1 = A21 L11^-T into W[:, 0:kb1]
+        int rc = cf_dgemm(0, 1, rest1, kb1, kb1, 1.0, a21_1, lda, strideA, D1, kb1, ws, 0.0, W, LDW, ws, nullptr, 0,
+                          0, batch, 0, stream);
+        if (rc) return rc;
+        const int kb2 = rest1 < NB ? rest1 : NB;
+        // panel 2's columns, every row below panel 1: A -= T1 T1[0:kb2]^T
+        rc = cf_dgemm(0, 1, rest1, kb2, kb1, -1.0, W, LDW, ws, W, LDW, ws, 1.0, a21_1 + kb1, lda, strideA, nullptr,
+                      0, 0, batch, 0, stream);
+        if (rc) return rc;
+        k_copy2d<<<dim3(cf_cdiv(kb1, 32), cf_cdiv(rest1, 8), batch), dim3(32, 8), 0, st>>>(rest1, kb1, W, LDW, ws,
+                                                                                          a21_1, lda, strideA);
+        CF_CHECK_LAUNCH();
+        const int k1 = k0 + kb1;
+        k_potrf_diag_inv<<<batch, 256, DIAG_SMEM, st>>>(A, lda, strideA, k1, kb2, Dinv + (long)blk * NB * NB, ws,
+                                                        info);
+        CF_CHECK_LAUNCH();
+        const double* D2 = Dinv + (long)blk * NB * NB;
+        ++blk;
+        const int rest2 = rest1 - kb2;
+        if (rest2 <= 0) break;
+        double* a21_2 = A + (long)(k1 + kb2) * lda + k1;
+        double* W2 = W + (long)kb2 * LDW;  // rows of W at and below the trailing matrix
+        // T2 = A21_2 L22^-T into W[kb2:, kb1:kb1+kb2]
+        rc = cf_dgemm(0, 1, rest2, kb2, kb2, 1.0, a21_2, lda, strideA, D2, kb2, ws, 0.0, W2 + kb1, LDW, ws, nullptr,
+                      0, 0, batch, 0, stream);
+        if (rc) return rc;
+        // trailing update with both panels (kb1 == NB here): A22 -= [T1 T2] [T1 T2]^T, lower tiles
+        rc = cf_dgemm(0, 1, rest2, rest2, kb1 + kb2, -1.0, W2, LDW, ws, W2, LDW, ws, 1.0, a21_2 + kb2, lda, strideA,
+                      nullptr, 0, 0, batch, 1, stream);
+        if (rc) return rc;
+        k_copy2d<<<dim3(cf_cdiv(kb2, 32), cf_cdiv(rest2, 8), batch), dim3(32, 8), 0, st>>>(rest2, kb2, W2 + kb1, LDW,
+                                                                                          ws, a21_2, lda, strideA);
+        CF_CHECK_LAUNCH();
     }
     return CF_OK;
 }
@@ -273,12 +306,12 @@ extern "C" int cf_spd_inverse(int n, double* A, long lda, long strideA, int batc
 // integrations that must not fragment a pool they do not own.  Its workspace
 // (L^-1, the Jacobi scale factors, the diagonal-block inverses and one panel)
 // lives in this file-scope array, which every GPU that loads the library holds
-// until the process exits: 1.18 M doubles = 9.4 MB per device.
+// until the process exits: 1.25 M doubles = 10.0 MB per device.
 #define CF_SPD_STATIC_MAX_N 1024
 static __device__ __align__(256) double g_spd_static_scratch[(size_t)CF_SPD_STATIC_MAX_N * CF_SPD_STATIC_MAX_N +
                                                              CF_SPD_STATIC_MAX_N +
                                                              (size_t)((CF_SPD_STATIC_MAX_N + NB - 1) / NB) * NB * NB +
-                                                             (size_t)CF_SPD_STATIC_MAX_N * NB];
+                                                             (size_t)CF_SPD_STATIC_MAX_N * 2 * NB];
 
 namespace {
 constexpr int kMaxDevices = 64;

@@ -187,7 +187,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
 template <int BN, int STAGES, bool TRACE, int KC, int PLS, int BKT, bool SPLIT>
 __global__ void __launch_bounds__(NTHREADS, 1)
     k_umma_gemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int K,
-                int n_split, Terms terms, EpiArgs epi, TraceArgs tr, int* err)
+                int n_split, Terms terms, EpiArgs epi, TraceArgs tr, int group_m, int* err)
 {
     // Persistent: each CTA walks output tiles blockIdx.x, +gridDim.x, ...; the
     // shared-memory ring, TMEM and all mbarrier phases carry over between
@@ -231,10 +231,19 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     const long n_tiles = (long)n_mt * n_nt * n_split;
     const int nl = TRACE ? (tr.K2 + BKT - 1) / BKT : 1;
     const long kt_total = TRACE ? (long)tr.K1 * nl : (long)((K + BKT - 1) / BKT);
+    // Tile order: groups of group_m row tiles, the column tiles walked inside
+    // a group, so the CTAs running at one time share a few A row panels
+    // (L2-resident across the sweep) instead of touching every one of them.
     auto coords = [&](long tile, int& m0, int& n0, long& t_lo, int& kt) {
-        const int mt = (int)(tile % n_mt);
-        const long rest = tile / n_mt;
-        const int nt = (int)(rest % n_nt), z = (int)(rest / n_nt);
+        const long per_z = (long)n_mt * n_nt;
+        const int z = (int)(tile / per_z);
+        const long t_in = tile % per_z;
+        const int gm_full = group_m < n_mt ? group_m : n_mt;
+        const int g = (int)(t_in / ((long)gm_full * n_nt));
+        const int gm = min(gm_full, n_mt - g * gm_full);
+        const long within = t_in - (long)g * gm_full * n_nt;
+        const int mt = g * gm_full + (int)(within % gm);
+        const int nt = (int)(within / gm);
         m0 = mt * BM;
         n0 = nt * BN;
         t_lo = kt_total * z / n_split;
@@ -545,6 +554,11 @@ int make_map4(CUtensorMap* map, const void* base, long K2, long K1, long rows, i
     return r == CUDA_SUCCESS ? CF_OK : CF_ERR_ARG;
 }
 
+// Promotion interval (k-tiles of 64 per FP32 accumulator): 1, 2, 4, 8, 16 or 32.
+int g_promote_kc = 16;
+// Row tiles per group of the persistent tile order.
+int g_group_m = 16;
+
 template <int BN, int STAGES, bool TRACE, int KC, int PLS = 1, int BKT = BK, bool SPLIT = false>
 int launch_gemm_kc(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, int K, const Terms& t,
                    const EpiArgs& e, const TraceArgs& tr, int splits, int* err, cudaStream_t st)
@@ -564,13 +578,11 @@ int launch_gemm_kc(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, i
     const long tiles = (long)cf_cdiv(M, BM) * cf_cdiv(N, BN) * splits;
     const int grid = (int)(tiles < sms ? tiles : sms);
     k_umma_gemm<BN, STAGES, TRACE, KC, PLS, BKT, SPLIT><<<grid, NTHREADS, smem, st>>>(ma, mb, K, splits, t, e, tr,
-                                                                                     err);
+                                                                                     g_group_m, err);
     CF_CHECK_LAUNCH();
     return CF_OK;
 }
 
-// Promotion interval (k-tiles of 64 per FP32 accumulator): 1, 2, 4, 8, 16 or 32.
-int g_promote_kc = 16;
 // GEMM mode: 1 = all planes of a 32-wide k-slice per stage with split
 // accumulators where the planes allow it, 0 = 64-wide k-tiles term by term.
 int g_all_planes = 1;
@@ -605,6 +617,14 @@ extern "C" int cf_umma_set_promotion(int kc)
 {
     const int prev = g_promote_kc;
     if (kc == 1 || kc == 2 || kc == 4 || kc == 8 || kc == 16 || kc == 32) g_promote_kc = kc;
+    return prev;
+}
+
+// Row tiles per group of the persistent tile order (>= 1); returns the previous value.
+extern "C" int cf_umma_set_group(int group_m)
+{
+    const int prev = g_group_m;
+    if (group_m >= 1) g_group_m = group_m;
     return prev;
 }
 

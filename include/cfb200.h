@@ -128,7 +128,7 @@ int cf_spd_inverse(int n, double* A, long lda, long strideA, int batch, void* wo
 /*
  * Allocation-free SPD inverse: cf_spd_inverse for one n x n matrix with its
  * workspace taken from a scratch array compiled into the library (a
- * file-scope __device__ array of 1.18 M doubles, 9.4 MB held by every
+ * file-scope __device__ array of 1.25 M doubles, 10.0 MB held by every
  * GPU that loads the library until exit), for callers that cannot call
  * cudaMalloc (host callbacks, allocator hooks, plugins whose host owns the
  * memory pool).  Allocates nothing.  n > cf_spd_inverse_static_max_n()
@@ -268,6 +268,12 @@ int cf_umma_set_promotion(int kc);
  * same 2 or 3 planes; 0 walks 64-wide k-tiles term by term.  Returns the
  * previous setting.  No counterpart in the reference. */
 int cf_umma_set_all_planes(int on);
+
+/* Row tiles per group in the persistent tile order of the tcgen05 kernels
+ * (default 16): the CTAs running at one time share group_m A row panels,
+ * which stay in L2 while the group's column tiles are swept.  Returns the
+ * previous value.  No counterpart in the reference. */
+int cf_umma_set_group(int group_m);
 
 /* ---- Mixed-precision pixel likelihood (FP32 factor, FP64-refined chi2) ---- */
 
