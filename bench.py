@@ -309,6 +309,21 @@ def secondary(args, dev):
                                                     / out["emulator"]["exact_mh"]["steps_per_s"])
     del E, ch_da, ch_mh
 
+    # ---- bandpower window function on config 1 binned by 5 multipoles ----
+    pbw = workloads.config1()
+    bw = {"workload": "config1_bandpower_window_dl5", "precision": "mixed"}
+    fw = qube.Fisher(pbw.params | {"delta_ell": 5}, basis=False, mask=pbw.mask, noise_cov1=pbw.noise,
+                     cls_data=pbw.cls, beam=pbw.beam, precision="mixed", device=dev)
+    fw.run()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    Wbp = fw.get_bandpower_window_function()
+    torch.cuda.synchronize()
+    bw.update(seconds=time.perf_counter() - t0, shape=list(Wbp.shape),
+              row_sum_max_dev=float(np.max(np.abs(Wbp.reshape(6, fw.layout.nbins, 6, -1).sum(axis=(2, 3)) - 1.0))))
+    out["bandpower"] = bw
+    del fw, Wbp
+
     # ---- config 2: 2048 map-solves given C, and 48 sky patches ----
     pb1 = workloads.config1()
     L1 = build_layout(pb1.params, pb1.mask, pb1.beam)

@@ -202,6 +202,76 @@ class Fisher(_Base):
             return None
         return self.layout.bandpower_slices()
 
+    def set_binning(self, bins) -> None:
+        """Bins for the next run() (any object with ``lmins`` / ``lmaxs``; CC/core.py:1295-1326)."""
+        self.params.bin_lmins = [int(v) for v in bins.lmins]
+        self.params.bin_lmaxs = [int(v) for v in bins.lmaxs]
+        self._bandpower_window = None
+
+    def _compute_per_ell_fisher(self) -> torch.Tensor:
+        """Fisher matrix with one bin per multipole, lmin..lmax, on the same C^-1.
+
+        The reference re-runs its compute phase with Bins.fromdeltal(lmin, lmax, 1)
+        (qube/fisher.py:1236-1268); the covariance does not depend on the binning,
+        so the resident C^-1 is reused and only the derivatives change.
+        """
+        p = dict(vars(self.params))
+        p.pop("bin_lmins", None)
+        p.pop("bin_lmaxs", None)
+        p["delta_ell"] = 1
+        L1 = _layout(p, self._mask, self._beam)
+        E1 = eng.Engine(L1, self.device)
+        if self.precision == "mixed":
+            from . import engine_mixed
+
+            return engine_mixed.fisher(E1, self._dev_Cinv)
+        return E1.fisher_qml(self._dev_Cinv)[0]
+
+    def get_bandpower_window_function(self, per_ell_fisher=None):
+        """W = F_b^-1 Q F_perell, (nspectra nbins) x (nspectra n_ell) (qube/fisher.py:1050-1190).
+
+        Q sums the multipoles of each bin; both Fisher matrices are spectrum-major.
+        The per-multipole Fisher is computed on demand (and cached) unless given.
+        """
+        if self.fisher is None:
+            raise ValueError("Bandpower window requires a completed Fisher run. Call run() first.")
+        if per_ell_fisher is None and getattr(self, "_bandpower_window", None) is not None:
+            return self._bandpower_window
+        L = self.layout
+        lmin, lmax = int(self.params.lmin), int(self.params.lmax)
+        n_ell = lmax - lmin + 1
+        if per_ell_fisher is None:
+            Fpe = self._compute_per_ell_fisher()
+        else:
+            Fpe = torch.as_tensor(np.asarray(per_ell_fisher, dtype=np.float64), device=self.device)
+        Qb = np.zeros((L.nbins, n_ell))
+        for b, (lo, hi) in enumerate(zip(L.bin_lmins, L.bin_lmaxs)):
+            Qb[b, lo - lmin: hi - lmin + 1] = 1.0
+        Q = torch.as_tensor(np.kron(np.eye(L.nspectra), Qb), device=self.device).contiguous()
+        E = self.engine
+        QF = E.gemm(Q, Fpe.contiguous())
+        Finv = E.spd_inverse(self._dev_F.clone())
+        W = E.gemm(Finv, QF).cpu().numpy()
+        if per_ell_fisher is None:
+            self._bandpower_window = W
+        return W
+
+    def get_effective_ells(self):
+        """Per bin, the window-weighted multipole sum_l W[b,l] l / sum_l W[b,l] (qube/fisher.py:1192-1234)."""
+        if self.fisher is None:
+            raise ValueError("get_effective_ells requires a completed Fisher run. Call run() first.")
+        W = self.get_bandpower_window_function()
+        L = self.layout
+        lmin = int(self.params.lmin)
+        n_ell = int(self.params.lmax) - lmin + 1
+        ells = np.arange(lmin, lmin + n_ell, dtype=np.float64)
+        nb = L.nbins
+        eff = np.empty(L.nspectra * nb)
+        for s in range(L.nspectra):
+            Wb = W[s * nb:(s + 1) * nb, s * n_ell:(s + 1) * n_ell]
+            eff[s * nb:(s + 1) * nb] = (Wb @ ells) / Wb.sum(axis=1)
+        return eff
+
     def get_fisher_block(self, label_i: str, label_j: str | None = None):
         F = self.get_fisher_matrix()
         sl = self.get_bandpower_slices()

@@ -129,6 +129,7 @@ def _params_arrays(params):
         "p_lmax_signal": params["lmax_signal"],
         "p_output_convention": params.get("output_convention", "Cl"),
         "p_remove_nb": int(params.get("remove_nb", True)),
+        "p_delta_ell": int(params.get("delta_ell", 1)),
     }
 
 
@@ -302,6 +303,37 @@ def case_tqu_cut():
     _save("tqu_cut_nside4", **out)
 
 
+def _bandpower(params, mask, noise, cls, beam):
+    """Reference Fisher with its bandpower window function and effective multipoles."""
+    from qube import Fisher
+
+    f = Fisher(params, basis=False, mask=mask, noise_cov1=noise, cls_data=cls, beam=beam)
+    f.run()
+    W = f.get_bandpower_window_function()
+    eff = f.get_effective_ells()
+    return f, W, eff
+
+
+def case_bandpower_tt():
+    """Bandpower window of the config-0 TT problem binned by 3 multipoles (l = 2..24)."""
+    pb = workloads.config0()
+    params = pb.params | {"delta_ell": 3}
+    f, W, eff = _bandpower(params, pb.mask, pb.noise, pb.cls, pb.beam)
+    _save("bandpower_tt_nside8", mask=pb.mask, noise_diag=pb.noise_diag, beam=pb.beam,
+          **_cls_arrays(pb.cls), **_params_arrays(params), ref_fisher=f.get_fisher_matrix(),
+          ref_window=W, ref_eff_ells=eff, spectra_labels=np.array(_spectra_labels(f)))
+
+
+def case_bandpower_tqu():
+    """Bandpower window of the cut-sky TQU case binned by 3 multipoles (l = 2..10)."""
+    pb = workloads.config1(seed=3, nside=4, lmax=10, lmax_signal=16, n_lowrank=8)
+    params = pb.params | {"delta_ell": 3}
+    f, W, eff = _bandpower(params, pb.mask, pb.noise, pb.cls, pb.beam)
+    _save("bandpower_tqu_cut_nside4", mask=pb.mask, noise=pb.noise, beam=pb.beam,
+          **_cls_arrays(pb.cls), **_params_arrays(params), ref_fisher=f.get_fisher_matrix(),
+          ref_window=W, ref_eff_ells=eff, spectra_labels=np.array(_spectra_labels(f)))
+
+
 def _picslike_points(params, mask, noise, beam, maps, fid_cls, point_cls):
     """Run the reference PICSLike over explicit per-point spectra."""
     from picslike import PICSLike
@@ -404,6 +436,8 @@ CASES = {
     "tqu_cut": case_tqu_cut,
     "fortran_picslike": case_fortran_picslike_nside8,
     "picslike_tqu": case_picslike_tqu,
+    "bandpower_tt": case_bandpower_tt,
+    "bandpower_tqu": case_bandpower_tqu,
 }
 
 if __name__ == "__main__":

@@ -18,7 +18,8 @@ def params_of(d: dict) -> dict:
     return dict(
         nside=int(d["p_nside"]), spins=[int(s) for s in d["p_spins"]],
         labels=[str(s) for s in d["p_labels"]], lmin=int(d["p_lmin"]), lmax=int(d["p_lmax"]),
-        lmax_signal=int(d["p_lmax_signal"]), delta_ell=1, ordering="RING",
+        lmax_signal=int(d["p_lmax_signal"]),
+        delta_ell=int(d["p_delta_ell"]) if "p_delta_ell" in d else 1, ordering="RING",
         nsims=int(d["maps"].shape[1]) if "maps" in d else 1,
         remove_nb=bool(int(d["p_remove_nb"])),
         output_convention=str(d["p_output_convention"]), feedback=0,
