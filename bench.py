@@ -319,8 +319,14 @@ def secondary(args, dev):
     t0 = time.perf_counter()
     Wbp = fw.get_bandpower_window_function()
     torch.cuda.synchronize()
+    Lw = fw.layout
+    lmin_w, n_ell_w = int(fw.params.lmin), int(fw.params.lmax) - int(fw.params.lmin) + 1
+    Qw = np.zeros((Lw.nbins, n_ell_w))
+    for b, (lo, hi) in enumerate(zip(Lw.bin_lmins, Lw.bin_lmaxs)):
+        Qw[b, lo - lmin_w: hi - lmin_w + 1] = 1.0
+    Qw = np.kron(np.eye(Lw.nspectra), Qw)
     bw.update(seconds=time.perf_counter() - t0, shape=list(Wbp.shape),
-              row_sum_max_dev=float(np.max(np.abs(Wbp.reshape(6, fw.layout.nbins, 6, -1).sum(axis=(2, 3)) - 1.0))))
+              max_abs_WQt_minus_I=float(np.max(np.abs(Wbp @ Qw.T - np.eye(Qw.shape[0])))))
     out["bandpower"] = bw
     del fw, Wbp
 
