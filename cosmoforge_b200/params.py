@@ -2,8 +2,10 @@
 
 Mirrors the subset of ``cosmocore/settings.py`` (``InputParams`` defaults at
 178-253, label expansion at 451-507) that the pixel-space QML / Fisher /
-likelihood path reads.  File-path parameters are accepted and ignored: this
-package takes every input through the in-memory seams.
+likelihood path reads.  File-path parameters (``maskfile``, ``covmatfile1``,
+``load_reduced``, ``inputclfile``, ``beam_file``, ``inputmapfile1``) are read by
+``fileio`` when the matching array is not injected; output-file parameters are
+ignored.
 """
 
 from __future__ import annotations

@@ -58,9 +58,9 @@ class PICSLike(_Base):
         _check_basis(basis)
         super().__init__(params, params_file, mask, noise_cov1, noise_cov2, cls_data, fiducial_cls,
                          beam, precision, device, kwargs)
-        if maps1 is None:
-            raise NotImplementedError("inject maps1 (file inputs unsupported)")
-        self._maps_in = maps1
+        if maps1 is None and not getattr(self.params, "inputmapfile1", None):
+            raise ValueError("no maps: inject maps1= or set params.inputmapfile1")
+        self._maps_in = maps1  # None: read from inputmapfile1 once the layout is known
         if isinstance(parameter_grid, tuple):
             parameter_grid = _ListGrid(*parameter_grid)
         self.parameter_grid = parameter_grid
@@ -72,6 +72,10 @@ class PICSLike(_Base):
     def setup(self):
         self._setup()
         self.engine = eng.Engine(self.layout, self.device)
+        if self._maps_in is None:
+            from .qube import _read_maps_file
+
+            self._maps_in = _read_maps_file(self)
         X = self._maps_in
         if isinstance(X, torch.Tensor):
             X = X.to(self.device, torch.float64)

@@ -11,8 +11,11 @@ when those attributes are read.
 
 Supported: the pixel-space estimator (``basis=False`` / ``"pixel"``; the
 default ``None`` is served by the same exact pixel path), SYMMETRIC spectra,
-auto-spectra (``do_cross=False``), injected arrays.  The harmonic / compressed
-bases, pixel filters and file inputs raise ``NotImplementedError``.
+auto-spectra (``do_cross=False``), injected arrays or the reference's file
+inputs (``maskfile``, ``covmatfile1`` / ``load_reduced``, ``inputclfile``,
+``smoothing_type`` file / gaussian / none with ``beam_file`` / ``fwhmarcmin``,
+``inputmapfile1``; ``fileio``).  The harmonic / compressed bases and pixel
+filters raise ``NotImplementedError``.
 
 ``precision``: ``"fp64"`` (plain FP64 everywhere) or ``"mixed"`` (BF16x3 /
 FP32 tensor-core traces with FP64 refinement, see ``engine_mixed``).
@@ -24,6 +27,7 @@ import numpy as np
 import torch
 
 from . import engine as eng
+from . import fileio
 from . import layout as lay
 from . import params as prm
 
@@ -70,10 +74,28 @@ class _Base:
         _check_kwargs(kwargs)
         if self.params.do_cross:
             raise NotImplementedError("do_cross=True (two-map cross spectra) is not supported")
-        if mask is None or noise_cov1 is None or (cls_data is None and fiducial_cls is None):
-            raise NotImplementedError("inject mask, noise_cov1 and cls_data (file inputs unsupported)")
+        p = self.params
+        ncomp = sum(1 if s == 0 else 2 for s in p.spins)
+        if mask is None:  # file adapter of cosmocore/core.py:403-472
+            mf = getattr(p, "maskfile", None)
+            if not mf:
+                raise ValueError("no mask: inject mask= or set params.maskfile")
+            mask = fileio.read_mask(str(mf), ncomp, str(getattr(p, "ordering", "RING")))
+        if cls_data is None and fiducial_cls is None:
+            cf = getattr(p, "inputclfile", None) or getattr(p, "fiducialfile", None)
+            if not cf:
+                raise ValueError("no spectra: inject cls_data= or set params.inputclfile")
+            cls_data = fileio.read_cls(str(cf), self.lmax_signal, getattr(p, "input_convention", "Cl"))
+        if beam is None:
+            kind = str(getattr(p, "smoothing_type", "none")).lower()
+            if kind in ("file", "gaussian"):
+                beam = fileio.read_beam(p, self.lmax_signal)
+            elif kind != "none":
+                raise NotImplementedError(f"smoothing_type={kind!r} without an injected beam")
+        if noise_cov1 is None and not getattr(p, "covmatfile1", None):
+            raise ValueError("no noise covariance: inject noise_cov1= or set params.covmatfile1")
         self._mask = mask
-        self._noise_in = noise_cov1
+        self._noise_in = noise_cov1  # None: read from covmatfile1 once the layout is known
         self._cls = cls_data if cls_data is not None else fiducial_cls
         self._beam = beam
         if precision not in ("fp64", "mixed"):
@@ -93,6 +115,13 @@ class _Base:
         self.layout = _layout(p, self._mask, self._beam)
         L = self.layout
         n = L.n
+        if self._noise_in is None:  # cosmocore/core.py:577-700
+            path = str(self.params.covmatfile1)
+            if getattr(self.params, "load_reduced", False):
+                self._noise_in = fileio.read_covmat_reduced(path, n)
+            else:
+                ncomp = sum(1 if f.spin == 0 else 2 for f in L.fields)
+                self._noise_in = fileio.read_covmat(path, 12 * L.nside ** 2, ncomp, fileio.active_indices(L))
         N = self._noise_in
         if isinstance(N, torch.Tensor):
             if tuple(N.shape) != (n, n):
@@ -108,6 +137,25 @@ class _Base:
         self.beam_smoothing = L.beam_smoothing_vector()
         self.n_params = L.n_params
         self.bins = lay_bins(L)
+
+
+def _read_maps_file(obj):
+    """Maps from params.inputmapfile1 (file adapter of cosmocore/core.py:700-716)."""
+    p, L = obj.params, obj.layout
+    phys = getattr(p, "physical_labels", None)
+    if not phys:
+        phys = []
+        k = 0
+        for f in L.fields:
+            if f.spin == 0:
+                phys.append(str(p.labels[k]))
+                k += 1
+            else:
+                phys += ["Q", "U"]
+                k += 2
+    pixact = [f.pixels for f in L.fields for _ in range(1 if f.spin == 0 else 2)]
+    nsims = int(getattr(p, "nsims", None) or 1)
+    return fileio.read_maps(str(p.inputmapfile1), pixact, list(phys), nsims)
 
 
 class lay_bins:
@@ -310,9 +358,9 @@ class Spectra(_Base):
             self.fisher_instance = None
         super().__init__(params, params_file, mask, noise_cov1, noise_cov2, cls_data, fiducial_cls,
                          beam, precision or "fp64", device, kwargs)
-        if maps1 is None:
-            raise NotImplementedError("inject maps1 (file inputs unsupported)")
-        self._maps_in = maps1
+        if maps1 is None and not getattr(self.params, "inputmapfile1", None):
+            raise ValueError("no maps: inject maps1= or set params.inputmapfile1")
+        self._maps_in = maps1  # None: read from inputmapfile1 once the layout is known
         self.qml_results = None
         self.qml_noise_bias = None
         self.invfisher = None
@@ -338,6 +386,8 @@ class Spectra(_Base):
         self.beam_smoothing = f.beam_smoothing
         self.bins = f.bins
         self.n_params = L.n_params
+        if self._maps_in is None:
+            self._maps_in = _read_maps_file(self)
         maps = self._maps_in
         if isinstance(maps, torch.Tensor):
             X = maps.to(self.device, torch.float64)
