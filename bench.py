@@ -19,7 +19,7 @@ the emulator and delayed-acceptance sampler against exact Metropolis, the
 (the oracle: C build with OpenMP, LAPACK/OpenBLAS linear algebra) on a
 bounded sample of the same problem and extrapolates it to a full solve.
 
-Multi-GPU (``torchrun``): the path does not shard (north_star: one GPU per
+Multi-GPU (``torchrun``): the path does not shard (one GPU per
 problem), so N GPUs run N independent replicas; time is the max over ranks.
 """
 
@@ -59,6 +59,8 @@ def parse():
                     help="split-product scheme of the mixed path")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sub-steps", type=int, default=128,
+                    help="emulator Metropolis steps per exact evaluation in the two-level sampler")
     ap.add_argument("--lmax", type=int, default=None,
                     help="override the inference lmax (smaller profiling case; not a bench line)")
     return ap.parse_args()
@@ -286,10 +288,13 @@ def secondary(args, dev):
     ex_ms, _ = _cuda_ms(torch, lambda: sampler.exact_m2lnl(E, T, N, X, pts[:64]), 3)
     s_da = sampler.Sampler(E, N, X, emulator=emu, prop_cov=prop, seed=1)
     ch_da, st_da = s_da.run_da(64, 400)
+    s_sub = sampler.Sampler(E, N, X, emulator=emu, prop_cov=prop, seed=3)
+    ch_sub, st_sub = s_sub.run_da_subchain(64, 200, sub_steps=args.sub_steps)
     s_mh = sampler.Sampler(E, N, X, prop_cov=prop, seed=2)
-    ch_mh, st_mh = s_mh.run_exact_mh(64, 100)
+    ch_mh, st_mh = s_mh.run_exact_mh(64, 300)
     ess_da = sampler.effective_sample_size(ch_da.samples.cpu().numpy(), burn=80)
-    ess_mh = sampler.effective_sample_size(ch_mh.samples.cpu().numpy(), burn=20)
+    ess_sub = sampler.effective_sample_size(ch_sub.samples.cpu().numpy(), burn=20)
+    ess_mh = sampler.effective_sample_size(ch_mh.samples.cpu().numpy(), burn=50)
     out["emulator"] = {
         "workload": "config4_mlp_delayed_acceptance", "chains": 64,
         "training_points": 32768, "training_set_s": t_set, "fit_steps": 3000, "fit_s": t_fit,
@@ -299,15 +304,30 @@ def secondary(args, dev):
                "exact_evals_per_step": st_da["exact_evals"] / st_da["steps"],
                "stage2_acceptance": st_da["accepted"] / max(st_da["exact_evals"], 1),
                "min_ess_per_s": float(ess_da.min()) / st_da["seconds"]},
+        "da_two_level": {"sub_steps": st_sub["sub_steps"], "steps": st_sub["steps"], "seconds": st_sub["seconds"],
+                         "steps_per_s": st_sub["steps"] / st_sub["seconds"],
+                         "emulator_steps_per_s": st_sub["steps"] * st_sub["sub_steps"] / st_sub["seconds"],
+                         "exact_evals_per_step": st_sub["exact_evals"] / st_sub["steps"],
+                         "sub_chain_acceptance": st_sub["sub_accepted"] / (st_sub["steps"] * st_sub["sub_steps"]),
+                         "stage2_acceptance": st_sub["accepted"] / max(st_sub["exact_evals"], 1),
+                         "min_ess": float(ess_sub.min()),
+                         "min_ess_per_s": float(ess_sub.min()) / st_sub["seconds"],
+                         "exact_evals_per_ess": st_sub["exact_evals"] / float(ess_sub.min())},
         "exact_mh": {"steps": st_mh["steps"], "seconds": st_mh["seconds"],
                      "steps_per_s": st_mh["steps"] / st_mh["seconds"],
                      "exact_evals_per_step": st_mh["exact_evals"] / st_mh["steps"],
                      "acceptance": st_mh["accepted"] / st_mh["steps"],
-                     "min_ess_per_s": float(ess_mh.min()) / st_mh["seconds"]},
+                     "min_ess": float(ess_mh.min()),
+                     "min_ess_per_s": float(ess_mh.min()) / st_mh["seconds"],
+                     "exact_evals_per_ess": st_mh["exact_evals"] / float(ess_mh.min())},
     }
-    out["emulator"]["da_over_exact_steps_per_s"] = (out["emulator"]["da"]["steps_per_s"]
-                                                    / out["emulator"]["exact_mh"]["steps_per_s"])
-    del E, ch_da, ch_mh
+    em_ = out["emulator"]
+    em_["da_over_exact_steps_per_s"] = em_["da"]["steps_per_s"] / em_["exact_mh"]["steps_per_s"]
+    em_["da_over_exact_ess_per_s"] = em_["da"]["min_ess_per_s"] / em_["exact_mh"]["min_ess_per_s"]
+    em_["two_level_over_exact_ess_per_s"] = em_["da_two_level"]["min_ess_per_s"] / em_["exact_mh"]["min_ess_per_s"]
+    em_["two_level_exact_evals_saved"] = (em_["exact_mh"]["exact_evals_per_ess"]
+                                          / em_["da_two_level"]["exact_evals_per_ess"])
+    del E, ch_da, ch_mh, ch_sub
 
     # ---- bandpower window function on config 1 binned by 5 multipoles ----
     pbw = workloads.config1()

@@ -73,6 +73,10 @@ SIGNATURES = {
     "cf_qform_reduce_f64": (_i, [_i, _i, _l, _p, _l, _p, _l, _l, _i, _d, _p, _l, _i, _p]),
     "cf_qform_reduce_f32": (_i, [_i, _i, _l, _p, _l, _p, _l, _l, _i, _d, _p, _l, _i, _p]),
     "cf_mcmc_mh_accept": (_i, [_i, _i, _p, _p, _p, _p, _p, _p, _p, _p, _i, _p, _p, _p]),
+    "cf_mcmc_sub_accept": (_i, [_i, _i, _p, _p, _d, _d, _p, _p, _p, _p, _p, _p]),
+    "cf_mcmc_sub_final": (_i, [_i, _i, _p, _p, _p, _p, _p, _p, _p, _p, _p, _i, _p, _p, _p]),
+    "cf_mcmc_subchain": (_i, [_i, _i, _i, _i, _p, _p, _i, _p, _p, _p, _p, _p, _p, _p, _d, _d, _p, _p, _p, _p,
+                              _p]),
 }
 
 _lib = None

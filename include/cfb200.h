@@ -362,6 +362,33 @@ int cf_mcmc_mh_accept(int C, int D, const int* active, const double* lexact_p, d
                       double* theta, const double* theta_p, int* steps, double* samples, int max_steps,
                       int* n_exact, int* n_accept, void* stream);
 
+/* Two-level delayed acceptance, emulator sub-chain step: chains with
+ * active == 1 move theta_s to theta_p with probability
+ * min(1, exp(lnL~(theta_p) - ltil_s)) (lnL~ = -(mu + sigma y) / 2). */
+int cf_mcmc_sub_accept(int C, int D, const int* active, const float* y, double mu, double sigma, const double* u,
+                       const double* theta_p, double* theta_s, double* ltil_s, int* n_sub_accept, void* stream);
+
+/* Two-level delayed acceptance, exact stage: the sub-chain end point theta_s
+ * (exact lnL lexact_p) replaces theta with probability
+ * min(1, exp([lexact_p - lexact] - [ltil_s - ltil])); unfinished chains
+ * record a step; theta_s / ltil_s are reset to the chain's point. */
+int cf_mcmc_sub_final(int C, int D, const double* lexact_p, double* lexact, double* ltil, double* ltil_s,
+                      const double* u, double* theta, double* theta_s, int* steps, double* samples, int max_steps,
+                      int* n_exact, int* n_accept, void* stream);
+
+/* Fused emulator sub-chains: one CTA per chain computes lnL~ at theta (into
+ * ltil) and runs J Metropolis steps on the emulator posterior (proposals
+ * Lp xi[j][c], uniforms u[j][c]; xi J x C x D, u J x C), end point into
+ * theta_s / ltil_s, accepted moves added to n_sub.  The emulator: flat
+ * parameter vector (per layer W out x in row-major, then b) read as BF16
+ * weights (w16, 16-byte aligned) and FP32 biases (w32); sizes
+ * D -> 256 x n_hidden -> 1, SiLU, lnL~ = -(mu + sigma y) / 2.  Chains with
+ * steps >= max_steps copy theta to theta_s. */
+int cf_mcmc_subchain(int C, int D, int J, int n_hidden, const double* theta, const int* steps, int max_steps,
+                     const double* Lp, const double* xi, const double* u, const double* lo, const double* hi,
+                     const void* w16, const float* w32, double mu, double sigma, double* theta_s, double* ltil,
+                     double* ltil_s, int* n_sub, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

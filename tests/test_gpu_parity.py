@@ -1,7 +1,7 @@
 """Device path (plain FP64) against the oracle and the reference's golden outputs.
 
 Tolerances: 1e-13 relative for S and dC (same recurrences, FMA allowed),
-1e-11 for the intermediate C^-1, and north_star's 1e-10 relative for F, q, bias, C_hat, chi2
+1e-11 for the intermediate C^-1, and the drop-in's stated 1e-10 relative for F, q, bias, C_hat, chi2
 and lnL against the reference's own outputs on the same inputs.
 """
 
