@@ -196,12 +196,54 @@ class Engine:
             out[fa.offset: fa.offset + Cc, fb.offset: fb.offset + R] = D["ab"][:, b * R:(b + 1) * R]
         return out
 
+    def qml_reduce(self, M: torch.Tensor | None = None, Y: torch.Tensor | None = None):
+        """Raw bias b_p = 1/2 Tr(M dC_p) (M = C^-1 N C^-1) and q_p = 1/2 y^T dC_p y
+        for the columns y of Y = C^-1 X, building every dC_p entry in registers
+        and reducing it at once (no derivative matrix in HBM)."""
+        L = self.L
+        n, nb, P, Lp = L.n, L.nbins, L.n_params, L.lmax_signal + 1
+        bias = torch.zeros(P, dtype=F64, device=self.dev) if M is not None else None
+        nsims = 0 if Y is None else Y.shape[1]
+        q = torch.zeros((nsims, P), dtype=F64, device=self.dev) if nsims else None
+        if M is not None:
+            M = M.contiguous()
+        for s in range(L.nspectra):
+            blk = L.blocks[self.block_of_spec[s]]
+            fa, fb = L.fields[blk.fa], L.fields[blk.fb]
+            mode = L.spectra[s].mode
+            tab = _off(self.deriv_tab, s * Lp)
+            bins = _off(self.deriv_bin, s * Lp)
+            va, vb = self.vec[blk.fa], self.vec[blk.fb]
+            for m0 in range(0, max(nsims, 1), 4):
+                nv = min(4, nsims - m0) if nsims else 0
+                Yc = Y[:, m0:m0 + nv].contiguous() if nv else None
+                with_bias = M is not None and m0 == 0
+                if not with_bias and nv == 0:
+                    continue
+                check(self.lib.cf_build_block_reduce(
+                    blk.kind, mode, fa.npix, va.data_ptr(), fb.npix, vb.data_ptr(), L.lmax_signal,
+                    tab, None, None, bins, nb, ptr(M) if with_bias else None, n,
+                    ptr(Yc), nv, nv, fb.offset, fa.offset, 0.5,
+                    _off(bias, s * nb) if with_bias else None, _off(q, m0 * P + s * nb) if nv else None, P,
+                    stream()), "cf_build_block_reduce")
+        return bias, q
+
     def fisher_qml(self, Cinv: torch.Tensor, N: torch.Tensor | None = None,
-                   maps: torch.Tensor | None = None, want_fisher: bool = True):
-        """F (P x P), raw bias (P,), raw q (nsims x P) by per-spectrum passes."""
+                   maps: torch.Tensor | None = None, want_fisher: bool = True, fused_reduce: bool = True):
+        """F (P x P), raw bias (P,), raw q (nsims x P) by per-spectrum passes.
+
+        Without the Fisher matrix (want_fisher False) and with fused_reduce,
+        bias and q come from qml_reduce (derivative entries reduced where they
+        are built); otherwise from the derivative blocks the Fisher pass
+        builds anyway."""
         L = self.L
         n, nb, P = L.n, L.nbins, L.n_params
         dev = self.dev
+        if not want_fisher and fused_reduce and nb <= 128 and (N is not None or maps is not None):
+            Y = self.gemm(Cinv, maps.to(dev, F64).contiguous()) if maps is not None else None
+            M = self.gemm(Cinv, self.gemm(N, Cinv)) if N is not None else None
+            bias, q = self.qml_reduce(M, Y)
+            return torch.zeros((P, P), dtype=F64, device=dev), bias, q
         F = torch.zeros((P, P), dtype=F64, device=dev)
         bias = torch.zeros(P, dtype=F64, device=dev) if N is not None else None
         Y = None

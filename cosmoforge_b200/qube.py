@@ -222,10 +222,13 @@ class Fisher(_Base):
         self.compute()
 
     def compute(self) -> None:
+        self._dev_bias = None
         if self.precision == "mixed":
             from . import engine_mixed
 
-            F = engine_mixed.fisher(self.engine, self._dev_Cinv)
+            # the noise bias needs only C^-1, N and dC_b: contract it against
+            # the resident A_b slabs now instead of rebuilding dC_b in Spectra
+            F, self._dev_bias, _ = engine_mixed.fisher_qml(self.engine, self._dev_Cinv, N=self._dev_N)
         else:
             F, _, _ = self.engine.fisher_qml(self._dev_Cinv)
         self._dev_F = F
@@ -397,7 +400,11 @@ class Spectra(_Base):
         nsims = self.params.nsims or X.shape[1]
         if tuple(X.shape) != (L.n, nsims):
             raise ValueError(f"injected maps have shape {tuple(X.shape)}, expected ({L.n}, {nsims})")
-        _, bias, q = E.fisher_qml(f._dev_Cinv, f._dev_N, X, want_fisher=False)
+        if self.precision == "mixed" and getattr(f, "_dev_bias", None) is not None:
+            _, _, q = E.fisher_qml(f._dev_Cinv, None, X, want_fisher=False)
+            bias = f._dev_bias
+        else:
+            _, bias, q = E.fisher_qml(f._dev_Cinv, f._dev_N, X, want_fisher=False)
         if L.remove_nb:
             q = q - bias[None, :]
         self._dev_invF = E.spd_inverse(f._dev_F.clone())

@@ -218,6 +218,21 @@ int cf_build_block_planes(int kind, int mode, int na, const double* va, int nb, 
                           long binT_stride, int batch, long tstride, long ostride, int planes,
                           long plane_stride, long planeT_stride, int flags, void* stream);
 
+/* Build-and-reduce: the binned derivative entries of one block (kind, mode,
+ * fields and tables as cf_build_block) are consumed where they are formed;
+ * nothing but the sums is written:
+ *   bias[b]        += scale * sum_{r,c} W[gro + r, gco + c] dC_b[r, c]
+ *   q[m * ldq + b] += scale * sum_{r,c} Y[gro + r, m] Y[gco + c, m] dC_b[r, c]
+ * over the block and its mirror (scale 1/2 gives 1/2 Tr(W dC_b) and
+ * 1/2 y^T dC_b y).  W: symmetric, row stride ldW, or NULL (no bias); Y:
+ * nv <= 4 map columns, row stride ldY, or nv = 0; nbins <= 128.  Replaces the
+ * dC_b rebuild of qube/spectra.py:1124-1186 (via
+ * cosmocore/core.py:1328-1409) together with its traces. */
+int cf_build_block_reduce(int kind, int mode, int na, const double* va, int nb, const double* vb, int lmax,
+                          const double* t0, const double* t1, const double* t2, const int* bin_of, int nbins,
+                          const double* W, long ldW, const double* Y, long ldY, int nv, long gro, long gco,
+                          double scale, double* bias, double* q, long ldq, void* stream);
+
 /*
  * C = sum_t A_{ta[t]} B_{tb[t]}^T on tcgen05 (FP32 accumulation in TMEM,
  * partial sums promoted to registers every few k-tiles).  A: planes of

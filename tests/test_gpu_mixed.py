@@ -99,3 +99,34 @@ def test_mixed_qml_matches_fp64(name):
     cm = (qm - bm) @ np.linalg.inv(Fm)
     print(f"{name}: |dC_hat|/sigma {np.max(np.abs(cm - c64) / sig):.2e}")
     assert np.max(np.abs(cm - c64) / sig) < QML_SIGMA_TOL[name]
+
+
+@pytest.mark.parametrize("name", ["tqu_cut_nside4", "config0_tt_nside8"])
+def test_mixed_dropin_classes_match_fp64(name):
+    """Fisher / Spectra with precision="mixed" (F and the noise bias from the
+    tensor-core pass in Fisher.run, raw q from the FP64 derivative entries in
+    Spectra.run; q net of the bias carries the bias's error) against the same
+    classes in plain FP64."""
+    from cosmoforge_b200 import qube
+
+    d, p, mask, N, maps = _case(name)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        f = qube.Fisher(p, basis=False, mask=mask, noise_cov1=N, cls_data=cls_of(d), beam=d["beam"],
+                        precision=prec)
+        f.run()
+        s = qube.Spectra(p, fisher=f, maps1=maps)
+        s.run()
+        out[prec] = (f.get_fisher_matrix(), s.get_noise_bias(), s.qml_results, s.get_power_spectra(),
+                     s.qml_noise_bias)
+    F64, nb64, q64, c64, b64 = out["fp64"]
+    Fm, nbm, qm, cm, bm = out["mixed"]
+    corr = np.sqrt(np.outer(np.diag(F64), np.diag(F64)))
+    sig = np.sqrt(np.diag(np.linalg.inv(F64)))
+    e_f = np.max(np.abs(Fm - F64) / corr)
+    e_b = np.max(np.abs(bm - b64)) / np.max(np.abs(b64))
+    e_q = np.max(np.abs(qm - q64)) / np.max(np.abs(q64))
+    e_c = np.max(np.abs(cm - c64) / sig)
+    print(f"{name}: F {e_f:.1e} bias {e_b:.1e} q {e_q:.1e} C_hat {e_c:.1e} sigma")
+    assert e_f <= 5e-5 and e_b <= 1e-5 and e_q <= 1e-5 and e_c <= 1e-3
+    assert np.max(np.abs(nbm - nb64) / sig) <= 1e-3

@@ -72,6 +72,23 @@ def test_qml(solved):
     assert _rel(r["noise_bias"], d["ref_noise_bias"]) <= 1e-8
 
 
+def test_fused_reduce_matches_reference(solved):
+    """Bias and q with the derivative entries reduced where they are built
+    (the drop-in Spectra path) against the reference's raw outputs and the
+    blocks-in-HBM path."""
+    d, L, E, r = solved
+    Cinv = torch.from_numpy(r["Cinv"]).cuda()
+    N = torch.from_numpy(noise_of(d)).cuda()
+    X = torch.from_numpy(d["maps"]).cuda()
+    _, b_f, q_f = E.fisher_qml(Cinv, N, X, want_fisher=False, fused_reduce=True)
+    _, b_d, q_d = E.fisher_qml(Cinv, N, X, want_fisher=False, fused_reduce=False)
+    b_f, q_f, b_d, q_d = (t.cpu().numpy() for t in (b_f, q_f, b_d, q_d))
+    assert _rel(b_f, d["ref_noise_bias_raw"]) <= 1e-10
+    # the reference's q is net of the noise bias when remove_nb is set
+    assert _rel(q_f - b_f[None, :] if L.remove_nb else q_f, d["ref_q_raw"]) <= 1e-10
+    assert _rel(b_f, b_d) <= 1e-10 and _rel(q_f, q_d) <= 1e-10
+
+
 def test_derivatives_match_oracle(solved):
     from oracle import oracle as orc
 
