@@ -13,6 +13,7 @@ metric through the drop-in ``Fisher`` / ``Spectra`` API with host inputs
 Secondary sections of the same line (skipped with ``--no-extra``): the
 batched pixel likelihood (1024 parameter points, FP64 and FP32+refinement),
 the emulator and delayed-acceptance sampler against exact Metropolis, the
+bandpower window function, the same QML solve in the harmonic basis, the
 2048-map solves and the 48-patch batch.
 
 ``--impl reference`` times the CPU restatement of the reference algorithm
@@ -355,6 +356,28 @@ def secondary(args, dev):
     L1 = build_layout(pb1.params, pb1.mask, pb1.beam)
     E1 = engine.Engine(L1, dev)
     N1 = torch.from_numpy(pb1.noise).to(dev)
+
+    # ---- config 1 in the harmonic basis (the reference's default basis here) ----
+    from cosmoforge_b200 import harmonic
+
+    x1 = qube.draw_maps(L1, pb1.cls, N1, 1, seed=0, device=dev)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    hplan = harmonic.HarmonicPlan(E1)
+    torch.cuda.synchronize()
+    t_plan = time.perf_counter() - t0
+    ms_h, rh = _cuda_ms(torch, lambda: harmonic.qml_solve(E1, pb1.cls, N1, x1, plan=hplan), 3)
+    Fp, _, _ = E1.fisher_qml(rh["Cinv"])
+    dg = torch.diagonal(Fp)
+    out["harmonic"] = {
+        "workload": "config1_tqu_nside16_harmonic_basis", "modes": hplan.nm, "precision": "fp64",
+        "basis_chosen_by_reference_cost_model": harmonic.auto_method(L1),
+        "solves_per_s": 1e3 / ms_h, "ms_per_solve": ms_h, "plan_seconds": t_plan,
+        "fisher_vs_pixel_fp64_corr_normalised": float(((rh["fisher"] - Fp).abs()
+                                                        / torch.sqrt(torch.outer(dg, dg))).max()),
+        "step": "S = S_fixed + V^T Lambda V, C^-1, Z = V C^-1, G = Z V^T, F, bias, q, F^-1, C_hat",
+    }
+    del rh, Fp, hplan, x1
     X1 = qube.draw_maps(L1, pb1.cls, N1, 2048, seed=0, device=dev)
     Cinv = E1.spd_inverse(E1.signal(L1.smoothed_cl_table(pb1.cls)) + N1)
     part1 = {}

@@ -30,6 +30,10 @@ SIGNATURES = {
                             _l, _l, _l, _i, _l, _l, _p]),
     "cf_build_block_planes": (_i, [_i, _i, _i, _p, _i, _p, _i, _p, _p, _p, _p, _p, _l, _l, _l, _l, _p,
                                    _l, _l, _l, _l, _i, _l, _l, _i, _l, _l, _i, _p]),
+    "cf_harmonic_operator": (_i, [_i, _i, _i, _p, _i, _i, _p, _l, _l, _l, _p]),
+    "cf_harmonic_lambda": (_i, [_l, _l, _i, _i, _p, _p, _p, _i, _p, _l, _p, _l, _p]),
+    "cf_harmonic_fisher": (_i, [_i, _i, _i, _i, _p, _l, _p, _i, _p, _p, _p, _p, _i, _p, _l, _p]),
+    "cf_harmonic_pair": (_i, [_i, _i, _i, _p, _l, _p, _l, _l, _i, _p, _i, _p, _p, _p, _p, _i, _p, _l, _p]),
     "cf_build_block_reduce": (_i, [_i, _i, _i, _p, _i, _p, _i, _p, _p, _p, _p, _i, _p, _l, _p, _l, _i, _l, _l,
                                    _d, _p, _p, _l, _p]),
     "cf_dgemm": (_i, [_i, _i, _i, _i, _i, _d, _p, _l, _l, _p, _l, _l, _d, _p, _l, _l, _p, _l, _l,

@@ -55,7 +55,10 @@ class PICSLike(_Base):
                  cls_data=None, fiducial_cls=None, beam=None, maps1=None, maps2=None, *,
                  params_file=None, parameter_grid=None, noise_scale_fn=None, batch_size: int = 128,
                  precision: str = "fp64", device=None, **kwargs):
-        _check_basis(basis)
+        # the likelihood is evaluated exactly in pixel space; "auto" / None are
+        # served by that path, an explicit harmonic basis is not implemented
+        if _check_basis(basis) == "harmonic":
+            raise NotImplementedError("PICSLike: the harmonic basis is not implemented; use basis=False")
         super().__init__(params, params_file, mask, noise_cov1, noise_cov2, cls_data, fiducial_cls,
                          beam, precision, device, kwargs)
         if maps1 is None and not getattr(self.params, "inputmapfile1", None):

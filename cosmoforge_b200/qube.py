@@ -9,16 +9,19 @@ injected N stays in ``reduced_noise_cov1``.  The computation runs on the GPU
 through ``libcfb200.so``; host copies of the n x n matrices are made only
 when those attributes are read.
 
-Supported: the pixel-space estimator (``basis=False`` / ``"pixel"``; the
-default ``None`` is served by the same exact pixel path), SYMMETRIC spectra,
-auto-spectra (``do_cross=False``), injected arrays or the reference's file
-inputs (``maskfile``, ``covmatfile1`` / ``load_reduced``, ``inputclfile``,
-``smoothing_type`` file / gaussian / none with ``beam_file`` / ``fwhmarcmin``,
-``inputmapfile1``; ``fileio``).  The harmonic / compressed bases and pixel
-filters raise ``NotImplementedError``.
+Supported: the pixel-space estimator (``basis=False`` / ``"pixel"``), the
+harmonic basis (``"harmonic"``, see ``harmonic``), the default ``None`` /
+``"auto"`` choosing between them by the reference's cost model, SYMMETRIC
+spectra, auto-spectra (``do_cross=False``), injected arrays or the
+reference's file inputs (``maskfile``, ``covmatfile1`` / ``load_reduced``,
+``inputclfile``, ``smoothing_type`` file / gaussian / none with
+``beam_file`` / ``fwhmarcmin``, ``inputmapfile1``; ``fileio``).  Compressed
+pixel bases (``epsilon`` / ``mode_fraction``) and pixel filters raise
+``NotImplementedError``.
 
 ``precision``: ``"fp64"`` (plain FP64 everywhere) or ``"mixed"`` (BF16x3 /
-FP32 tensor-core traces with FP64 refinement, see ``engine_mixed``).
+FP32 tensor-core traces with FP64 refinement, see ``engine_mixed``) on the
+pixel-space path; the harmonic basis always runs in FP64.
 """
 
 from __future__ import annotations
@@ -53,12 +56,32 @@ def _layout(p: dict, mask, beam) -> lay.Layout:
 
 
 def _check_basis(basis):
-    if basis is None or basis is False or basis == "pixel":
-        return
-    if isinstance(basis, dict) and basis.get("method", "pixel") == "pixel" and not (
-            set(basis) & {"epsilon", "compression_target", "mode_fraction"}):
-        return
-    raise NotImplementedError(f"basis={basis!r}: only the exact pixel-space path is implemented")
+    """The basis request as "pixel", "harmonic" or "auto" (cosmocore/core.py:135-160)."""
+    if basis is False:
+        return "pixel"
+    if basis is None:
+        return "auto"
+    if isinstance(basis, str):
+        if basis not in ("auto", "harmonic", "pixel"):
+            raise ValueError(f"unknown basis {basis!r}; expected 'auto'/'harmonic'/'pixel', a dict, False or None")
+        return basis
+    if isinstance(basis, dict):
+        if set(basis) & {"epsilon", "compression_target", "mode_fraction"}:
+            raise NotImplementedError(f"basis={basis!r}: compressed pixel bases are not implemented")
+        method = basis.get("method", "auto")
+        if method not in ("auto", "harmonic", "pixel"):
+            raise ValueError(f"unknown basis method {method!r}")
+        return method
+    raise TypeError(f"basis must be None/False/str/dict, got {type(basis).__name__}")
+
+
+def _resolve_method(req: str, L) -> str:
+    """"auto" by the reference's cost model (cosmocore/basis/__init__.py:87-115)."""
+    if req != "auto":
+        return req
+    from .harmonic import auto_method
+
+    return auto_method(L) if L.lmin >= 2 else "pixel"
 
 
 def _check_kwargs(kwargs):
@@ -177,7 +200,7 @@ class Fisher(_Base):
     def __init__(self, params=None, basis=None, cache_derivatives: bool = False, symmetry_mode=None,
                  mask=None, noise_cov1=None, noise_cov2=None, cls_data=None, fiducial_cls=None,
                  beam=None, *, params_file=None, precision: str = "fp64", device=None, **kwargs):
-        _check_basis(basis)
+        self._basis_req = _check_basis(basis)
         if symmetry_mode not in (None, "SYMMETRIC", "symmetric") and getattr(
                 symmetry_mode, "name", "SYMMETRIC") != "SYMMETRIC":
             raise NotImplementedError("only SymmetryMode.SYMMETRIC is supported")
@@ -216,14 +239,26 @@ class Fisher(_Base):
         L = self.layout
         self.engine = eng.Engine(L, self.device)
         self._host = {}
-        self._dev_S = self.engine.signal(L.smoothed_cl_table(self._cls))
+        self.method = _resolve_method(self._basis_req, L)
+        self._hplan = None
+        if self.method == "harmonic":
+            from .harmonic import HarmonicPlan
+
+            self._hplan = HarmonicPlan(self.engine)
+            self._dev_S = self._hplan.signal(L.smoothed_cl_table(self._cls))
+        else:
+            self._dev_S = self.engine.signal(L.smoothed_cl_table(self._cls))
         C = self._dev_S + self._dev_N
         self._dev_Cinv = self.engine.spd_inverse(C)
         self.compute()
 
     def compute(self) -> None:
         self._dev_bias = None
-        if self.precision == "mixed":
+        if self._hplan is not None:
+            # harmonic basis (always FP64): F and the noise bias from
+            # G = V C^-1 V^T and Z N Z^T; Spectra adds q from z = Z x
+            F, self._dev_bias, _ = self._hplan.fisher_qml(self._dev_Cinv, self._dev_N)
+        elif self.precision == "mixed":
             from . import engine_mixed
 
             # the noise bias needs only C^-1, N and dC_b: contract it against
@@ -272,6 +307,10 @@ class Fisher(_Base):
         p["delta_ell"] = 1
         L1 = _layout(p, self._mask, self._beam)
         E1 = eng.Engine(L1, self.device)
+        if getattr(self, "_hplan", None) is not None:
+            from .harmonic import HarmonicPlan
+
+            return HarmonicPlan(E1).fisher_qml(self._dev_Cinv)[0]
         if self.precision == "mixed":
             from . import engine_mixed
 
@@ -347,6 +386,7 @@ class Spectra(_Base):
                  noise_cov1=None, noise_cov2=None, cls_data=None, fiducial_cls=None, beam=None,
                  maps1=None, maps2=None, *, params_file=None, precision: str | None = None,
                  device=None, **kwargs):
+        self._basis = basis
         _check_basis(basis)
         if fisher is not None:
             self.fisher_instance = fisher
@@ -372,7 +412,7 @@ class Spectra(_Base):
     def _fisher(self) -> Fisher:
         f = self.fisher_instance
         if f is None:
-            f = Fisher(vars(self.params), mask=self._mask, noise_cov1=self._noise_in,
+            f = Fisher(vars(self.params), basis=self._basis, mask=self._mask, noise_cov1=self._noise_in,
                        cls_data=self._cls, beam=self._beam, precision=self.precision,
                        device=self.device)
             self.fisher_instance = f
@@ -400,7 +440,10 @@ class Spectra(_Base):
         nsims = self.params.nsims or X.shape[1]
         if tuple(X.shape) != (L.n, nsims):
             raise ValueError(f"injected maps have shape {tuple(X.shape)}, expected ({L.n}, {nsims})")
-        if self.precision == "mixed" and getattr(f, "_dev_bias", None) is not None:
+        if getattr(f, "_hplan", None) is not None:
+            _, _, q = f._hplan.fisher_qml(f._dev_Cinv, None, X, want_fisher=False)
+            bias = f._dev_bias
+        elif self.precision == "mixed" and getattr(f, "_dev_bias", None) is not None:
             _, _, q = E.fisher_qml(f._dev_Cinv, None, X, want_fisher=False)
             bias = f._dev_bias
         else:

@@ -404,6 +404,47 @@ int cf_mcmc_subchain(int C, int D, int J, int n_hidden, const double* theta, con
                      const void* w16, const float* w32, double mu, double sigma, double* theta_s, double* ltil,
                      double* ltil_s, int* n_sub, void* stream);
 
+/* ---- harmonic basis (basis="harmonic") ----------------------------------
+ * V: real spherical harmonics of the active pixels, rows component-major
+ * (T of a spin-0 field; E then B of a spin-2 field over its [Q | U] columns),
+ * then multipole l in [lmin, lmax], then m = 0 and (cos m, sin m) pairs.
+ * dC/dC_l = t_l V_(u,l)^T V_(v,l) (+ transpose for cross spectra) turns the
+ * Fisher traces, the noise bias and the quadratic forms into contractions of
+ * G = V C^-1 V^T, Z N Z^T and z = Z x (Z = V C^-1).
+ * Replaces: cosmocore/basis/harmonic_basis.py:20-180 (V, with
+ * cosmocore/basics/legendre.py:153-210 and cosmocore/basics/wigner.py:12-120),
+ * the harmonic Fisher of qube/fisher.py:416-500, 575-583 and the harmonic
+ * quadratic forms of cosmocore/basis/harmonic.py:191-1252. */
+
+/* Rows [row0, row0 + (lmax+1)^2 - lmin^2) of V (row stride ldV, zeroed by the
+ * caller) for one component over columns col0..: spin 0, or spin 2 with
+ * is_b 0 (E) / 1 (B) over [Q | U] (2 npix columns).  vec: SoA x[npix] y[npix]
+ * z[npix].  lmax <= 255; spin 2 needs lmin >= 2. */
+int cf_harmonic_operator(int spin, int is_b, int npix, const double* vec, int lmin, int lmax, double* V, long ldV,
+                         long row0, long col0, void* stream);
+
+/* LV[(u,l,m), j] = sum_v lam[(u nc + v) Lp + l] V[(v,l,m), j] for nm rows and
+ * ncol columns; rowinfo int[2 nm] (component, multipole) of each row; off
+ * long[nc Lp] first row of (component, multipole). */
+int cf_harmonic_lambda(long nm, long ncol, int nc, int lmin, const int* rowinfo, const long* off, const double* lam,
+                       int Lp, const double* V, long ldV, double* LV, long ldL, void* stream);
+
+/* F += the binned Fisher matrix (nspec nb square, row stride ldF) from
+ * G = V C^-1 V^T (row stride ldG); nc <= 3 components; su / sv int[nspec]
+ * the components of each spectrum; tab / bin [nspec Lp] the weight and bin of
+ * each multipole (bin -1 outside the bins). */
+int cf_harmonic_fisher(int nc, int lmin, int lmax, int Lp, const double* G, long ldG, const long* off, int nspec,
+                       const int* su, const int* sv, const double* tab, const int* bin, int nb, double* F, long ldF,
+                       void* stream);
+
+/* out[p] (per_col 0) or out[k ldo + p] (per_col 1) += 1/2 t_(s,l) sum_m
+ * A_(u,l,m) . B_(v,l,m) (+ the swapped pair for cross spectra), summed over
+ * the ncol columns or per column: A = Z N, B = Z gives the raw noise bias,
+ * A = B = Z X the raw quadratic forms. */
+int cf_harmonic_pair(int lmin, int lmax, int Lp, const double* A, long ldA, const double* B, long ldB, long ncol,
+                     int per_col, const long* off, int nspec, const int* su, const int* sv, const double* tab,
+                     const int* bin, int nb, double* out, long ldo, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -5,7 +5,8 @@ runs the reference package (ggalloni/CosmoForge v1.3.0) from its sources,
 importing it through the stand-ins in ``_standins/`` (a closed-form
 ``healpy`` and an ``astropy.io.fits`` import shim), with every input
 injected through the in-memory seams and ``basis=False`` (the traditional
-pixel path, the one the device path restates).  It writes one compressed
+pixel path, the one the device path restates); the ``harmonic_*`` cases run
+``basis="harmonic"`` on the inputs of a pixel-path fixture.  It writes one compressed
 ``.npz`` per case holding the inputs, the reference's outputs and, where the
 reference's own tests ship them, the Fortran known answers.
 
@@ -90,6 +91,16 @@ def _run_qml(params, mask, noise, cls, beam, maps):
         s.run()
     t2 = time.perf_counter()
     return f, s, (t1 - t0, t2 - t1)
+
+
+def _run_qml_basis(params, mask, noise, cls, beam, maps, basis):
+    from qube import Fisher, Spectra
+
+    f = Fisher(params, basis=basis, mask=mask, noise_cov1=noise, cls_data=cls, fiducial_cls=cls, beam=beam)
+    f.run()
+    s = Spectra(params, fisher=f, basis=basis, maps1=maps)
+    s.run()
+    return f, s
 
 
 def _spectra_labels(f):
@@ -334,6 +345,26 @@ def case_bandpower_tqu():
           ref_window=W, ref_eff_ells=eff, spectra_labels=np.array(_spectra_labels(f)))
 
 
+def _harmonic_case(src: str, name: str):
+    """The reference's harmonic-basis path (basis="harmonic") on the inputs of
+    an existing pixel-path fixture: F, raw q, noise bias and C_hat."""
+    d = np.load(HERE / f"{src}.npz")
+    params = {"nside": int(d["p_nside"]), "spins": [int(x) for x in d["p_spins"]],
+              "labels": [str(x) for x in d["p_labels"]], "lmin": int(d["p_lmin"]), "lmax": int(d["p_lmax"]),
+              "lmax_signal": int(d["p_lmax_signal"]), "output_convention": str(d["p_output_convention"]),
+              "remove_nb": bool(int(d["p_remove_nb"])), "nsims": int(d["maps"].shape[1])}
+    noise = d["noise"] if "noise" in d.files else np.diag(d["noise_diag"])
+    cls = {k[3:]: d[k] for k in d.files if k.startswith("cl_")}
+    f, s = _run_qml_basis(params, d["mask"], noise, cls, d["beam"], d["maps"], "harmonic")
+    out = {k: d[k] for k in d.files if not k.startswith("ref_") and not k.startswith("fort_")
+           and k not in ("s_rows_idx",)}
+    out.update(ref_fisher=np.asarray(f.get_fisher_matrix()), ref_q_raw=np.asarray(s.qml_results),
+               ref_noise_bias_raw=np.asarray(s.qml_noise_bias), ref_clhat=np.asarray(s.get_power_spectra()),
+               ref_noise_bias=np.asarray(s.get_noise_bias()), ref_invfisher=np.asarray(s.invfisher),
+               ref_basis=np.array("harmonic"))
+    _save(name, **out)
+
+
 def _picslike_points(params, mask, noise, beam, maps, fid_cls, point_cls):
     """Run the reference PICSLike over explicit per-point spectra."""
     from picslike import PICSLike
@@ -438,6 +469,9 @@ CASES = {
     "picslike_tqu": case_picslike_tqu,
     "bandpower_tt": case_bandpower_tt,
     "bandpower_tqu": case_bandpower_tqu,
+    "harmonic_tqu_cut": lambda: _harmonic_case("tqu_cut_nside4", "harmonic_tqu_cut_nside4"),
+    "harmonic_config0": lambda: _harmonic_case("config0_tt_nside8", "harmonic_config0_tt_nside8"),
+    "harmonic_nside4_TEB": lambda: _harmonic_case("nside4_TEB", "harmonic_nside4_TEB"),
 }
 
 if __name__ == "__main__":
