@@ -377,7 +377,29 @@ def secondary(args, dev):
                                                         / torch.sqrt(torch.outer(dg, dg))).max()),
         "step": "S = S_fixed + V^T Lambda V, C^-1, Z = V C^-1, G = Z V^T, F, bias, q, F^-1, C_hat",
     }
-    del rh, Fp, hplan, x1
+    # the eigen-truncated pixel basis (epsilon 1e-3, noise-weighted) on the same problem
+    tab1 = L1.smoothed_cl_table(pb1.cls)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    cplan = harmonic.CompressedPlan(hplan, N1, tab1, epsilon=1e-3)
+    torch.cuda.synchronize()
+    t_cplan = time.perf_counter() - t0
+
+    def csolve():
+        Cci = E1.spd_inverse(cplan.project(hplan.signal(tab1) + N1))
+        Fc, bc, _ = cplan.fisher_qml(Cci)
+        _, _, qc = cplan.fisher_qml(Cci, with_bias=False, maps=x1, want_fisher=False)
+        qc = qc - bc[None, :]
+        return Fc, E1.gemm(qc, E1.spd_inverse(Fc.clone()))
+
+    ms_c, (Fc, _) = _cuda_ms(torch, csolve, 3)
+    out["harmonic"]["compressed"] = {
+        "basis": {"method": "pixel", "epsilon": 1e-3, "compression_target": "noise_weighted"},
+        "dim": cplan.dim, "of_n": L1.n, "setup_seconds": t_cplan, "solves_per_s": 1e3 / ms_c, "ms_per_solve": ms_c,
+        "fisher_diag_rel_change_vs_uncompressed": float((torch.diagonal(Fc) / torch.diagonal(rh["fisher"]) - 1)
+                                                        .abs().max()),
+    }
+    del rh, Fp, hplan, x1, cplan, Fc
     X1 = qube.draw_maps(L1, pb1.cls, N1, 2048, seed=0, device=dev)
     Cinv = E1.spd_inverse(E1.signal(L1.smoothed_cl_table(pb1.cls)) + N1)
     part1 = {}

@@ -113,13 +113,19 @@ class HarmonicPlan:
                   "cf_harmonic_operator")
 
     # ------------------------------------------------------------------
-    def signal(self, cl_table) -> torch.Tensor:
-        """S = S_fixed + V^T Lambda V from a beam-smoothed (nspectra, L+1) table."""
+    def outside(self, cl_table) -> torch.Tensor:
+        """The table with the inference window [lmin, lmax] zeroed (the S_fixed spectra)."""
+        t = torch.as_tensor(cl_table, dtype=F64, device=self.E.dev).clone()
+        t[:, self.lmin:self.lmax + 1] = 0.0
+        return t
+
+    def signal(self, cl_table, fixed_table=None) -> torch.Tensor:
+        """S = S_fixed + V^T Lambda V from beam-smoothed (nspectra, L+1) tables:
+        the window from cl_table, S_fixed from fixed_table (the fiducial
+        spectra; default cl_table)."""
         E, L = self.E, self.L
         tab = torch.as_tensor(cl_table, dtype=F64, device=E.dev).contiguous()
-        fixed = tab.clone()
-        fixed[:, self.lmin:self.lmax + 1] = 0.0
-        S = E.signal(fixed)
+        S = E.signal(self.outside(tab if fixed_table is None else fixed_table))
         lam = torch.zeros((self.nc, self.nc, self.Lp), dtype=F64, device=E.dev)
         for s, (u, v) in enumerate(self.pairs):
             lam[u, v, self.lmin:self.lmax + 1] = tab[s, self.lmin:self.lmax + 1]
@@ -132,19 +138,25 @@ class HarmonicPlan:
         return S
 
     def fisher_qml(self, Cinv: torch.Tensor, N: torch.Tensor | None = None, maps: torch.Tensor | None = None,
-                   want_fisher: bool = True):
-        """F (P x P), raw bias (P,) and raw q (nsims x P), same convention as Engine.fisher_qml."""
+                   want_fisher: bool = True, V: torch.Tensor | None = None, tables=None):
+        """F (P x P), raw bias (P,) and raw q (nsims x P), same convention as Engine.fisher_qml.
+
+        V: the operator whose columns span the space of Cinv / N / maps
+        (default the pixel-space V; a compressed basis passes V U).
+        tables: (deriv_tab, deriv_bin, nbins, n_params) of another binning."""
         E, L = self.E, self.L
-        P, nb, n = L.n_params, L.nbins, L.n
+        V = self.V if V is None else V
+        tab_t, bin_t, nb, P = tables if tables is not None else (E.deriv_tab, E.deriv_bin, L.nbins, L.n_params)
+        n = V.shape[1]
         dev = E.dev
-        Z = E.gemm(self.V, Cinv)
+        Z = E.gemm(V, Cinv)
         F = torch.zeros((P, P), dtype=F64, device=dev)
         lib = E.lib
         if want_fisher:
-            G = E.gemm(Z, self.V, transb=True)
+            G = E.gemm(Z, V, transb=True)
             check(lib.cf_harmonic_fisher(self.nc, self.lmin, self.lmax, self.Lp, G.data_ptr(), self.nm,
                                          self.off.data_ptr(), L.nspectra, self.su.data_ptr(), self.sv.data_ptr(),
-                                         E.deriv_tab.data_ptr(), E.deriv_bin.data_ptr(), nb, F.data_ptr(), P,
+                                         tab_t.data_ptr(), bin_t.data_ptr(), nb, F.data_ptr(), P,
                                          stream()), "cf_harmonic_fisher")
             del G
         bias = q = None
@@ -153,7 +165,7 @@ class HarmonicPlan:
             bias = torch.zeros(P, dtype=F64, device=dev)
             check(lib.cf_harmonic_pair(self.lmin, self.lmax, self.Lp, ZN.data_ptr(), n, Z.data_ptr(), n, n, 0,
                                        self.off.data_ptr(), L.nspectra, self.su.data_ptr(), self.sv.data_ptr(),
-                                       E.deriv_tab.data_ptr(), E.deriv_bin.data_ptr(), nb, bias.data_ptr(), 0,
+                                       tab_t.data_ptr(), bin_t.data_ptr(), nb, bias.data_ptr(), 0,
                                        stream()), "cf_harmonic_pair")
             del ZN
         if maps is not None:
@@ -163,9 +175,106 @@ class HarmonicPlan:
             q = torch.zeros((ns, P), dtype=F64, device=dev)
             check(lib.cf_harmonic_pair(self.lmin, self.lmax, self.Lp, zx.data_ptr(), ns, zx.data_ptr(), ns, ns, 1,
                                        self.off.data_ptr(), L.nspectra, self.su.data_ptr(), self.sv.data_ptr(),
-                                       E.deriv_tab.data_ptr(), E.deriv_bin.data_ptr(), nb, q.data_ptr(), P,
+                                       tab_t.data_ptr(), bin_t.data_ptr(), nb, q.data_ptr(), P,
                                        stream()), "cf_harmonic_pair")
         return F, bias, q
+
+
+def keep_modes(evals: np.ndarray, epsilon=None, mode_fraction=None) -> np.ndarray:
+    """Indices of the kept eigenvectors, by descending eigenvalue
+    (cosmocore/basis/pixel.py:265-311): |lambda| > epsilon max |lambda|, or the
+    leading ceil(mode_fraction n_significant), or everything above 1e-10 max."""
+    order = np.argsort(evals)[::-1]
+    ev = evals[order]
+    amax = float(np.max(np.abs(ev)))
+    if mode_fraction is not None:
+        n_sig = int(np.sum(ev > 1e-10 * amax))
+        keep = np.zeros(ev.size, bool)
+        keep[:max(1, int(np.ceil(mode_fraction * n_sig)))] = True
+    elif epsilon is not None:
+        keep = np.abs(ev) > epsilon * amax
+    else:
+        keep = np.abs(ev) > 1e-10 * amax
+    return order[keep]
+
+
+def _per_field(x, nf, what):
+    """A scalar or a per-field list of thresholds as one value per field."""
+    if x is None or isinstance(x, (int, float)):
+        return [x] * nf
+    x = list(x)
+    if len(x) != nf:
+        raise ValueError(f"{what} needs one value per field ({nf}), got {len(x)}")
+    if any(isinstance(v, (tuple, list)) for v in x):
+        raise NotImplementedError(f"{what}: separate E / B thresholds are not implemented")
+    return x
+
+
+class CompressedPlan:
+    """Eigen-truncated pixel basis (the reference's PixelBasis with epsilon /
+    mode_fraction, cosmocore/basis/pixel.py:265-557, 965-1055, 1493-1996).
+
+    Per field f, the kept eigenvectors U_f of P_f = V_f^T V_f ("harmonic") or
+    P_f (N_eff^-1)_ff P_f ("noise_weighted", the default), with
+    N_eff = N + S_fixed when the inference window is narrower than the signal
+    band; U = diag(U_f) (n x dim).  The estimator then runs in the kept
+    subspace: C_c = U^T C U, derivatives (V U)^T E_l (V U), noise U^T N U,
+    maps U^T x, through the same harmonic contractions.  The symmetric
+    eigendecompositions are cuSOLVER's (torch.linalg.eigh, once per basis).
+    """
+
+    TARGETS = ("harmonic", "noise_weighted")
+
+    def __init__(self, hp: HarmonicPlan, N: torch.Tensor, fixed_table, epsilon=None, mode_fraction=None,
+                 target: str = "noise_weighted"):
+        if epsilon is not None and mode_fraction is not None:
+            raise ValueError("epsilon and mode_fraction are mutually exclusive")
+        if target not in self.TARGETS:
+            raise NotImplementedError(f"compression_target={target!r}: only {self.TARGETS} are implemented")
+        E, L = hp.E, hp.L
+        nf = len(L.fields)
+        eps = _per_field(epsilon, nf, "epsilon")
+        mfs = _per_field(mode_fraction, nf, "mode_fraction")
+        for mf in mfs:
+            if mf is not None and not (0 < mf <= 1):
+                raise ValueError(f"mode_fraction must be in (0, 1], got {mf}")
+        if epsilon is None and mode_fraction is None:
+            eps = [1e-6] * nf
+        self.hp, self.E, self.L = hp, E, L
+        N = N.to(E.dev, F64).contiguous()
+        switch = hp.lmax < L.lmax_signal or hp.lmin > 2
+        N_eff = N + E.signal(hp.outside(fixed_table)) if switch else N.clone()
+        Ninv = E.spd_inverse(N_eff) if target == "noise_weighted" else None
+        blocks = []
+        for fi, f in enumerate(L.fields):
+            cols = slice(f.offset, f.offset + f.nrows)
+            cs = [c for c, (g, _) in enumerate(hp.comps) if g == fi]
+            Vf = hp.V[cs[0] * hp.nrow:(cs[-1] + 1) * hp.nrow, cols].contiguous()
+            P = E.gemm(Vf, Vf, transa=True)
+            M = P if Ninv is None else E.gemm(E.gemm(P, Ninv[cols, cols].contiguous()), P)
+            M = 0.5 * (M + M.T)
+            ev, vec = torch.linalg.eigh(M)
+            keep = keep_modes(ev.cpu().numpy(), eps[fi], mfs[fi])
+            blocks.append((cols, vec[:, torch.from_numpy(keep.copy()).to(E.dev)]))
+        self.dim = sum(b.shape[1] for _, b in blocks)
+        self.dims = [b.shape[1] for _, b in blocks]
+        self.U = torch.zeros((L.n, self.dim), dtype=F64, device=E.dev)
+        c = 0
+        for cols, b in blocks:
+            self.U[cols, c:c + b.shape[1]] = b
+            c += b.shape[1]
+        self.VU = E.gemm(hp.V, self.U)
+        self.Nc = E.gemm(E.gemm(self.U, N, transa=True), self.U)
+
+    def project(self, C: torch.Tensor) -> torch.Tensor:
+        """U^T C U."""
+        return self.E.gemm(self.E.gemm(self.U, C, transa=True), self.U)
+
+    def fisher_qml(self, Cc_inv, with_bias: bool = True, maps=None, want_fisher: bool = True, tables=None):
+        """F, raw bias, raw q in the kept subspace (maps in pixel space)."""
+        xc = self.E.gemm(self.U, maps.to(self.E.dev, F64).contiguous(), transa=True) if maps is not None else None
+        return self.hp.fisher_qml(Cc_inv, self.Nc if with_bias else None, xc, want_fisher=want_fisher, V=self.VU,
+                                  tables=tables)
 
 
 def qml_solve(E: Engine, cls: dict, N: torch.Tensor, maps: torch.Tensor, plan: HarmonicPlan | None = None):

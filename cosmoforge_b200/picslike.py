@@ -57,8 +57,8 @@ class PICSLike(_Base):
                  precision: str = "fp64", device=None, **kwargs):
         # the likelihood is evaluated exactly in pixel space; "auto" / None are
         # served by that path, an explicit harmonic basis is not implemented
-        if _check_basis(basis) == "harmonic":
-            raise NotImplementedError("PICSLike: the harmonic basis is not implemented; use basis=False")
+        if _check_basis(basis) in ("harmonic", "compressed"):
+            raise NotImplementedError("PICSLike: harmonic / compressed bases are not implemented; use basis=False")
         super().__init__(params, params_file, mask, noise_cov1, noise_cov2, cls_data, fiducial_cls,
                          beam, precision, device, kwargs)
         if maps1 is None and not getattr(self.params, "inputmapfile1", None):

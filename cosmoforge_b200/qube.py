@@ -66,13 +66,24 @@ def _check_basis(basis):
             raise ValueError(f"unknown basis {basis!r}; expected 'auto'/'harmonic'/'pixel', a dict, False or None")
         return basis
     if isinstance(basis, dict):
-        if set(basis) & {"epsilon", "compression_target", "mode_fraction"}:
-            raise NotImplementedError(f"basis={basis!r}: compressed pixel bases are not implemented")
         method = basis.get("method", "auto")
         if method not in ("auto", "harmonic", "pixel"):
             raise ValueError(f"unknown basis method {method!r}")
+        unknown = set(basis) - {"method", "epsilon", "mode_fraction", "compression_target"}
+        if unknown:
+            raise NotImplementedError(f"basis options {sorted(unknown)} are not implemented")
+        if basis.get("epsilon") is not None or basis.get("mode_fraction") is not None:
+            # compression intent: the V-based pixel basis (cosmocore/core.py:940-950)
+            return "compressed"
         return method
     raise TypeError(f"basis must be None/False/str/dict, got {type(basis).__name__}")
+
+
+def _compression_of(basis) -> dict:
+    if not isinstance(basis, dict):
+        return {}
+    return dict(epsilon=basis.get("epsilon"), mode_fraction=basis.get("mode_fraction"),
+                target=basis.get("compression_target", "noise_weighted"))
 
 
 def _resolve_method(req: str, L) -> str:
@@ -120,6 +131,7 @@ class _Base:
         self._mask = mask
         self._noise_in = noise_cov1  # None: read from covmatfile1 once the layout is known
         self._cls = cls_data if cls_data is not None else fiducial_cls
+        self._fid = fiducial_cls if fiducial_cls is not None else self._cls
         self._beam = beam
         if precision not in ("fp64", "mixed"):
             raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
@@ -201,6 +213,7 @@ class Fisher(_Base):
                  mask=None, noise_cov1=None, noise_cov2=None, cls_data=None, fiducial_cls=None,
                  beam=None, *, params_file=None, precision: str = "fp64", device=None, **kwargs):
         self._basis_req = _check_basis(basis)
+        self._compression = _compression_of(basis)
         if symmetry_mode not in (None, "SYMMETRIC", "symmetric") and getattr(
                 symmetry_mode, "name", "SYMMETRIC") != "SYMMETRIC":
             raise NotImplementedError("only SymmetryMode.SYMMETRIC is supported")
@@ -240,21 +253,33 @@ class Fisher(_Base):
         self.engine = eng.Engine(L, self.device)
         self._host = {}
         self.method = _resolve_method(self._basis_req, L)
-        self._hplan = None
-        if self.method == "harmonic":
-            from .harmonic import HarmonicPlan
+        self._hplan = self._cplan = None
+        table = L.smoothed_cl_table(self._cls)
+        if self.method in ("harmonic", "compressed"):
+            from .harmonic import CompressedPlan, HarmonicPlan
 
+            # S_fixed (multipoles outside the inference window) from the
+            # fiducial spectra, the window from cls_data (cosmocore/core.py:950-1010)
+            fixed = L.smoothed_cl_table(self._fid)
             self._hplan = HarmonicPlan(self.engine)
-            self._dev_S = self._hplan.signal(L.smoothed_cl_table(self._cls))
+            self._dev_S = self._hplan.signal(table, fixed)
+            C = self._dev_S + self._dev_N
+            if self.method == "compressed":
+                self._cplan = CompressedPlan(self._hplan, self._dev_N, fixed, **self._compression)
+                self.dim = self._cplan.dim
+                C = self._cplan.project(C)
         else:
-            self._dev_S = self.engine.signal(L.smoothed_cl_table(self._cls))
-        C = self._dev_S + self._dev_N
+            self._dev_S = self.engine.signal(table)
+            C = self._dev_S + self._dev_N
         self._dev_Cinv = self.engine.spd_inverse(C)
         self.compute()
 
     def compute(self) -> None:
         self._dev_bias = None
-        if self._hplan is not None:
+        if self._cplan is not None:
+            # compressed basis: the same contractions in the kept subspace
+            F, self._dev_bias, _ = self._cplan.fisher_qml(self._dev_Cinv)
+        elif self._hplan is not None:
             # harmonic basis (always FP64): F and the noise bias from
             # G = V C^-1 V^T and Z N Z^T; Spectra adds q from z = Z x
             F, self._dev_bias, _ = self._hplan.fisher_qml(self._dev_Cinv, self._dev_N)
@@ -307,10 +332,11 @@ class Fisher(_Base):
         p["delta_ell"] = 1
         L1 = _layout(p, self._mask, self._beam)
         E1 = eng.Engine(L1, self.device)
+        tables = (E1.deriv_tab, E1.deriv_bin, L1.nbins, L1.n_params)
+        if getattr(self, "_cplan", None) is not None:
+            return self._cplan.fisher_qml(self._dev_Cinv, with_bias=False, tables=tables)[0]
         if getattr(self, "_hplan", None) is not None:
-            from .harmonic import HarmonicPlan
-
-            return HarmonicPlan(E1).fisher_qml(self._dev_Cinv)[0]
+            return self._hplan.fisher_qml(self._dev_Cinv, tables=tables)[0]
         if self.precision == "mixed":
             from . import engine_mixed
 
@@ -440,7 +466,10 @@ class Spectra(_Base):
         nsims = self.params.nsims or X.shape[1]
         if tuple(X.shape) != (L.n, nsims):
             raise ValueError(f"injected maps have shape {tuple(X.shape)}, expected ({L.n}, {nsims})")
-        if getattr(f, "_hplan", None) is not None:
+        if getattr(f, "_cplan", None) is not None:
+            _, _, q = f._cplan.fisher_qml(f._dev_Cinv, with_bias=False, maps=X, want_fisher=False)
+            bias = f._dev_bias
+        elif getattr(f, "_hplan", None) is not None:
             _, _, q = f._hplan.fisher_qml(f._dev_Cinv, None, X, want_fisher=False)
             bias = f._dev_bias
         elif self.precision == "mixed" and getattr(f, "_dev_bias", None) is not None:

@@ -230,14 +230,13 @@ def fisher_harmonic(L, Cinv, lmin, lmax, weights=None):
     return F
 
 
-def signal_harmonic(L, cl_table, lmin, lmax, signal_pixel):
+def signal_harmonic(L, cl_table, lmin, lmax, signal_pixel, fixed_table=None):
     """S as the harmonic basis assembles it (cosmocore/core.py:950-1010):
     V^T Lambda V over the inference window [lmin, lmax] plus the pixel-space
-    signal of the multipoles outside it (S_fixed).  cl_table: beam-smoothed
+    signal of the multipoles outside it (S_fixed, from fixed_table, the
+    fiducial spectra, default cl_table).  Tables: beam-smoothed
     (nspectra, lmax_signal + 1); signal_pixel(table) builds a pixel S."""
-    fixed = np.array(cl_table, dtype=np.float64, copy=True)
-    fixed[:, lmin:lmax + 1] = 0.0
-    S = signal_pixel(fixed)
+    S = signal_pixel(_outside(cl_table if fixed_table is None else fixed_table, lmin, lmax))
     V = harmonic_operator(L, lmin, lmax)
     off, _ = mode_offsets(L, lmin, lmax)
     LV = np.zeros_like(V)
@@ -279,3 +278,123 @@ def qml_harmonic(L, Cinv, N, maps, lmin, lmax, weights=None):
             bias[p] += 0.5 * f * t * np.trace(h[ru:ru + k, rv:rv + k])
             q[:, p] += 0.5 * f * t * np.sum(z[ru:ru + k] * z[rv:rv + k], axis=0)
     return bias, q
+
+
+def _fisher_from_G(L, G, lmin, lmax, W):
+    off, _ = mode_offsets(L, lmin, lmax)
+    nc = len(components(L))
+    nb, P = L.nbins, L.n_params
+    pairs = []
+    for s in range(L.nspectra):
+        u, v = spectrum_components(L, s)
+        pairs.append([(u, v)] if u == v else [(u, v), (v, u)])
+    F = np.zeros((P, P))
+    for l1 in range(lmin, lmax + 1):
+        for l2 in range(lmin, lmax + 1):
+            g = np.stack([G[off[(p, l1)]: off[(p, l1)] + 2 * l1 + 1, off[(q, l2)]: off[(q, l2)] + 2 * l2 + 1].ravel()
+                          for p in range(nc) for q in range(nc)])
+            K = g @ g.T
+            for p1 in range(P):
+                t1 = W[p1, l1]
+                if t1 == 0.0:
+                    continue
+                for p2 in range(P):
+                    t2 = W[p2, l2]
+                    if t2 == 0.0:
+                        continue
+                    acc = sum(K[v * nc + a, u * nc + b] for (u, v) in pairs[p1 // nb] for (a, b) in pairs[p2 // nb])
+                    F[p1, p2] += 0.5 * t1 * t2 * acc
+    return F
+
+
+def _qml_from_Z(L, Z, Nm, xm, lmin, lmax, W):
+    off, _ = mode_offsets(L, lmin, lmax)
+    h = Z @ Nm @ Z.T
+    z = Z @ xm
+    nb, P = L.nbins, L.n_params
+    bias = np.zeros(P)
+    q = np.zeros((xm.shape[1], P))
+    for p in range(P):
+        u, v = spectrum_components(L, p // nb)
+        f = 1.0 if u == v else 2.0
+        for ell in range(lmin, lmax + 1):
+            t = W[p, ell]
+            if t == 0.0:
+                continue
+            k = 2 * ell + 1
+            ru, rv = off[(u, ell)], off[(v, ell)]
+            bias[p] += 0.5 * f * t * np.trace(h[ru:ru + k, rv:rv + k])
+            q[:, p] += 0.5 * f * t * np.sum(z[ru:ru + k] * z[rv:rv + k], axis=0)
+    return bias, q
+
+
+def keep_modes(evals, epsilon=None, mode_fraction=None):
+    """Indices of the kept eigenvectors, eigenvalues sorted descending
+    (cosmocore/basis/pixel.py:265-311)."""
+    order = np.argsort(evals)[::-1]
+    ev = evals[order]
+    amax = np.max(np.abs(ev))
+    if mode_fraction is not None:
+        n_sig = int(np.sum(ev > 1e-10 * amax))
+        keep = np.zeros(ev.size, bool)
+        keep[:max(1, int(np.ceil(mode_fraction * n_sig)))] = True
+    elif epsilon is not None:
+        keep = np.abs(ev) > epsilon * amax
+    else:
+        keep = np.abs(ev) > 1e-10 * amax
+    return order[keep]
+
+
+def compression_basis(L, V, N_eff, lmin, lmax, epsilon=None, mode_fraction=None, target="noise_weighted"):
+    """Block-diagonal U (n x dim): per field, the kept eigenvectors of
+    P_f = V_f^T V_f ("harmonic") or P_f (N_eff^-1)_ff P_f ("noise_weighted")
+    (cosmocore/basis/pixel.py:447-557, 1493-1612)."""
+    comps = components(L)
+    off, _ = mode_offsets(L, lmin, lmax)
+    nrow = (lmax + 1) ** 2 - lmin ** 2
+    Ninv = np.linalg.inv(N_eff)
+    blocks = []
+    for fi, f in enumerate(L.fields):
+        cols = np.arange(f.offset, f.offset + f.nrows)
+        rows = np.concatenate([np.arange(ci * nrow, (ci + 1) * nrow) for ci, (g, _) in enumerate(comps) if g == fi])
+        Vf = V[np.ix_(rows, cols)]
+        P = Vf.T @ Vf
+        M = P if target == "harmonic" else P @ Ninv[np.ix_(cols, cols)] @ P
+        ev, vec = np.linalg.eigh(M)
+        blocks.append((cols, vec[:, keep_modes(ev, epsilon, mode_fraction)]))
+    dim = sum(b.shape[1] for _, b in blocks)
+    U = np.zeros((L.n, dim))
+    c = 0
+    for cols, b in blocks:
+        U[cols, c:c + b.shape[1]] = b
+        c += b.shape[1]
+    return U
+
+
+def compressed_estimator(L, N, tab, tab_fixed, maps, signal_pixel, epsilon=None, mode_fraction=None,
+                         target="noise_weighted", weights=None):
+    """F, raw bias, raw q of the compressed pixel basis: C_c = U^T C U with C
+    the harmonic-basis covariance, derivatives (V U)^T E_l (V U), bias with
+    U^T N U, maps U^T x (cosmocore/basis/pixel.py:1614-1996)."""
+    lmin, lmax = L.lmin, L.lmax
+    W = L.param_weights() if weights is None else weights
+    V = harmonic_operator(L, lmin, lmax)
+    S = signal_harmonic(L, tab, lmin, lmax, signal_pixel, tab_fixed)
+    S_fixed = signal_pixel(_outside(tab_fixed, lmin, lmax))
+    switch = lmax < L.lmax_signal or lmin > 2
+    N_eff = N + S_fixed if switch else N
+    U = compression_basis(L, V, N_eff, lmin, lmax, epsilon, mode_fraction, target)
+    Cc = U.T @ (N + S) @ U
+    Cc_inv = np.linalg.inv(Cc)
+    VU = V @ U
+    G = VU @ Cc_inv @ VU.T
+    F = _fisher_from_G(L, G, lmin, lmax, W)
+    Z = VU @ Cc_inv
+    bias, q = _qml_from_Z(L, Z, U.T @ N @ U, U.T @ maps, lmin, lmax, W)
+    return F, bias, q, U.shape[1]
+
+
+def _outside(tab, lmin, lmax):
+    out = np.array(tab, dtype=np.float64, copy=True)
+    out[:, lmin:lmax + 1] = 0.0
+    return out

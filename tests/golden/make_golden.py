@@ -345,6 +345,26 @@ def case_bandpower_tqu():
           ref_window=W, ref_eff_ells=eff, spectra_labels=np.array(_spectra_labels(f)))
 
 
+def _compressed_case(src: str, name: str, basis: dict):
+    """The reference's compressed pixel basis (V-based, eigen-truncated) on the
+    inputs of an existing pixel-path fixture."""
+    d = np.load(HERE / f"{src}.npz")
+    params = {"nside": int(d["p_nside"]), "spins": [int(x) for x in d["p_spins"]],
+              "labels": [str(x) for x in d["p_labels"]], "lmin": int(d["p_lmin"]), "lmax": int(d["p_lmax"]),
+              "lmax_signal": int(d["p_lmax_signal"]), "output_convention": str(d["p_output_convention"]),
+              "remove_nb": bool(int(d["p_remove_nb"])), "nsims": int(d["maps"].shape[1])}
+    noise = d["noise"] if "noise" in d.files else np.diag(d["noise_diag"])
+    cls = {k[3:]: d[k] for k in d.files if k.startswith("cl_")}
+    f, s = _run_qml_basis(params, d["mask"], noise, cls, d["beam"], d["maps"], dict(basis))
+    out = {k: d[k] for k in d.files if not k.startswith("ref_") and not k.startswith("fort_")
+           and k not in ("s_rows_idx",)}
+    out.update(ref_fisher=np.asarray(f.get_fisher_matrix()), ref_q_raw=np.asarray(s.qml_results),
+               ref_noise_bias_raw=np.asarray(s.qml_noise_bias), ref_clhat=np.asarray(s.get_power_spectra()),
+               ref_noise_bias=np.asarray(s.get_noise_bias()), ref_invfisher=np.asarray(s.invfisher),
+               ref_basis=np.array(repr(basis)), ref_dim=int(f.basis_manager.dim))
+    _save(name, **out)
+
+
 def _harmonic_case(src: str, name: str):
     """The reference's harmonic-basis path (basis="harmonic") on the inputs of
     an existing pixel-path fixture: F, raw q, noise bias and C_hat."""
@@ -472,6 +492,10 @@ CASES = {
     "harmonic_tqu_cut": lambda: _harmonic_case("tqu_cut_nside4", "harmonic_tqu_cut_nside4"),
     "harmonic_config0": lambda: _harmonic_case("config0_tt_nside8", "harmonic_config0_tt_nside8"),
     "harmonic_nside4_TEB": lambda: _harmonic_case("nside4_TEB", "harmonic_nside4_TEB"),
+    "compressed_tqu_cut": lambda: _compressed_case("tqu_cut_nside4", "compressed_tqu_cut_nside4",
+                                                   {"method": "pixel", "epsilon": 1e-3}),
+    "compressed_config0": lambda: _compressed_case("config0_tt_nside8", "compressed_config0_tt_nside8",
+                                                   {"method": "pixel", "epsilon": 1e-3}),
 }
 
 if __name__ == "__main__":

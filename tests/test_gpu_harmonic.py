@@ -8,6 +8,8 @@
   amount by which its own harmonic and pixel-space C_hat differ).
 * The drop-in classes with basis="harmonic" and with the default basis (which
   the reference's cost model sends to the harmonic basis on these problems).
+* The compressed pixel basis (epsilon, noise-weighted eigen-truncation)
+  through the drop-in classes against the reference's PixelBasis run.
 * At the TQU nside-16 size (n = 5952, l = 2..47): harmonic F against the
   pixel-space FP64 F of the same engine; they differ by the rounding of the
   pixel-space spin-2 kernels (~1e-8), not by the method.
@@ -99,3 +101,24 @@ def test_harmonic_matches_pixel_at_config1_size():
     e_f = float(np.max(np.abs(Fh - Fp) / corr))
     print(f"n = {L.n}, modes = {plan.nm}: |dS| {e_s:.1e}, F corr-normalised {e_f:.1e}")
     assert e_s <= 2e-8 and e_f <= 2e-8
+
+
+@pytest.mark.parametrize("name", ["compressed_tqu_cut_nside4", "compressed_config0_tt_nside8"])
+def test_compressed_dropin_matches_reference(name):
+    """basis={"method": "pixel", "epsilon": 1e-3}: the eigen-truncated pixel basis
+    (noise-weighted target, cuSOLVER eigenvectors) against the reference's run:
+    same kept dimension; F, raw bias, raw q, C_hat 1e-10."""
+    from cosmoforge_b200 import qube
+
+    d = load(name)
+    p = params_of(d)
+    f = qube.Fisher(p, basis={"method": "pixel", "epsilon": 1e-3}, mask=d["mask"], noise_cov1=noise_of(d),
+                    cls_data=cls_of(d), beam=d["beam"])
+    f.run()
+    assert f.method == "compressed" and f.dim == int(d["ref_dim"])
+    s = qube.Spectra(p, fisher=f, maps1=d["maps"])
+    s.run()
+    e = {"F": _rel(f.get_fisher_matrix(), d["ref_fisher"]), "q": _rel(s.qml_results, d["ref_q_raw"]),
+         "bias": _rel(s.qml_noise_bias, d["ref_noise_bias_raw"]), "C_hat": _rel(s.get_power_spectra(), d["ref_clhat"])}
+    print(name, f.dim, {k: f"{v:.1e}" for k, v in e.items()})
+    assert max(e.values()) <= 1e-10

@@ -6,6 +6,8 @@ to the reference's own harmonic-basis outputs.
   spin-0 blocks; 1e-7 where spin-2 rotation angles enter, the rounding level
   of the pixel-space 22 / 02 kernels (the harmonic form is exact there; the
   reference's pixel and harmonic outputs differ by the same amount).
+* The compressed pixel basis (epsilon, noise-weighted eigen-truncation)
+  against the reference's PixelBasis run: kept dimension, F, q, bias, C_hat.
 * F, raw bias, raw q against the reference run with basis="harmonic"
   (fixtures harmonic_*.npz, made by tests/golden/make_golden.py): 1e-10
   relative; C_hat 1e-9 (the reference's harmonic F^-1 carries ~2e-10 of
@@ -65,3 +67,22 @@ def test_harmonic_estimator_matches_reference(src, hname):
     assert _rel(b, h["ref_noise_bias_raw"]) <= 1e-10
     assert _rel(q, h["ref_q_raw"]) <= 1e-10
     assert _rel(cl, h["ref_clhat"]) <= 1e-9
+
+
+@pytest.mark.parametrize("name", ["compressed_tqu_cut_nside4", "compressed_config0_tt_nside8"])
+def test_compressed_estimator_matches_reference(name):
+    """The eigen-truncated pixel basis (epsilon 1e-3, noise-weighted target)
+    against the reference's PixelBasis run: same kept dimension; F, raw bias,
+    raw q, C_hat 1e-10."""
+    d = load(name)
+    L = build_layout(params_of(d), d["mask"], d["beam"])
+    tab = L.smoothed_cl_table(cls_of(d))
+    F, b, q, dim = ho.compressed_estimator(L, noise_of(d), tab, tab, d["maps"],
+                                           lambda t: orc.signal_matrix(L, t), epsilon=1e-3)
+    if L.remove_nb:
+        q = q - b[None, :]
+    assert dim == int(d["ref_dim"])
+    assert _rel(F, d["ref_fisher"]) <= 1e-10
+    assert _rel(b, d["ref_noise_bias_raw"]) <= 1e-10
+    assert _rel(q, d["ref_q_raw"]) <= 1e-10
+    assert _rel(q @ orc.matrix_inverse_symm(F), d["ref_clhat"]) <= 1e-10
