@@ -21,6 +21,9 @@ Here:
 For the config-1 problem (n = 5952, three components, l = 2..47) this is four
 n_modes x n x n-class GEMMs (~2e12 FLOP) instead of 276 A_b = C^-1 dC_b
 products.  Always FP64.
+
+``CompressedPlan`` is the reference's eigen-truncated pixel basis on top of
+the same contractions (V -> V U in the kept subspace U).
 """
 
 from __future__ import annotations

@@ -15,8 +15,9 @@ harmonic basis (``"harmonic"``, see ``harmonic``), the default ``None`` /
 spectra, auto-spectra (``do_cross=False``), injected arrays or the
 reference's file inputs (``maskfile``, ``covmatfile1`` / ``load_reduced``,
 ``inputclfile``, ``smoothing_type`` file / gaussian / none with
-``beam_file`` / ``fwhmarcmin``, ``inputmapfile1``; ``fileio``).  Compressed
-pixel bases (``epsilon`` / ``mode_fraction``) and pixel filters raise
+``beam_file`` / ``fwhmarcmin``, ``inputmapfile1``; ``fileio``), and the
+compressed pixel basis (``basis={"method": "pixel", "epsilon": ...}`` or
+``"mode_fraction"``; ``harmonic.CompressedPlan``).  Pixel filters raise
 ``NotImplementedError``.
 
 ``precision``: ``"fp64"`` (plain FP64 everywhere) or ``"mixed"`` (BF16x3 /
