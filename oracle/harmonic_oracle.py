@@ -361,7 +361,11 @@ def compression_basis(L, V, N_eff, lmin, lmax, epsilon=None, mode_fraction=None,
         P = Vf.T @ Vf
         M = P if target == "harmonic" else P @ Ninv[np.ix_(cols, cols)] @ P
         ev, vec = np.linalg.eigh(M)
-        blocks.append((cols, vec[:, keep_modes(ev, epsilon, mode_fraction)]))
+        e_f = epsilon[fi] if isinstance(epsilon, (list, tuple)) else epsilon
+        m_f = mode_fraction[fi] if isinstance(mode_fraction, (list, tuple)) else mode_fraction
+        if e_f is None and m_f is None and epsilon is None and mode_fraction is None:
+            e_f = 1e-6
+        blocks.append((cols, vec[:, keep_modes(ev, e_f, m_f)]))
     dim = sum(b.shape[1] for _, b in blocks)
     U = np.zeros((L.n, dim))
     c = 0

@@ -103,17 +103,20 @@ def test_harmonic_matches_pixel_at_config1_size():
     assert e_s <= 2e-8 and e_f <= 2e-8
 
 
-@pytest.mark.parametrize("name", ["compressed_tqu_cut_nside4", "compressed_config0_tt_nside8"])
-def test_compressed_dropin_matches_reference(name):
-    """basis={"method": "pixel", "epsilon": 1e-3}: the eigen-truncated pixel basis
-    (noise-weighted target, cuSOLVER eigenvectors) against the reference's run:
+@pytest.mark.parametrize("name,basis", [
+    ("compressed_tqu_cut_nside4", {"method": "pixel", "epsilon": 1e-3}),
+    ("compressed_config0_tt_nside8", {"method": "pixel", "epsilon": 1e-3}),
+    ("compressed_mf_tqu_cut_nside4", {"method": "pixel", "mode_fraction": [0.9, 0.7]}),
+    ("compressed_h_config0_tt_nside8", {"method": "pixel", "epsilon": 1e-2, "compression_target": "harmonic"})])
+def test_compressed_dropin_matches_reference(name, basis):
+    """The eigen-truncated pixel basis (cuSOLVER eigenvectors) through the
+    drop-in classes against the reference's run with the same basis dict:
     same kept dimension; F, raw bias, raw q, C_hat 1e-10."""
     from cosmoforge_b200 import qube
 
     d = load(name)
     p = params_of(d)
-    f = qube.Fisher(p, basis={"method": "pixel", "epsilon": 1e-3}, mask=d["mask"], noise_cov1=noise_of(d),
-                    cls_data=cls_of(d), beam=d["beam"])
+    f = qube.Fisher(p, basis=basis, mask=d["mask"], noise_cov1=noise_of(d), cls_data=cls_of(d), beam=d["beam"])
     f.run()
     assert f.method == "compressed" and f.dim == int(d["ref_dim"])
     s = qube.Spectra(p, fisher=f, maps1=d["maps"])

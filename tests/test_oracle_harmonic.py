@@ -69,16 +69,22 @@ def test_harmonic_estimator_matches_reference(src, hname):
     assert _rel(cl, h["ref_clhat"]) <= 1e-9
 
 
-@pytest.mark.parametrize("name", ["compressed_tqu_cut_nside4", "compressed_config0_tt_nside8"])
-def test_compressed_estimator_matches_reference(name):
-    """The eigen-truncated pixel basis (epsilon 1e-3, noise-weighted target)
-    against the reference's PixelBasis run: same kept dimension; F, raw bias,
-    raw q, C_hat 1e-10."""
+COMPRESSED = [("compressed_tqu_cut_nside4", dict(epsilon=1e-3)),
+              ("compressed_config0_tt_nside8", dict(epsilon=1e-3)),
+              ("compressed_mf_tqu_cut_nside4", dict(mode_fraction=[0.9, 0.7])),
+              ("compressed_h_config0_tt_nside8", dict(epsilon=1e-2, target="harmonic"))]
+
+
+@pytest.mark.parametrize("name,kw", COMPRESSED)
+def test_compressed_estimator_matches_reference(name, kw):
+    """The eigen-truncated pixel basis (noise-weighted or harmonic target,
+    epsilon or per-field mode fractions) against the reference's PixelBasis
+    run: same kept dimension; F, raw bias, raw q, C_hat 1e-10."""
     d = load(name)
     L = build_layout(params_of(d), d["mask"], d["beam"])
     tab = L.smoothed_cl_table(cls_of(d))
     F, b, q, dim = ho.compressed_estimator(L, noise_of(d), tab, tab, d["maps"],
-                                           lambda t: orc.signal_matrix(L, t), epsilon=1e-3)
+                                           lambda t: orc.signal_matrix(L, t), **kw)
     if L.remove_nb:
         q = q - b[None, :]
     assert dim == int(d["ref_dim"])
