@@ -497,7 +497,7 @@ CASES = {
     "compressed_config0": lambda: _compressed_case("config0_tt_nside8", "compressed_config0_tt_nside8",
                                                    {"method": "pixel", "epsilon": 1e-3}),
     "compressed_mf_tqu_cut": lambda: _compressed_case(
-        "tqu_cut_nside4", "compressed_mf_tqu_cut_nside4", {"method": "pixel", "mode_fraction": [0.9, 0.7]}),
+        "tqu_cut_nside4", "compressed_mf_tqu_cut_nside4", {"method": "pixel", "mode_fraction": [0.7, 0.6]}),
     "compressed_h_config0": lambda: _compressed_case(
         "config0_tt_nside8", "compressed_h_config0_tt_nside8",
         {"method": "pixel", "epsilon": 1e-2, "compression_target": "harmonic"}),

@@ -71,7 +71,7 @@ def test_harmonic_estimator_matches_reference(src, hname):
 
 COMPRESSED = [("compressed_tqu_cut_nside4", dict(epsilon=1e-3)),
               ("compressed_config0_tt_nside8", dict(epsilon=1e-3)),
-              ("compressed_mf_tqu_cut_nside4", dict(mode_fraction=[0.9, 0.7])),
+              ("compressed_mf_tqu_cut_nside4", dict(mode_fraction=[0.7, 0.6])),
               ("compressed_h_config0_tt_nside8", dict(epsilon=1e-2, target="harmonic"))]
 
 
@@ -79,7 +79,11 @@ COMPRESSED = [("compressed_tqu_cut_nside4", dict(epsilon=1e-3)),
 def test_compressed_estimator_matches_reference(name, kw):
     """The eigen-truncated pixel basis (noise-weighted or harmonic target,
     epsilon or per-field mode fractions) against the reference's PixelBasis
-    run: same kept dimension; F, raw bias, raw q, C_hat 1e-10."""
+    run: same kept dimension; F, raw bias, raw q, C_hat 1e-10.  Each cut sits
+    at an eigenvalue gap of 1e-4 or more of the largest eigenvalue: a cut
+    inside a near-degenerate pair (gap ~1e-9, e.g. mode_fraction 0.9 on the
+    T field here) leaves the kept subspace undetermined to ~1e-7 for any
+    eigensolver, and q moves at the 1e-10 level."""
     d = load(name)
     L = build_layout(params_of(d), d["mask"], d["beam"])
     tab = L.smoothed_cl_table(cls_of(d))
