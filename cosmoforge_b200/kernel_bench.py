@@ -4,6 +4,7 @@
     python -m cosmoforge_b200.kernel_bench umma_trace P1,P2,K1,K2 [--planes 3]
     python -m cosmoforge_b200.kernel_bench dgemm M,N,K
     python -m cosmoforge_b200.kernel_bench spd_inverse N
+    python -m cosmoforge_b200.kernel_bench harmonic 1        (config-1 harmonic-basis solve)
 
 Each case fills seeded random operands on cuda:0, runs two untimed launches,
 then times `reps` launches with CUDA events on the launching stream and prints
@@ -134,9 +135,34 @@ def spd_inverse_case(n):
     return fn, float(n) ** 3, None
 
 
+def harmonic_case(which):
+    """One harmonic-basis QML solve of the TQU nside-16 problem (which = 1:
+    n = 5952, l = 2..47; S, C^-1, F, bias, q, F^-1, C_hat), seeded map."""
+    from . import harmonic, qube, workloads
+    from .engine import Engine
+    from .layout import build_layout
+
+    if which != 1:
+        raise SystemExit("harmonic: only the config-1 problem (shape 1) is defined")
+    pb = workloads.config1()
+    L = build_layout(pb.params, pb.mask, pb.beam)
+    E = Engine(L)
+    N = torch.from_numpy(pb.noise).cuda()
+    x = qube.draw_maps(L, pb.cls, N, 1, seed=0)
+    plan = harmonic.HarmonicPlan(E)
+
+    def fn():
+        harmonic.qml_solve(E, pb.cls, N, x, plan=plan)
+
+    n, nm = L.n, plan.nm
+    flop = 2.0 * n * n * nm * 3 + 2.0 * nm * nm * n + n ** 3  # V^T LV, Z, Z N; G; inverse
+    fn._keep = (E, N, x, plan)
+    return fn, flop, None
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("case", choices=["umma_gemm", "umma_trace", "dgemm", "spd_inverse"])
+    ap.add_argument("case", choices=["umma_gemm", "umma_trace", "dgemm", "spd_inverse", "harmonic"])
     ap.add_argument("shape", help="comma-separated sizes")
     ap.add_argument("--planes", type=int, default=3)
     ap.add_argument("--reps", type=int, default=5)
@@ -152,6 +178,8 @@ def main(argv=None):
         fn, fl, err = umma_trace_case(*dims, planes=a.planes, splits=a.splits)
     elif a.case == "dgemm":
         fn, fl, err = dgemm_case(*dims)
+    elif a.case == "harmonic":
+        fn, fl, err = harmonic_case(*dims)
     else:
         fn, fl, err = spd_inverse_case(*dims)
     ms = time_launches(fn, a.reps)
