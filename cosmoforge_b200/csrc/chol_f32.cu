@@ -65,16 +65,25 @@ __global__ void __launch_bounds__(256) k_potrf_diag_inv_f32(float* A, long lda, 
         const int r = e / kb, c = e % kb;
         A[(long)(k0 + r) * lda + k0 + c] = (c <= r) ? S[r * LDS + c] : 0.0f;
     }
-    if (tid < kb) {  // L11^-1 by forward substitution, one thread per column
-        const int c = tid;
-        for (int r = 0; r < kb; ++r) {
-            float x = 0.0f;
-            if (r >= c) {
-                float acc = (r == c) ? 1.0f : 0.0f;
-                for (int t = c; t < r; ++t) acc -= S[r * LDS + t] * Xs[t * LDS + c];
-                x = acc / S[r * LDS + r];
+    // L11^-1 by column-oriented forward substitution: a warp per column c,
+    // lane l holding rows l and l + 32; x_t = acc_t / L_tt is broadcast and
+    // every later row subtracts L_rt x_t (the same terms in the same order as
+    // the row-oriented sum, so the same values)
+    {
+        const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+        for (int c = warp; c < kb; c += nw) {
+            float a0 = (lane == c) ? 1.0f : 0.0f, a1 = (lane + 32 == c) ? 1.0f : 0.0f;
+            float x0 = 0.0f, x1 = 0.0f;
+            for (int t = c; t < kb; ++t) {
+                const float at = __shfl_sync(0xffffffffu, t < 32 ? a0 : a1, t & 31);
+                const float xt = at / S[t * LDS + t];
+                if (lane == t) x0 = xt;
+                if (lane + 32 == t) x1 = xt;
+                if (lane > t) a0 -= S[lane * LDS + t] * xt;
+                if (lane + 32 > t && lane + 32 < kb) a1 -= S[(lane + 32) * LDS + t] * xt;
             }
-            Xs[r * LDS + c] = x;
+            if (lane < kb) Xs[lane * LDS + c] = x0;
+            if (lane + 32 < kb) Xs[(lane + 32) * LDS + c] = x1;
         }
     }
     __syncthreads();
