@@ -52,11 +52,19 @@ __global__ void __launch_bounds__(256) k_potrf_diag_inv(double* A, long lda, lon
         }
         if (tid == 0) piv[j] = sqrt(d);
         const double inv_d = 1.0 / d;
-        // trailing update with the unscaled column j; column j - 1 gets its scaling now
-        // trailing lower triangle: one warp per row, lanes over columns
-        for (int rr = j + 1 + (tid >> 5); rr < kb; rr += blockDim.x >> 5) {
-            const double srj = S[rr * LDS + j] * inv_d;
-            for (int cc = j + 1 + (tid & 31); cc <= rr; cc += 32) S[rr * LDS + cc] -= srj * S[cc * LDS + j];
+        // trailing update with the unscaled column j; column j - 1 gets its scaling now.
+        // The m x m trailing square is flattened over all threads (independent
+        // entries, so their shared-memory latencies overlap); entries above the
+        // diagonal are skipped
+        {
+            const int m = kb - j - 1;
+            for (int e = tid; e < m * m; e += blockDim.x) {
+                const int rr = j + 1 + e / m, cc = j + 1 + e % m;
+                if (cc <= rr) {
+                    const double srj = S[rr * LDS + j] * inv_d;
+                    S[rr * LDS + cc] -= srj * S[cc * LDS + j];
+                }
+            }
         }
         if (j > 0)
             for (int r = j + tid; r < kb; r += blockDim.x) S[r * LDS + j - 1] /= piv[j - 1];
