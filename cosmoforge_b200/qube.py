@@ -91,9 +91,13 @@ def _resolve_method(req: str, L) -> str:
     """"auto" by the reference's cost model (cosmocore/basis/__init__.py:87-115)."""
     if req != "auto":
         return req
-    from .harmonic import auto_method
+    from .harmonic import auto_method, components
 
-    return auto_method(L) if L.lmin >= 2 else "pixel"
+    # layouts the device harmonic basis does not take (more than three
+    # components, lmin < 2) are served by the exact pixel path
+    if L.lmin < 2 or len(components(L)) > 3:
+        return "pixel"
+    return auto_method(L)
 
 
 def _check_kwargs(kwargs):

@@ -65,3 +65,14 @@ def test_per_field_thresholds():
         harmonic._per_field([0.7], 2, "mode_fraction")
     with pytest.raises(NotImplementedError):
         harmonic._per_field([(0.7, 0.5), 0.6], 2, "mode_fraction")
+
+
+def test_auto_falls_back_to_pixel_for_unsupported_layouts():
+    from cosmoforge_b200.qube import _resolve_method
+
+    class _L:  # four components: two spin-0 fields and a spin-2 field
+        lmin, lmax, n, nbins = 2, 10, 10 ** 6, 1
+        fields = [type("F", (), {"spin": s})() for s in (0, 0, 2)]
+
+    assert _resolve_method("auto", _L) == "pixel"
+    assert _resolve_method("harmonic", _L) == "harmonic"  # an explicit request is passed on (and raises later)
