@@ -5,6 +5,7 @@
     python -m cosmoforge_b200.kernel_bench dgemm M,N,K
     python -m cosmoforge_b200.kernel_bench spd_inverse N
     python -m cosmoforge_b200.kernel_bench harmonic 1        (config-1 harmonic-basis solve)
+    python -m cosmoforge_b200.kernel_bench map_solves NMAPS [--precision fp64|mixed]
 
 Each case fills seeded random operands on cuda:0, runs two untimed launches,
 then times `reps` launches with CUDA events on the launching stream and prints
@@ -160,14 +161,39 @@ def harmonic_case(which):
     return fn, flop, None
 
 
+def map_solves_case(nmaps, precision="mixed"):
+    """Raw q of nmaps seeded maps given C^-1 on the TQU nside-16 problem
+    (config 2 part 1): signal build, C^-1 and the maps are set up once; each
+    call is batch.map_solves (GEMMs against the derivative blocks and the
+    k_qform reductions)."""
+    from . import batch, qube, workloads
+    from .engine import Engine
+    from .layout import build_layout
+
+    pb = workloads.config1()
+    L = build_layout(pb.params, pb.mask, pb.beam)
+    E = Engine(L)
+    N = torch.from_numpy(pb.noise).cuda()
+    Cinv = E.spd_inverse(E.signal(L.smoothed_cl_table(pb.cls)) + N)
+    X = qube.draw_maps(L, pb.cls, N, nmaps, seed=0)
+
+    def fn():
+        batch.map_solves(E, Cinv, X, precision=precision)
+
+    fn._keep = (E, N, Cinv, X)
+    return fn, 0.0, None
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("case", choices=["umma_gemm", "umma_trace", "dgemm", "spd_inverse", "harmonic"])
+    ap.add_argument("case", choices=["umma_gemm", "umma_trace", "dgemm", "spd_inverse", "harmonic",
+                                           "map_solves"])
     ap.add_argument("shape", help="comma-separated sizes")
     ap.add_argument("--planes", type=int, default=3)
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--kc", type=int, default=16, help="promotion interval of the tensor-core kernels")
     ap.add_argument("--splits", type=int, default=0)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed", help="map_solves only")
     a = ap.parse_args(argv)
     dims = [int(x) for x in a.shape.split(",")]
     lib = _lib.lib()
@@ -180,11 +206,14 @@ def main(argv=None):
         fn, fl, err = dgemm_case(*dims)
     elif a.case == "harmonic":
         fn, fl, err = harmonic_case(*dims)
+    elif a.case == "map_solves":
+        fn, fl, err = map_solves_case(*dims, precision=a.precision)
     else:
         fn, fl, err = spd_inverse_case(*dims)
     ms = time_launches(fn, a.reps)
     bad = int(err.item()) if err is not None else 0
-    print(f"{a.case} {a.shape} planes={a.planes} kc={a.kc}: {ms:.3f} ms  {fl / ms / 1e9:.1f} TFLOP/s  err={bad}")
+    print(f"{a.case} {a.shape} planes={a.planes} kc={a.kc}: {ms:.3f} ms  {fl / ms / 1e9:.1f} TFLOP/s  err={bad}"
+          if fl else f"{a.case} {a.shape} {a.precision}: {ms:.3f} ms per call")
     if bad:
         raise SystemExit("a bounded device wait ran out")
 
