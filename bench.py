@@ -120,6 +120,25 @@ def cpu_threads() -> int:
         return os.cpu_count() or 1
 
 
+def max_over_ranks(value: float, world: int, device) -> float:
+    """The largest of a per-rank scalar over all ranks (a multi-GPU time is the
+    slowest replica's); the identity for one rank."""
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(units_per_rank: float, seconds_max: float, world: int) -> float:
+    """Whole-job throughput of `world` replicas that each processed
+    units_per_rank units, timed as the slowest rank."""
+    return world * units_per_rank / seconds_max
+
+
 def run_reference(args):
     """Reference arm: the oracle restatement on host cores (rank 0 only)."""
     rank = int(os.environ.get("RANK", "0"))
@@ -511,12 +530,8 @@ def main():
         torch.cuda.synchronize()
     barrier()
     launches = (lib.cf_launch_count() - n0) // max(args.steps, 1)
-    elapsed = t_start.elapsed_time(t_end) / 1e3
-    t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    elapsed = float(t.item())
-    value = world * args.steps / elapsed
+    elapsed = max_over_ranks(t_start.elapsed_time(t_end) / 1e3, world, dev)
+    value = job_throughput(args.steps, elapsed, world)
     clocks = clk.summary()
     tags = E.probe
     E.probe = None
@@ -543,16 +558,14 @@ def main():
         s1.record()
         torch.cuda.synchronize()
         t64 = s0.elapsed_time(s1) / 1e3
-        tt64 = torch.tensor([t64], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(tt64, op=dist.ReduceOp.MAX)
-        t64 = float(tt64.item())
+        t64 = max_over_ranks(t64, world, dev)
         dF = (F_m - F_d).abs()
         dg = torch.diagonal(F_d)
         sig = torch.diagonal(Finv_d).sqrt()
         fp64_leg = {
-            "value": world * args.fp64_steps / t64, "unit": UNIT, "ms_per_step": t64 / args.fp64_steps * 1e3,
-            "steps": args.fp64_steps, "mixed_over_fp64": (world * args.steps / elapsed) / (world * args.fp64_steps / t64),
+            "value": job_throughput(args.fp64_steps, t64, world), "unit": UNIT,
+            "ms_per_step": t64 / args.fp64_steps * 1e3, "steps": args.fp64_steps,
+            "mixed_over_fp64": job_throughput(args.steps, elapsed, world) / job_throughput(args.fp64_steps, t64, world),
             "mixed_error": {
                 "fisher_max_rel_diag": float((torch.diagonal(dF) / dg).max()),
                 "fisher_max_corr_normalised": float((dF / torch.sqrt(torch.outer(dg, dg))).max()),
@@ -583,11 +596,8 @@ def main():
                + clhat.nbytes)
         if i > 0:
             e2e_times.append(dt)
-    tt = torch.tensor([max(e2e_times) if e2e_times else float("nan")], dtype=torch.float64,
-                      device=dev)
-    if world > 1:
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-    e2e_value = world / float(tt.item()) if e2e_times else None
+    t_e2e = max_over_ranks(max(e2e_times) if e2e_times else float("nan"), world, dev)
+    e2e_value = job_throughput(1, t_e2e, world) if e2e_times else None
 
     line = None
     if rank == 0:
