@@ -75,6 +75,8 @@ def _check_basis(basis):
             raise NotImplementedError(f"basis options {sorted(unknown)} are not implemented")
         if basis.get("epsilon") is not None or basis.get("mode_fraction") is not None:
             # compression intent: the V-based pixel basis (cosmocore/core.py:940-950)
+            if method != "pixel":
+                raise NotImplementedError(f"basis={basis!r}: compression is implemented for method='pixel' only")
             return "compressed"
         return method
     raise TypeError(f"basis must be None/False/str/dict, got {type(basis).__name__}")

@@ -22,7 +22,9 @@ def test_basis_request(basis, method):
 
 
 @pytest.mark.parametrize("basis,exc", [("smw", ValueError), (3, TypeError), ({"method": "svd"}, ValueError),
-                                       ({"method": "pixel", "pixel_filter": 1}, NotImplementedError)])
+                                       ({"method": "pixel", "pixel_filter": 1}, NotImplementedError),
+                                       ({"epsilon": 1e-3}, NotImplementedError),
+                                       ({"method": "harmonic", "mode_fraction": 0.5}, NotImplementedError)])
 def test_basis_rejects(basis, exc):
     with pytest.raises(exc):
         _check_basis(basis)
