@@ -35,3 +35,20 @@ def test_bandpower_window_matches_reference(name, precision):
         assert e_w <= 1e-4 and e_l <= 1e-5
     # rows of W sum to one over each bin's own multipoles (W Q^T = I)
     assert W is f.get_bandpower_window_function()
+
+
+@pytest.mark.parametrize("basis", ["harmonic"])
+def test_bandpower_window_other_bases(basis):
+    """Per-multipole Fisher through the harmonic contractions: on the spin-0 TT
+    case (where the harmonic and pixel-space estimators agree to rounding) the
+    window and effective multipoles equal the pixel-space reference's."""
+    from cosmoforge_b200 import qube
+
+    d = load("bandpower_tt_nside8")
+    f = qube.Fisher(params_of(d), basis=basis, mask=d["mask"], noise_cov1=noise_of(d), cls_data=cls_of(d),
+                    beam=d["beam"])
+    f.run()
+    W = f.get_bandpower_window_function()
+    e_w, e_l = _rel(W, d["ref_window"]), _rel(f.get_effective_ells(), d["ref_eff_ells"])
+    print(f"{basis}: W {e_w:.1e}  l_eff {e_l:.1e}")
+    assert e_w <= 1e-9 and e_l <= 1e-9
