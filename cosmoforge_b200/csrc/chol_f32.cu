@@ -75,9 +75,11 @@ __global__ void __launch_bounds__(256) k_potrf_diag_inv_f32(float* A, long lda, 
         A[(long)(k0 + r) * lda + k0 + c] = (c <= r) ? S[r * LDS + c] : 0.0f;
     }
     // L11^-1 by column-oriented forward substitution: a warp per column c,
-    // lane l holding rows l and l + 32; x_t = acc_t / L_tt is broadcast and
-    // every later row subtracts L_rt x_t (the same terms in the same order as
-    // the row-oriented sum, so the same values)
+    // lane l holding rows l and l + 32; x_t = acc_t (1 / L_tt) is broadcast and
+    // every later row subtracts L_rt x_t (reciprocal pivots formed once)
+    __shared__ float rdiag[NB];
+    for (int t = tid; t < kb; t += blockDim.x) rdiag[t] = 1.0f / S[t * LDS + t];
+    __syncthreads();
     {
         const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
         for (int c = warp; c < kb; c += nw) {
@@ -85,7 +87,7 @@ __global__ void __launch_bounds__(256) k_potrf_diag_inv_f32(float* A, long lda, 
             float x0 = 0.0f, x1 = 0.0f;
             for (int t = c; t < kb; ++t) {
                 const float at = __shfl_sync(0xffffffffu, t < 32 ? a0 : a1, t & 31);
-                const float xt = at / S[t * LDS + t];
+                const float xt = at * rdiag[t];
                 if (lane == t) x0 = xt;
                 if (lane + 32 == t) x1 = xt;
                 if (lane > t) a0 -= S[lane * LDS + t] * xt;
