@@ -271,7 +271,7 @@ def secondary(args, dev):
     lnl = {"workload": "config3_tqu_nside8_lnl", "n_pixels": L.n, "points_per_batch": 1024,
            "fp64_evals_per_s": 1024 / res["fp64"][0] * 1e3, "mixed_evals_per_s": 1024 / res["mixed"][0] * 1e3,
            "mixed_max_abs_dlnL": float(d.max()), "mixed_form": "FP32 Cholesky, FP64-refined chi2"}
-    if int(os.environ.get("RANK", "0")) == 0 and not args.no_cpu_baseline:
+    if int(os.environ.get("WORLD_SIZE", "1")) == 1 and not args.no_cpu_baseline:
         from oracle import oracle as orc
 
         thc = workloads.sobol_points(8, seed=5)
@@ -621,7 +621,7 @@ def main():
         if tf.exists():
             traffic = _json.loads(tf.read_text()).get(f"{dom}_{args.precision}")
         cpu = None
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:  # the host baseline is an N = 1 figure
             pbc = workloads.config1()
             pbc.extra["maps"] = X.cpu().numpy()
             v, sample, _ = cpu_sample(pbc, L, k_params=2)
