@@ -31,3 +31,27 @@ extern unsigned long long g_cf_launch_count;
     } while (0)
 
 static inline int cf_cdiv(long a, long b) { return (int)((a + b - 1) / b); }
+
+#ifdef __cplusplus
+#include <atomic>
+
+#define CF_MAX_DEVICES 64
+
+// Opt `kernel` in to `bytes` of dynamic shared memory on the calling thread's
+// current device.  cudaFuncSetAttribute acts on the current device only, so
+// each call site keeps one flag per device (`done`, a zero-initialised static
+// array of CF_MAX_DEVICES); two host threads that race on a device's first
+// call both set the attribute, which is idempotent.  Devices past the table
+// set it on every call.
+template <typename K>
+static inline int cf_smem_optin(K* kernel, int bytes, std::atomic<int>* done)
+{
+    int dev = -1;
+    CF_CHECK(cudaGetDevice(&dev));
+    const bool tracked = dev >= 0 && dev < CF_MAX_DEVICES;
+    if (tracked && done[dev].load(std::memory_order_acquire)) return CF_OK;
+    CF_CHECK(cudaFuncSetAttribute((const void*)kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    if (tracked) done[dev].store(1, std::memory_order_release);
+    return CF_OK;
+}
+#endif

@@ -448,12 +448,9 @@ extern "C" int cf_chi2_logdet_mixed(int n, const float* L, long lda, long stride
     if (nrhs > 0) {
         if (!X || !C || !chi2) return CF_ERR_ARG;
         const size_t smem = 2 * (size_t)n * sizeof(double);
-        static bool attr = false;
-        if (!attr) {
-            CF_CHECK(cudaFuncSetAttribute(k_chi2_refined, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          2 * 12288 * (int)sizeof(double)));
-            attr = true;
-        }
+        static std::atomic<int> attr[CF_MAX_DEVICES];
+        int rc = cf_smem_optin(k_chi2_refined, 2 * 12288 * (int)sizeof(double), attr);
+        if (rc) return rc;
         k_chi2_refined<<<batch * nrhs, CNT, smem, st>>>(n, L, lda, strideL, C, ldc, strideC, X, ldx, strideX, nrhs,
                                                        chi2);
         CF_CHECK_LAUNCH();

@@ -188,11 +188,8 @@ extern "C" int cf_potrf(int n, double* A, long lda, long strideA, int batch, voi
     if (n <= 0 || batch < 1 || !A || !work) return CF_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     constexpr size_t DIAG_SMEM = 2 * NB * LDS * sizeof(double);
-    static bool attr = false;
-    if (!attr) {
-        CF_CHECK(cudaFuncSetAttribute(k_potrf_diag_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DIAG_SMEM));
-        attr = true;
-    }
+    static std::atomic<int> attr[CF_MAX_DEVICES];
+    if (int rc0 = cf_smem_optin(k_potrf_diag_inv, (int)DIAG_SMEM, attr)) return rc0;
     const long ws = (long)potrf_ws(n);
     double* Dinv = (double*)work;                   // [batch][nblocks][NB][NB]
     double* W = Dinv + (long)nblocks(n) * NB * NB;  // [batch][n][2 NB] (same stride ws)
@@ -320,13 +317,15 @@ extern "C" int cf_spd_inverse(int n, double* A, long lda, long strideA, int batc
 }
 
 // ---------------------------------------------------------------------------
-// Allocation-free variant of cf_spd_inverse for callers that cannot allocate
-// device memory: code running inside a host callback or a custom allocator's
-// own hooks, plugins whose host forbids cudaMalloc after start-up, or
-// integrations that must not fragment a pool they do not own.  Its workspace
-// (L^-1, the Jacobi scale factors, the diagonal-block inverses and one panel)
-// lives in this file-scope array, which every GPU that loads the library holds
-// until the process exits: 1.25 M doubles = 10.0 MB per device.
+// Allocation-free variant of cf_spd_inverse for callers that must not
+// allocate device memory where they need the inverse: allocator hooks,
+// plugins whose host application owns the memory pool and forbids allocations
+// after start-up, integrations that must not fragment a pool they do not own.
+// It launches kernels, so it is not for use inside a host callback, where CUDA
+// calls are not permitted.  Its workspace (L^-1, the Jacobi scale factors, the
+// diagonal-block inverses and one panel) lives in this file-scope array: a
+// device allocates it when this module is first used there (lazy module
+// loading) and holds it until the process exits, 1.25 M doubles = 10.0 MB.
 #define CF_SPD_STATIC_MAX_N 1024
 static __device__ __align__(256) double g_spd_static_scratch[(size_t)CF_SPD_STATIC_MAX_N * CF_SPD_STATIC_MAX_N +
                                                              CF_SPD_STATIC_MAX_N +
@@ -350,7 +349,10 @@ int static_scratch(double** out)
     if (g_static_ptr[dev] == nullptr) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_spd_static_scratch);
-        if (e != cudaSuccess || p == nullptr) return CF_ERR_CUDA;
+        if (e != cudaSuccess || p == nullptr) {
+            (void)cudaGetLastError();  // do not leave the error for an unrelated later launch check
+            return CF_ERR_CUDA;
+        }
         g_static_ptr[dev] = static_cast<double*>(p);
     }
     *out = g_static_ptr[dev];
@@ -362,7 +364,8 @@ extern "C" int cf_spd_inverse_static_max_n(void) { return CF_SPD_STATIC_MAX_N; }
 
 // Same result as cf_spd_inverse(n, A, lda, n*n, 1, work, info, stream) with no
 // caller workspace and no allocation.  The first call on a device looks up the
-// scratch address (make it before any stream capture).  All calls share one
+// scratch address and sets kernel attributes: make it at start-up, outside
+// the no-allocation context and before any stream capture.  All calls share one
 // scratch array: calls whose work overlaps on the GPU (different streams or
 // host threads on the same device) race.  Every scratch element the routine
 // reads is written by it first, so stale contents from a previous call do not

@@ -197,11 +197,8 @@ extern "C" int cf_trace_contract_f64(int P1, int P2, int K1, int K2, const doubl
     if (splits > T) splits = (int)T;
     dim3 grid(splits, cf_cdiv(P1, TBM), cf_cdiv(P2, TBN));
     const size_t smem = (size_t)TST * (TBM + TBN) * TPAD * sizeof(double);
-    static bool attr = false;
-    if (!attr) {
-        CF_CHECK(cudaFuncSetAttribute(k_trace_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr = true;
-    }
+    static std::atomic<int> attr[CF_MAX_DEVICES];
+    if (int rc = cf_smem_optin(k_trace_f64, (int)smem, attr)) return rc;
     k_trace_f64<<<grid, TNT, smem, (cudaStream_t)stream>>>(P1, P2, K1, K2, X, sXp, ldX, Y, sYq, ldY, scale,
                                                         F, ldF, p_off, q_off, sym);
     CF_CHECK_LAUNCH();

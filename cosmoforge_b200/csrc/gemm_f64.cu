@@ -184,12 +184,8 @@ int launch(int M, int N, int K, double alpha, const double* A, long lda, long sA
 {
     constexpr int SA = TileShape<AT>::elems, SB = TileShape<!BT>::elems;
     const size_t smem = (size_t)STAGES * (SA + SB) * sizeof(double);
-    static bool attr_set = false;
-    if (!attr_set) {
-        CF_CHECK(cudaFuncSetAttribute(k_dgemm<AT, BT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
-        attr_set = true;
-    }
+    static std::atomic<int> attr[CF_MAX_DEVICES];
+    if (int rc = cf_smem_optin(k_dgemm<AT, BT>, (int)smem, attr)) return rc;
     dim3 grid(cf_cdiv(N, BN), cf_cdiv(M, BM), batch);
     k_dgemm<AT, BT><<<grid, NT, smem, st>>>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC,
                                             CT, ldct, sCT, lower_only);

@@ -566,12 +566,8 @@ int launch_gemm_kc(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, i
     const size_t smem = 1024 + (size_t)STAGES * PLS * (BM * BKT * 2 + BN * BKT * 2) + 256;
     static_assert(1024 + (size_t)STAGES * PLS * (BM * BKT * 2 + BN * BKT * 2) + 256 <= 232448,
                   "shared memory ring exceeds 227 KB");
-    static bool attr = false;
-    if (!attr) {
-        CF_CHECK(cudaFuncSetAttribute(k_umma_gemm<BN, STAGES, TRACE, KC, PLS, BKT, SPLIT>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr = true;
-    }
+    static std::atomic<int> attr[CF_MAX_DEVICES];
+    if (int rc = cf_smem_optin(k_umma_gemm<BN, STAGES, TRACE, KC, PLS, BKT, SPLIT>, (int)smem, attr)) return rc;
     int dev = 0, sms = 0;
     CF_CHECK(cudaGetDevice(&dev));
     CF_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));

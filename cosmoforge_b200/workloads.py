@@ -202,10 +202,14 @@ def model_cls(theta, lmax: int) -> dict:
 
 
 def config3(lmax_signal: int = 23, nsims: int = 1) -> SkyProblem:
-    """nside 8 TQU likelihood: T |z| > sin 20 (480 px), Q/U |z| > sin 30 (384 px).
+    """nside 8 TQU likelihood: T |z| > sin 20 (480 px), Q/U |z| > sin 30 (416 px per field).
 
-    n = 1248, l = 2..23 with lmax_signal = 23.  Beam as config 0; white noise
-    sigma_T^2 = 4 muK^2, sigma_Q^2 = sigma_U^2 = 8 muK^2 (scaled by s).
+    n = 480 + 2 x 416 = 1312, l = 2..23 with lmax_signal = 23.  nside 8 has
+    two rings of 32 pixels at z = +-0.5 exactly, and sin 30 deg rounds to
+    0.49999999999999994 in FP64, so both pass the strict cut: 352 + 64 = 416
+    pixels per field.
+    Beam as config 0; white noise sigma_T^2 = 4 muK^2, sigma_Q^2 = sigma_U^2 =
+    8 muK^2 (scaled by s).
     """
     nside = 8
     mt = z_cut_mask(nside, SIN20)

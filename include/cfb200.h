@@ -126,16 +126,24 @@ int cf_spd_inverse(int n, double* A, long lda, long strideA, int batch, void* wo
                    void* stream);
 
 /*
- * Allocation-free SPD inverse: cf_spd_inverse for one n x n matrix with its
- * workspace taken from a scratch array compiled into the library (a
- * file-scope __device__ array of 1.25 M doubles, 10.0 MB held by every
- * GPU that loads the library until exit), for callers that cannot call
- * cudaMalloc (host callbacks, allocator hooks, plugins whose host owns the
- * memory pool).  Allocates nothing.  n > cf_spd_inverse_static_max_n()
- * returns CF_ERR_TOO_LARGE.  The first call on a device looks up the
- * scratch address (cudaGetSymbolAddress), so make it before any stream
- * capture.  All calls share the one array: calls that overlap on the GPU
- * race.  *info is zeroed on `stream` by the call.
+ * Allocation-free SPD inverse: cf_spd_inverse for one n x n matrix whose
+ * workspace is a scratch array compiled into the library (a file-scope
+ * __device__ array of 1.25 M doubles, 10.0 MB per device).  It serves
+ * callers that must not allocate device memory at the point where they need
+ * the inverse: allocator hooks, plugins whose host application owns the
+ * memory pool and forbids allocations after start-up, and integrations that
+ * must not fragment a pool they do not own.  It launches kernels and makes
+ * CUDA runtime calls, so it must not be called from inside a host callback
+ * (cudaLaunchHostFunc, cudaStreamAddCallback), where CUDA calls are not
+ * permitted.  With lazy module loading (the CUDA 12 default) a device
+ * allocates the array when the module that holds it is first used there,
+ * and the first call on a device also looks up the array's address
+ * (cudaGetSymbolAddress) and sets kernel attributes: make one warm-up call
+ * per device at start-up, outside the no-allocation context and before any
+ * stream capture; later calls allocate nothing.
+ * n > cf_spd_inverse_static_max_n() returns CF_ERR_TOO_LARGE.  All calls
+ * share the one array: calls that overlap on the GPU race.  *info is zeroed
+ * on `stream` by the call.
  * No counterpart in the reference (an addition of this library).
  */
 int cf_spd_inverse_static(int n, double* A, long lda, int* info, void* stream);

@@ -12,11 +12,11 @@ reference's own tests ship them, the Fortran known answers.
 
 Usage::
 
-    python tests/golden/make_golden.py [case ...]
+    COSMOFORGE_REFERENCE=<reference checkout> python tests/golden/make_golden.py [case ...]
 
-Run it where the reference sources are available (default location
-``/root/reference``, override with ``COSMOFORGE_REFERENCE``).  The fixtures
-it writes are small and committed, so tests never need the reference.
+``COSMOFORGE_REFERENCE`` names the root of a checkout of the reference
+sources (the directory holding ``src/cosmoforge.*``).  The fixtures it
+writes are small and committed, so tests never need the reference.
 """
 
 from __future__ import annotations
@@ -30,7 +30,9 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parent.parent
-REF = Path(os.environ.get("COSMOFORGE_REFERENCE", "/root/reference")) / "src"
+if not os.environ.get("COSMOFORGE_REFERENCE"):
+    raise SystemExit("set COSMOFORGE_REFERENCE to the root of a reference checkout")
+REF = Path(os.environ["COSMOFORGE_REFERENCE"]) / "src"
 QUBE_DATA = REF / "cosmoforge.qube" / "tests" / "data"
 PL_DATA = REF / "cosmoforge.picslike" / "tests" / "data"
 

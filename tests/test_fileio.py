@@ -2,8 +2,9 @@
 
 The nside-4 fixtures were produced by the reference from its own test data
 (mask.fits, NCVM1.bin, dls.txt, the beam table, all_sims_TQU.fits); reading the
-same files here must give the same arrays.  Skipped when the reference tree
-is not present.  Round trips of the plain formats run everywhere.
+same files here must give the same arrays.  That test reads the reference's
+data files from the checkout named by ``COSMOFORGE_REFERENCE`` and is skipped
+when the variable is unset.  Round trips of the plain formats run everywhere.
 """
 
 import os
@@ -16,8 +17,8 @@ from cosmoforge_b200 import fileio, params as prm
 from cosmoforge_b200.layout import build_layout
 from golden_cases import cls_of, load, params_of
 
-REF = Path(os.environ.get("COSMOFORGE_REFERENCE", "/root/reference")) / "src"
-QDATA = REF / "cosmoforge.qube" / "tests" / "data"
+_REF_ROOT = os.environ.get("COSMOFORGE_REFERENCE")
+QDATA = (Path(_REF_ROOT) / "src" / "cosmoforge.qube" / "tests" / "data") if _REF_ROOT else None
 
 
 def test_covmat_and_cls_round_trip(tmp_path):
@@ -50,7 +51,7 @@ def test_gaussian_beam_polarisation_factor():
     assert np.allclose(b[1], b[0] * np.exp(2 * s2), rtol=1e-14) and np.array_equal(b[1], b[2])
 
 
-@pytest.mark.skipif(not QDATA.exists(), reason="reference test data not present")
+@pytest.mark.skipif(QDATA is None or not QDATA.exists(), reason="COSMOFORGE_REFERENCE not set")
 @pytest.mark.parametrize("fields", ["T", "TQU"])
 def test_reference_files_give_the_fixture_arrays(fields):
     import yaml

@@ -1,15 +1,16 @@
 """Allocation-free SPD inverse (cf_spd_inverse_static) against cf_spd_inverse.
 
-Some callers of this library cannot allocate device memory at the point
-where they need an inverse: code running inside a host callback or an
-allocator hook, or a plugin whose host application owns the memory pool and
-forbids new allocations after start-up.  ``cf_spd_inverse_static`` serves them
-from a fixed scratch array compiled into the library.  This test calls it
-through the C ABI twice in a row (different sizes, so the second call runs on
-the stale scratch contents of the first) and once more at the first size,
-and compares each result with the workspace-taking ``cf_spd_inverse`` on the
-same matrix, at the 1e-12 tolerance used for the FP64 inverse.  It also checks
-that sizes above the stated maximum are refused.
+Some callers of this library must not allocate device memory at the point
+where they need an inverse: an allocator hook, or a plugin whose host
+application owns the memory pool and forbids new allocations after start-up.
+``cf_spd_inverse_static`` serves them from a fixed scratch array compiled into
+the library.  This test calls it through the C ABI twice in a row (different
+sizes, so the second call runs on the stale scratch contents of the first) and
+once more at the first size, and compares each result with the
+workspace-taking ``cf_spd_inverse`` on the same matrix, at the 1e-12 tolerance
+used for the FP64 inverse.  After a warm-up call it checks that a call leaves
+the device's free memory unchanged, and that sizes above the stated maximum
+are refused.
 
 The file name sorts last so that a ``-x`` run reaches it after every other test.
 """
@@ -75,3 +76,27 @@ def test_static_scratch_rejects_oversized_problems():
     rc = lib.cf_spd_inverse_static(nmax + 1, A.data_ptr(), nmax + 1, info.data_ptr(),
                                    torch.cuda.current_stream().cuda_stream)
     assert rc == _lib.CF_ERR_TOO_LARGE
+
+
+def test_static_scratch_inverse_allocates_nothing():
+    from cosmoforge_b200 import _lib
+
+    lib = _lib.lib()
+    n = 512
+    M = _spd(n, 4)
+    A = torch.from_numpy(M).cuda()
+    A0 = A.clone()
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    # warm-up: module load, scratch address look-up, kernel attributes
+    assert lib.cf_spd_inverse_static(n, A.data_ptr(), n, info.data_ptr(), st) == 0
+    torch.cuda.synchronize()
+    A.copy_(A0)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    assert lib.cf_spd_inverse_static(n, A.data_ptr(), n, info.data_ptr(), st) == 0
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free1 == free0
+    assert int(info.item()) == 0
+    assert np.allclose(A.cpu().numpy() @ M, np.eye(n), atol=1e-9)
