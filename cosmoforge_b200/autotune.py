@@ -160,8 +160,7 @@ def tune_fisher(E, Cinv: torch.Tensor, scheme: str = "bf16x6", tol: float = 6e-6
                     err = max(err, abs(_trace_AA(cols, L) / ref - 1.0))
                 results.append((ms, err, ap, kc))
             del outs
-            if int(plan.err.item()) != 0:
-                raise RuntimeError("tensor-core kernel reported a timed-out wait while tuning")
+            check(lib.cf_umma_status(plan.err.data_ptr(), stream()), "tensor-core kernel while tuning")
             floor = min(r[1] for r in results)
             ok = [r for r in results if r[1] <= max(tol, slack * floor)]
             best = min(ok)

@@ -86,8 +86,7 @@ def map_solves(E: eng.Engine, Cinv: torch.Tensor, X: torch.Tensor, precision: st
                                             q.data_ptr(), P, s * nb, st), "cf_qform_reduce_f32")
             del W
         del ops
-    if int(plan.err.item()) != 0:
-        raise RuntimeError("tensor-core kernel reported a timed-out wait")
+    check(E.lib.cf_umma_status(plan.err.data_ptr(), stream()), "tensor-core kernel")
     return q
 
 

@@ -15,95 +15,13 @@
 // order in the factor's backward error.  ln|C| = 2 sum ln L_ii carries the
 // factor's first-order error.
 #include "cf_common.cuh"
+#include "potrf_diag.cuh"
 
 namespace {
 
-constexpr int NB = 64;
-constexpr int LDS = NB + 1;
+constexpr int NB = cf_diag::NB;
 
-// Factor the kb x kb diagonal block at (k0, k0) of every batch matrix in place
-// (FP32) and write L11^-1 to Dinv (kb x kb, row-major).  One barrier per
-// column: the scaling of column j is folded into step j + 1.
-__global__ void __launch_bounds__(256) k_potrf_diag_inv_f32(float* A, long lda, long sA, int k0, int kb, float* Dinv,
-                                                            long sD, int* info)
-{
-    __shared__ float S[NB * LDS];
-    __shared__ float Xs[NB * LDS];
-    __shared__ float piv[NB];
-    __shared__ int bad;
-    const int b = blockIdx.x;
-    A += b * sA;
-    Dinv += b * sD;
-    const int tid = threadIdx.x;
-    for (int e = tid; e < kb * kb; e += blockDim.x) {
-        const int r = e / kb, c = e % kb;
-        S[r * LDS + c] = (c <= r) ? A[(long)(k0 + r) * lda + k0 + c] : 0.0f;
-    }
-    if (tid == 0) bad = 0;
-    __syncthreads();
-    for (int j = 0; j < kb; ++j) {
-        float d = S[j * LDS + j];
-        if (!(d > 0.0f)) {  // also catches NaN
-            if (tid == 0 && !bad) bad = k0 + j + 1;
-            d = 1.0f;
-        }
-        if (tid == 0) piv[j] = sqrtf(d);
-        const float inv_d = 1.0f / d;
-        // trailing update with the unscaled column j; column j - 1 gets its scaling now.
-        // The m x m trailing square is flattened over all threads (independent
-        // entries, so their shared-memory latencies overlap); entries above the
-        // diagonal are skipped
-        {
-            const int m = kb - j - 1;
-            for (int e = tid; e < m * m; e += blockDim.x) {
-                const int rr = j + 1 + e / m, cc = j + 1 + e % m;
-                if (cc <= rr) {
-                    const float srj = S[rr * LDS + j] * inv_d;
-                    S[rr * LDS + cc] -= srj * S[cc * LDS + j];
-                }
-            }
-        }
-        if (j > 0)
-            for (int r = j + tid; r < kb; r += blockDim.x) S[r * LDS + j - 1] /= piv[j - 1];
-        __syncthreads();
-    }
-    // the last column has no entries below its diagonal, which becomes piv
-    for (int r = tid; r < kb; r += blockDim.x) S[r * LDS + r] = piv[r];
-    __syncthreads();
-    for (int e = tid; e < kb * kb; e += blockDim.x) {
-        const int r = e / kb, c = e % kb;
-        A[(long)(k0 + r) * lda + k0 + c] = (c <= r) ? S[r * LDS + c] : 0.0f;
-    }
-    // L11^-1 by column-oriented forward substitution: a warp per column c,
-    // lane l holding rows l and l + 32; x_t = acc_t (1 / L_tt) is broadcast and
-    // every later row subtracts L_rt x_t (reciprocal pivots formed once)
-    __shared__ float rdiag[NB];
-    for (int t = tid; t < kb; t += blockDim.x) rdiag[t] = 1.0f / S[t * LDS + t];
-    __syncthreads();
-    {
-        const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-        for (int c = warp; c < kb; c += nw) {
-            float a0 = (lane == c) ? 1.0f : 0.0f, a1 = (lane + 32 == c) ? 1.0f : 0.0f;
-            float x0 = 0.0f, x1 = 0.0f;
-            for (int t = c; t < kb; ++t) {
-                const float at = __shfl_sync(0xffffffffu, t < 32 ? a0 : a1, t & 31);
-                const float xt = at * rdiag[t];
-                if (lane == t) x0 = xt;
-                if (lane + 32 == t) x1 = xt;
-                if (lane > t) a0 -= S[lane * LDS + t] * xt;
-                if (lane + 32 > t && lane + 32 < kb) a1 -= S[(lane + 32) * LDS + t] * xt;
-            }
-            if (lane < kb) Xs[lane * LDS + c] = x0;
-            if (lane + 32 < kb) Xs[(lane + 32) * LDS + c] = x1;
-        }
-    }
-    __syncthreads();
-    for (int e = tid; e < kb * kb; e += blockDim.x) {
-        const int r = e / kb, c = e % kb;
-        Dinv[r * kb + c] = Xs[r * LDS + c];
-    }
-    if (tid == 0 && bad && info && info[b] == 0) info[b] = bad;
-}
+using cf_diag::k_potrf_diag_inv;
 
 // FP32 SIMT GEMM, both operands K-contiguous (the "NT" form):
 //   C[M x N] = alpha A[M x K] B[N x K]^T + beta C, batch on blockIdx.z.
@@ -385,7 +303,7 @@ extern "C" int cf_potrf_f32(int n, float* A, long lda, long strideA, int batch, 
     // update per 128 columns.
     for (int k0 = 0; k0 < n; k0 += 2 * NB) {
         const int kb1 = n - k0 < NB ? n - k0 : NB;
-        k_potrf_diag_inv_f32<<<batch, 256, 0, st>>>(A, lda, strideA, k0, kb1, D1, ws, info);
+        k_potrf_diag_inv<float><<<batch, cf_diag::NTHREADS, cf_diag::smem_bytes<float>(), st>>>(A, lda, strideA, k0, kb1, D1, ws, info);
         CF_CHECK_LAUNCH();
         const int rest1 = n - k0 - kb1;
         if (rest1 <= 0) break;
@@ -399,7 +317,7 @@ extern "C" int cf_potrf_f32(int n, float* A, long lda, long strideA, int batch, 
                                                                                               a21_1, lda, strideA);
         CF_CHECK_LAUNCH();
         const int k1 = k0 + kb1;
-        k_potrf_diag_inv_f32<<<batch, 256, 0, st>>>(A, lda, strideA, k1, kb2, D2, ws, info);
+        k_potrf_diag_inv<float><<<batch, cf_diag::NTHREADS, cf_diag::smem_bytes<float>(), st>>>(A, lda, strideA, k1, kb2, D2, ws, info);
         CF_CHECK_LAUNCH();
         const int rest2 = rest1 - kb2;
         if (rest2 <= 0) break;

@@ -3,13 +3,14 @@
 // Restates the reference's matrix_inverse_symm (cosmocore/basics/linalg.py:
 // 152-219): Jacobi scaling D M D with D = diag(|M_ii|^-1/2), Cholesky, inverse
 // from the factor, unscaling D (.) D.  The factorisation is right-looking with
-// 64-wide panels: one CTA factors the diagonal block, a row-parallel kernel
-// solves the panel below it, and the trailing update is a lower-only DMMA
-// GEMM.  The inverse solves L Y = I block row by block row (an in-place
+// 64-wide panels: one CTA factors the diagonal block and inverts its factor
+// (potrf_diag.cuh), the panel below is a DMMA GEMM against that inverse, and
+// the trailing update is a lower-only DMMA GEMM.  The inverse solves L Y = I block row by block row (an in-place
 // triangular solve per diagonal block plus a DMMA GEMM update), then forms
 // C^-1 = Y^T Y with one lower-only GEMM.  Per-problem status `info` follows
 // LAPACK: 0 = success, k > 0 = the leading minor of order k is not positive.
 #include "cf_common.cuh"
+#include "potrf_diag.cuh"
 
 #include <mutex>
 
@@ -20,95 +21,9 @@ extern "C" int cf_dgemm(int transa, int transb, int M, int N, int K, double alph
 
 namespace {
 
-constexpr int NB = 64;
-constexpr int LDS = NB + 1;
+constexpr int NB = cf_diag::NB;
 
-// Factor the kb x kb diagonal block at (k0, k0) of each batch matrix in place
-// (right-looking, one barrier per column: the scaling of column j is folded
-// into step j + 1) and write L11^-1 to Dinv (kb x kb, row-major, lower).
-__global__ void __launch_bounds__(256) k_potrf_diag_inv(double* A, long lda, long sA, int k0, int kb, double* Dinv,
-                                                        long sD, int* info)
-{
-    extern __shared__ double dsm[];
-    double* S = dsm;             // the block, then L11
-    double* Xs = dsm + NB * LDS;  // L11^-1
-    __shared__ double piv[NB];
-    __shared__ int bad;
-    const int b = blockIdx.x;
-    A += b * sA;
-    Dinv += b * sD;
-    const int tid = threadIdx.x;
-    for (int e = tid; e < kb * kb; e += blockDim.x) {
-        int r = e / kb, c = e % kb;
-        S[r * LDS + c] = (c <= r) ? A[(long)(k0 + r) * lda + k0 + c] : 0.0;
-    }
-    if (tid == 0) bad = 0;
-    __syncthreads();
-    for (int j = 0; j < kb; ++j) {
-        double d = S[j * LDS + j];
-        if (!(d > 0.0)) {  // also catches NaN
-            if (tid == 0 && !bad) bad = k0 + j + 1;
-            d = 1.0;
-        }
-        if (tid == 0) piv[j] = sqrt(d);
-        const double inv_d = 1.0 / d;
-        // trailing update with the unscaled column j; column j - 1 gets its scaling now.
-        // The m x m trailing square is flattened over all threads (independent
-        // entries, so their shared-memory latencies overlap); entries above the
-        // diagonal are skipped
-        {
-            const int m = kb - j - 1;
-            for (int e = tid; e < m * m; e += blockDim.x) {
-                const int rr = j + 1 + e / m, cc = j + 1 + e % m;
-                if (cc <= rr) {
-                    const double srj = S[rr * LDS + j] * inv_d;
-                    S[rr * LDS + cc] -= srj * S[cc * LDS + j];
-                }
-            }
-        }
-        if (j > 0)
-            for (int r = j + tid; r < kb; r += blockDim.x) S[r * LDS + j - 1] /= piv[j - 1];
-        __syncthreads();
-    }
-    // the last column has no entries below its diagonal, which becomes piv
-    for (int r = tid; r < kb; r += blockDim.x) S[r * LDS + r] = piv[r];
-    __syncthreads();
-    for (int e = tid; e < kb * kb; e += blockDim.x) {
-        int r = e / kb, c = e % kb;
-        A[(long)(k0 + r) * lda + k0 + c] = (c <= r) ? S[r * LDS + c] : 0.0;
-    }
-    // L11^-1 by column-oriented forward substitution: a warp per column c,
-    // lane l holding rows l and l + 32; x_t = acc_t (1 / L_tt) is broadcast and
-    // every later row subtracts L_rt x_t.  The reciprocal pivots are formed
-    // once (a division is a long instruction sequence and this loop is
-    // latency-bound)
-    __shared__ double rdiag[NB];
-    for (int t = tid; t < kb; t += blockDim.x) rdiag[t] = 1.0 / S[t * LDS + t];
-    __syncthreads();
-    {
-        const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-        for (int c = warp; c < kb; c += nw) {
-            double a0 = (lane == c) ? 1.0 : 0.0, a1 = (lane + 32 == c) ? 1.0 : 0.0;
-            double x0 = 0.0, x1 = 0.0;
-            for (int t = c; t < kb; ++t) {
-                const double at = __shfl_sync(0xffffffffu, t < 32 ? a0 : a1, t & 31);
-                const double xt = at * rdiag[t];
-                if (lane == t) x0 = xt;
-                if (lane + 32 == t) x1 = xt;
-                if (lane > t) a0 -= S[lane * LDS + t] * xt;
-                if (lane + 32 > t && lane + 32 < kb) a1 -= S[(lane + 32) * LDS + t] * xt;
-            }
-            if (lane < kb) Xs[lane * LDS + c] = x0;
-            if (lane + 32 < kb) Xs[(lane + 32) * LDS + c] = x1;
-        }
-    }
-    __syncthreads();
-    for (int e = tid; e < kb * kb; e += blockDim.x) {
-        int r = e / kb, c = e % kb;
-        Dinv[r * kb + c] = Xs[r * LDS + c];
-    }
-    if (tid == 0 && bad && info && info[b] == 0) info[b] = bad;
-}
+using cf_diag::k_potrf_diag_inv;
 
 // Batched 2D copy: dst[r * ldd + c] = src[r * lds + c], r < R, c < C.
 __global__ void k_copy2d(int R, int C, const double* src, long lds, long ss, double* dst, long ldd, long sd)
@@ -140,14 +55,6 @@ __global__ void k_scale_sym(double* A, long lda, long sA, int n, const double* d
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     int r = blockIdx.y * blockDim.y + threadIdx.y;
     if (r < n && c < n && (!lower || c <= r)) A[(long)r * lda + c] *= d[r] * d[c];
-}
-
-__global__ void k_set_identity(double* Y, long ldy, long sY, int n)
-{
-    Y += blockIdx.z * sY;
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    int r = blockIdx.y * blockDim.y + threadIdx.y;
-    if (r < n && c < n) Y[(long)r * ldy + c] = (r == c) ? 1.0 : 0.0;
 }
 
 // Full symmetric result from the lower triangle, with the Jacobi unscaling.
@@ -187,9 +94,9 @@ extern "C" int cf_potrf(int n, double* A, long lda, long strideA, int batch, voi
 {
     if (n <= 0 || batch < 1 || !A || !work) return CF_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
-    constexpr size_t DIAG_SMEM = 2 * NB * LDS * sizeof(double);
+    constexpr size_t DIAG_SMEM = cf_diag::smem_bytes<double>();
     static std::atomic<int> attr[CF_MAX_DEVICES];
-    if (int rc0 = cf_smem_optin(k_potrf_diag_inv, (int)DIAG_SMEM, attr)) return rc0;
+    if (int rc0 = cf_smem_optin(k_potrf_diag_inv<double>, (int)DIAG_SMEM, attr)) return rc0;
     const long ws = (long)potrf_ws(n);
     double* Dinv = (double*)work;                   // [batch][nblocks][NB][NB]
     double* W = Dinv + (long)nblocks(n) * NB * NB;  // [batch][n][2 NB] (same stride ws)
@@ -201,7 +108,7 @@ extern "C" int cf_potrf(int n, double* A, long lda, long strideA, int batch, voi
     int blk = 0;
     for (int k0 = 0; k0 < n; k0 += 2 * NB) {
         const int kb1 = n - k0 < NB ? n - k0 : NB;
-        k_potrf_diag_inv<<<batch, 256, DIAG_SMEM, st>>>(A, lda, strideA, k0, kb1, Dinv + (long)blk * NB * NB, ws,
+        k_potrf_diag_inv<double><<<batch, cf_diag::NTHREADS, DIAG_SMEM, st>>>(A, lda, strideA, k0, kb1, Dinv + (long)blk * NB * NB, ws,
                                                         info);
         CF_CHECK_LAUNCH();
         const double* D1 = Dinv + (long)blk * NB * NB;
@@ -222,7 +129,7 @@ extern "C" int cf_potrf(int n, double* A, long lda, long strideA, int batch, voi
                                                                                           a21_1, lda, strideA);
         CF_CHECK_LAUNCH();
         const int k1 = k0 + kb1;
-        k_potrf_diag_inv<<<batch, 256, DIAG_SMEM, st>>>(A, lda, strideA, k1, kb2, Dinv + (long)blk * NB * NB, ws,
+        k_potrf_diag_inv<double><<<batch, cf_diag::NTHREADS, DIAG_SMEM, st>>>(A, lda, strideA, k1, kb2, Dinv + (long)blk * NB * NB, ws,
                                                         info);
         CF_CHECK_LAUNCH();
         const double* D2 = Dinv + (long)blk * NB * NB;
@@ -246,34 +153,90 @@ extern "C" int cf_potrf(int n, double* A, long lda, long strideA, int batch, voi
     return CF_OK;
 }
 
+namespace {
+// dst[r * ld + c] = v for r < R, c < C; batch (or pair) z advances dst by sd.
+__global__ void k_fill2d(int R, int C, double* dst, long ld, long sd, double v)
+{
+    dst += blockIdx.z * sd;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y * blockDim.y + threadIdx.y;
+    if (r < R && c < C) dst[(long)r * ld + c] = v;
+}
+
+// Y's diagonal 64-blocks <- the inverses cf_potrf left in `work`
+// (block b: kb x kb row-major at Dinv + b NB^2); grid (blocks, batch).
+__global__ void k_place_diag_inv(const double* Dinv, long sD, int n, double* Y, long ldy, long sY)
+{
+    const int blk = blockIdx.x;
+    Y += blockIdx.y * sY;
+    Dinv += blockIdx.y * sD + (long)blk * NB * NB;
+    const int k0 = blk * NB, kb = n - k0 < NB ? n - k0 : NB;
+    for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
+        const int r = e / kb, c = e - (e / kb) * kb;
+        Y[(long)(k0 + r) * ldy + k0 + c] = Dinv[r * kb + c];
+    }
+}
+
+// One merge step for `np` pairs of adjacent diagonal blocks (sizes s and s2)
+// whose inverses Y11, Y22 are in place: Y21 = -Y22 L21 Y11.  The first pair's
+// leading block starts at row / column c0; pairs are 2 s apart.  T^T =
+// Y11^T L21^T is staged in the (still zero) upper block of the pair and
+// cleared afterwards, so Y stays lower triangular.
+int merge_pairs(int s, int s2, int np, long c0, const double* L, long lda, long sL, double* Y, long ldy, long sY,
+                int batch, cudaStream_t st, void* stream)
+{
+    const long r0 = c0 + s;
+    const long pL = 2L * s * (lda + 1), pY = 2L * s * (ldy + 1);
+    // batch over pairs for one problem, or over problems pair by pair
+    const int outer = batch == 1 ? 1 : np;
+    const int inner = batch == 1 ? np : batch;
+    const long iL = batch == 1 ? pL : sL, iY = batch == 1 ? pY : sY;
+    for (int o = 0; o < outer; ++o) {
+        const double* l21 = L + (r0 + (long)o * 2 * s) * lda + c0 + (long)o * 2 * s;
+        double* y11 = Y + (c0 + (long)o * 2 * s) * (ldy + 1);
+        double* y22 = Y + (r0 + (long)o * 2 * s) * (ldy + 1);
+        double* tt = y11 + s;            // upper block (rows of block 1, columns of block 2)
+        double* y21 = y22 - s;           // lower block (rows of block 2, columns of block 1)
+        int rc = cf_dgemm(1, 1, s, s2, s, 1.0, y11, ldy, iY, l21, lda, iL, 0.0, tt, ldy, iY, nullptr, 0, 0, inner,
+                          2, stream);
+        if (rc) return rc;
+        rc = cf_dgemm(0, 1, s2, s, s2, -1.0, y22, ldy, iY, tt, ldy, iY, 0.0, y21, ldy, iY, nullptr, 0, 0, inner, 4,
+                      stream);
+        if (rc) return rc;
+        k_fill2d<<<dim3(cf_cdiv(s2, 32), cf_cdiv(s, 8), inner), dim3(32, 8), 0, st>>>(s, s2, tt, ldy, iY, 0.0);
+        CF_CHECK_LAUNCH();
+    }
+    return CF_OK;
+}
+}  // namespace
+
 // Y = L^-1 for the lower factor of cf_potrf, using the diagonal-block
-// inverses it left in `work`: block row i becomes L_ii^-1 Y_i (DMMA GEMM),
-// then the rows below take Y_below -= L_below,i Y_i.
+// inverses it left in `work`: the 64-blocks are placed on Y's diagonal, then
+// adjacent blocks are merged pairwise, level by level (64, 128, 256, ...):
+// [[Y11, 0], [Y21, Y22]] with Y21 = -Y22 L21 Y11.  Every merge of a level is
+// independent, so a level is two batched DMMA GEMMs that skip the triangular
+// zeros of Y11 and Y22 (log2(n / 64) levels instead of n / 64 dependent
+// block steps).
 extern "C" int cf_trtri_lower(int n, const double* L, long lda, long strideL, double* Y, long ldy, long strideY,
                               int batch, void* work, void* stream)
 {
     if (n <= 0 || batch < 1 || !L || !Y || !work) return CF_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     const long ws = (long)potrf_ws(n);
-    double* Dinv = (double*)work;
-    double* T = Dinv + (long)nblocks(n) * NB * NB;
-    dim3 b2(32, 8);
-    k_set_identity<<<dim3(cf_cdiv(n, 32), cf_cdiv(n, 8), batch), b2, 0, st>>>(Y, ldy, strideY, n);
+    const double* Dinv = (const double*)work;
+    k_fill2d<<<dim3(cf_cdiv(n, 32), cf_cdiv(n, 8), batch), dim3(32, 8), 0, st>>>(n, n, Y, ldy, strideY, 0.0);
     CF_CHECK_LAUNCH();
-    for (int k0 = 0, blk = 0; k0 < n; k0 += NB, ++blk) {
-        const int kb = n - k0 < NB ? n - k0 : NB;
-        const int ncols = k0 + kb;
-        double* Yi = Y + (long)k0 * ldy;
-        int rc = cf_dgemm(0, 0, kb, ncols, kb, 1.0, Dinv + (long)blk * NB * NB, kb, ws, Yi, ldy, strideY, 0.0, T,
-                          ncols, ws, nullptr, 0, 0, batch, 0, stream);
-        if (rc) return rc;
-        k_copy2d<<<dim3(cf_cdiv(ncols, 32), cf_cdiv(kb, 8), batch), b2, 0, st>>>(kb, ncols, T, ncols, ws, Yi, ldy,
-                                                                                strideY);
-        CF_CHECK_LAUNCH();
-        const int rest = n - k0 - kb;
-        if (rest > 0) {
-            rc = cf_dgemm(0, 0, rest, ncols, kb, -1.0, L + (long)(k0 + kb) * lda + k0, lda, strideL, Yi, ldy,
-                          strideY, 1.0, Y + (long)(k0 + kb) * ldy, ldy, strideY, nullptr, 0, 0, batch, 0, stream);
+    k_place_diag_inv<<<dim3(nblocks(n), batch), 256, 0, st>>>(Dinv, ws, n, Y, ldy, strideY);
+    CF_CHECK_LAUNCH();
+    for (long s = NB; s < n; s *= 2) {
+        const int nfull = (int)(n / s), rem = (int)(n % s);
+        if (nfull / 2 > 0) {
+            int rc = merge_pairs((int)s, (int)s, nfull / 2, 0, L, lda, strideL, Y, ldy, strideY, batch, st, stream);
+            if (rc) return rc;
+        }
+        if ((nfull & 1) && rem > 0) {  // the last full block with the partial one after it
+            int rc = merge_pairs((int)s, rem, 1, (long)(nfull - 1) * s, L, lda, strideL, Y, ldy, strideY, batch, st,
+                                 stream);
             if (rc) return rc;
         }
     }

@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(NT) k_dgemm(int M, int N, int K, double alpha,
     double* sBbuf = smem + STAGES * SA;
 
     const int tile_m = blockIdx.y * BM, tile_n = blockIdx.x * BN;
-    if (lower_only && tile_n > tile_m + BM - 1) return;
+    if ((lower_only & 1) && tile_n > tile_m + BM - 1) return;
     const long bz = blockIdx.z;
     A += bz * sA;
     B += bz * sB;
@@ -109,10 +109,15 @@ __global__ void __launch_bounds__(NT) k_dgemm(int M, int N, int K, double alpha,
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
-    const int KT = (K + BK - 1) / BK;
-    // lower_only bit 1: op(A) = Y^T with Y lower triangular (Y^T Y), so the
-    // K sum of a tile starts at its first row
+    int KT = (K + BK - 1) / BK;
+    // lower_only bit 1: op(A) is upper triangular (op(A) = Y^T with Y lower
+    // triangular, as in Y^T Y), so the K sum of a tile starts at its first row;
+    // bit 2: op(A) is lower triangular, so it ends after its last row
     const int kt0 = (lower_only & 2) ? tile_m / BK : 0;
+    if (lower_only & 4) {
+        const int kend = (tile_m + BM + BK - 1) / BK;
+        KT = kend < KT ? kend : KT;
+    }
     auto issue = [&](int kt, int st) {
         if (kt < KT) {
             load_tile<A_KMN>(sAbuf + st * SA, A, lda, tile_m, kt * BK, M, K, tid);

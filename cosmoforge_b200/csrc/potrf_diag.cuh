@@ -1,0 +1,212 @@
+// Diagonal block of the blocked Cholesky: factor a kb x kb SPD block
+// (kb <= 64) in place and form the inverse of its factor, one CTA per batch
+// matrix, for FP64 and FP32.
+//
+// The block is factored right-looking in 16-column panels:
+//   (a) warp 0 factors the panel's 16 x 16 diagonal tile in registers (lane i
+//       holds row i; pivots are broadcast by shuffles, one square root and
+//       one reciprocal per column);
+//   (b) every row below the tile is solved against it by one thread
+//       (x_k = a_k / l_kk, then a_j -= x_k l_jk for the later columns j);
+//   (c) the trailing lower triangle takes the rank-16 update, 3 x 3 entries
+//       per thread.
+// Three barriers per panel instead of one per column.  The inverse X = L^-1 is
+// formed by 16-row block rows: each warp t inverts diagonal tile t by forward
+// substitution (lane c = column c), then block row I takes
+// X_I = T_I^-1 (-sum_{K<I} L_IK X_K) with T_I^-1 the tile inverse.
+//
+// Per-problem status follows LAPACK: info = k0 + j + 1 for the first
+// non-positive (or NaN) pivot j of this block, left unchanged when the
+// problem already holds an earlier failure.  A failed pivot is replaced by 1
+// so the kernel completes with finite work.
+#pragma once
+#include "cf_common.cuh"
+
+namespace cf_diag {
+
+constexpr int NB = 64;
+constexpr int LDS = NB + 1;
+constexpr int PW = 16;
+constexpr int NTHREADS = 256;
+
+template <typename T>
+constexpr size_t smem_bytes() { return (size_t)(2 * NB * LDS + PW * NB) * sizeof(T); }
+
+template <typename T>
+__global__ void __launch_bounds__(NTHREADS) k_potrf_diag_inv(T* A, long lda, long sA, int k0, int kb, T* Dinv,
+                                                             long sD, int* info)
+{
+    extern __shared__ __align__(16) unsigned char diag_smem[];
+    T* S = reinterpret_cast<T*>(diag_smem);  // the block, then L (lower, zeros above)
+    T* X = S + NB * LDS;                     // L^-1
+    T* Tb = X + NB * LDS;                    // PW x NB scratch of the block-row products
+    __shared__ T rdg[NB];                    // reciprocal pivots 1 / l_jj
+    __shared__ int bad;
+    const int b = blockIdx.x;
+    A += (long)b * sA;
+    Dinv += (long)b * sD;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned FULL = 0xffffffffu;
+
+    // load the lower triangle (columns fastest: coalesced), zero the rest
+    {
+        const int c = tid & 63;
+        for (int r = tid >> 6; r < NB; r += NTHREADS / 64) {
+            T v = T(0);
+            if (r < kb && c <= r) v = A[(long)(k0 + r) * lda + k0 + c];
+            S[r * LDS + c] = v;
+            X[r * LDS + c] = T(0);
+        }
+    }
+    if (tid == 0) bad = 0;
+    __syncthreads();
+
+    for (int p = 0; p < kb; p += PW) {
+        const int pw = kb - p < PW ? kb - p : PW;
+        // (a) the pw x pw diagonal tile, warp 0, lane i = row p + i
+        if (warp == 0) {
+            T r[PW];
+#pragma unroll
+            for (int j = 0; j < PW; ++j) r[j] = (lane < pw && j <= lane) ? S[(p + lane) * LDS + p + j] : T(0);
+#pragma unroll
+            for (int k = 0; k < PW; ++k) {
+                if (k < pw) {
+                    T d = __shfl_sync(FULL, r[k], k);
+                    if (!(d > T(0))) {  // also catches NaN
+                        if (lane == 0 && bad == 0) bad = k0 + p + k + 1;
+                        d = T(1);
+                    }
+                    const T lkk = sqrt(d);
+                    const T rl = T(1) / lkk;
+                    if (lane == k) r[k] = lkk;
+                    else if (lane > k) r[k] *= rl;
+                    if (lane == 0) rdg[p + k] = rl;
+#pragma unroll
+                    for (int j = k + 1; j < PW; ++j) {
+                        const T ljk = __shfl_sync(FULL, r[k], j);
+                        if (j < pw && lane >= j) r[j] -= r[k] * ljk;
+                    }
+                }
+            }
+            if (lane < pw) {
+#pragma unroll
+                for (int j = 0; j < PW; ++j)
+                    if (j <= lane) S[(p + lane) * LDS + p + j] = r[j];
+            }
+        }
+        __syncthreads();
+        const int q = p + pw;  // first row / column of the trailing block
+        const int m = kb - q;
+        if (m <= 0) break;
+        // (b) rows below the tile: L[i][p:p+pw] = A[i][p:p+pw] L_tile^-T
+        if (tid < m) {
+            const int i = q + tid;
+            T a[PW];
+#pragma unroll
+            for (int j = 0; j < PW; ++j) a[j] = (j < pw) ? S[i * LDS + p + j] : T(0);
+#pragma unroll
+            for (int k = 0; k < PW; ++k) {
+                if (k < pw) {
+                    a[k] *= rdg[p + k];
+#pragma unroll
+                    for (int j = k + 1; j < PW; ++j)
+                        if (j < pw) a[j] -= a[k] * S[(p + j) * LDS + p + k];
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < PW; ++j)
+                if (j < pw) S[i * LDS + p + j] = a[j];
+        }
+        __syncthreads();
+        // (c) trailing update S[i][j] -= sum_k L[i][p+k] L[j][p+k], q <= j <= i < kb
+        {
+            const int ti = tid >> 4, tj = tid & 15;
+            T acc[3][3];
+#pragma unroll
+            for (int u = 0; u < 3; ++u)
+#pragma unroll
+                for (int v = 0; v < 3; ++v) acc[u][v] = T(0);
+            for (int k = 0; k < pw; ++k) {
+                T li[3], lj[3];
+#pragma unroll
+                for (int u = 0; u < 3; ++u) {
+                    const int i = q + ti + 16 * u, j = q + tj + 16 * u;
+                    li[u] = i < kb ? S[i * LDS + p + k] : T(0);
+                    lj[u] = j < kb ? S[j * LDS + p + k] : T(0);
+                }
+#pragma unroll
+                for (int u = 0; u < 3; ++u)
+#pragma unroll
+                    for (int v = 0; v < 3; ++v) acc[u][v] += li[u] * lj[v];
+            }
+#pragma unroll
+            for (int u = 0; u < 3; ++u)
+#pragma unroll
+                for (int v = 0; v < 3; ++v) {
+                    const int i = q + ti + 16 * u, j = q + tj + 16 * v;
+                    if (i < kb && j <= i) S[i * LDS + j] -= acc[u][v];
+                }
+        }
+        __syncthreads();
+    }
+
+    // write L back (zeros above the diagonal)
+    {
+        const int c = tid & 63;
+        for (int r = tid >> 6; r < kb; r += NTHREADS / 64)
+            if (c < kb) A[(long)(k0 + r) * lda + k0 + c] = (c <= r) ? S[r * LDS + c] : T(0);
+    }
+
+    // X = L^-1.  Step A: warp t inverts diagonal tile t (lane c = column c)
+    {
+        const int t0 = warp * PW;
+        if (t0 < kb) {
+            const int tw = kb - t0 < PW ? kb - t0 : PW;
+            const int c = lane;
+            if (c < tw) {
+                T x[PW];
+#pragma unroll
+                for (int r = 0; r < PW; ++r) {
+                    T acc = (r == c) ? T(1) : T(0);
+#pragma unroll
+                    for (int mm = 0; mm < r; ++mm)
+                        if (mm >= c) acc -= S[(t0 + r) * LDS + t0 + mm] * x[mm];
+                    x[r] = (r >= c && r < tw) ? acc * rdg[t0 + (r < tw ? r : 0)] : T(0);
+                }
+#pragma unroll
+                for (int r = 0; r < PW; ++r)
+                    if (r < tw && r >= c) X[(t0 + r) * LDS + t0 + c] = x[r];
+            }
+        }
+    }
+    __syncthreads();
+    // Step B: block rows I = 1, 2, 3: Tb = -sum_{m < 16 I} L[16I + r][m] X[m][c],
+    // then X[16I + r][c] = sum_{j <= r} X_II[r][j] Tb[j][c] for c < 16 I
+    for (int I0 = PW; I0 < kb; I0 += PW) {
+        const int rows = kb - I0 < PW ? kb - I0 : PW;
+        for (int e = tid; e < PW * I0; e += NTHREADS) {
+            const int r = e / I0, c = e - (e / I0) * I0;
+            T acc = T(0);
+            if (r < rows)
+                for (int mm = c; mm < I0; ++mm) acc -= S[(I0 + r) * LDS + mm] * X[mm * LDS + c];
+            Tb[r * NB + c] = acc;
+        }
+        __syncthreads();
+        for (int e = tid; e < PW * I0; e += NTHREADS) {
+            const int r = e / I0, c = e - (e / I0) * I0;
+            if (r < rows) {
+                T acc = T(0);
+                for (int j = 0; j <= r; ++j) acc += X[(I0 + r) * LDS + I0 + j] * Tb[j * NB + c];
+                X[(I0 + r) * LDS + c] = acc;
+            }
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < kb * kb; e += NTHREADS) {
+        const int r = e / kb, c = e - (e / kb) * kb;
+        Dinv[r * kb + c] = X[r * LDS + c];
+    }
+    if (tid == 0 && bad && info && info[b] == 0) info[b] = bad;
+}
+
+}  // namespace cf_diag

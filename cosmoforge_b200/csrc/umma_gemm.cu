@@ -91,14 +91,18 @@ __device__ __forceinline__ unsigned long long now_ns()
     return t;
 }
 
-// Wait bounded in time; false (and the abort flag raised) when it runs out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag)
+// Wait bounded in time (wait_ns; the clock is read every 256 tries, or on
+// every try for bounds under 1 ms); false (and the abort flag raised) when it
+// runs out.  A bound of 0 gives up at the first unsatisfied try.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                          unsigned long long wait_ns)
 {
     const unsigned long long t0 = now_ns();
+    const bool tight = wait_ns < 1000000ull;
     for (unsigned i = 0;; ++i) {
         if (mbar_try(bar, parity)) return true;
         if (*abort_flag) return false;
-        if ((i & 255) == 255 && now_ns() - t0 > WAIT_NS) break;
+        if ((tight || (i & 255) == 255) && now_ns() - t0 >= wait_ns) break;
     }
     *abort_flag = 1;
     return false;
@@ -187,7 +191,8 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
 template <int BN, int STAGES, bool TRACE, int KC, int PLS, int BKT, bool SPLIT>
 __global__ void __launch_bounds__(NTHREADS, 1)
     k_umma_gemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int K,
-                int n_split, Terms terms, EpiArgs epi, TraceArgs tr, int group_m, int* err)
+                int n_split, Terms terms, EpiArgs epi, TraceArgs tr, int group_m, unsigned long long wait_ns,
+                int* err)
 {
     // Persistent: each CTA walks output tiles blockIdx.x, +gridDim.x, ...; the
     // shared-memory ring, TMEM and all mbarrier phases carry over between
@@ -285,7 +290,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 for (int it = 0; it < iters; ++it, ++g) {
                     const int s = (int)(g % STAGES);
                     const long r = g / STAGES;
-                    if (r > 0 && !mbar_wait(&empty[s], (uint32_t)((r - 1) & 1), abort_flag)) {
+                    if (r > 0 && !mbar_wait(&empty[s], (uint32_t)((r - 1) & 1), abort_flag, wait_ns)) {
                         stop = true;
                         break;
                     }
@@ -345,21 +350,21 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     const bool first = pos == 0;
                     if (first) {
                         if (SPLIT) {  // both accumulators drained by the epilogue
-                            if (gc >= 1 && !mbar_wait(&acce[0], (uint32_t)((gc - 1) & 1), abort_flag)) {
+                            if (gc >= 1 && !mbar_wait(&acce[0], (uint32_t)((gc - 1) & 1), abort_flag, wait_ns)) {
                                 aborted = true;
                                 break;
                             }
                         } else {
                             buf = (int)(gc & 1);
                             const long u = gc >> 1;
-                            if (u >= 1 && !mbar_wait(&acce[buf], (uint32_t)((u - 1) & 1), abort_flag)) {
+                            if (u >= 1 && !mbar_wait(&acce[buf], (uint32_t)((u - 1) & 1), abort_flag, wait_ns)) {
                                 aborted = true;
                                 break;
                             }
                         }
                     }
                     const int s = (int)(g % STAGES);
-                    if (!mbar_wait(&full[s], (uint32_t)((g / STAGES) & 1), abort_flag)) {
+                    if (!mbar_wait(&full[s], (uint32_t)((g / STAGES) & 1), abort_flag, wait_ns)) {
                         aborted = true;
                         break;
                     }
@@ -408,7 +413,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             for (int c = 0; c < nchunks; ++c, ++gc) {
                 const int buf = SPLIT ? 0 : (int)(gc & 1);
                 const uint32_t par = SPLIT ? (uint32_t)(gc & 1) : (uint32_t)((gc >> 1) & 1);
-                if (!mbar_wait(&accf[buf], par, abort_flag)) {
+                if (!mbar_wait(&accf[buf], par, abort_flag, wait_ns)) {
                     ok = false;
                     break;
                 }
@@ -558,6 +563,8 @@ int make_map4(CUtensorMap* map, const void* base, long K2, long K1, long rows, i
 int g_promote_kc = 16;
 // Row tiles per group of the persistent tile order.
 int g_group_m = 16;
+// Bound of the kernels' waits on pipeline barriers (drains of issued work keep WAIT_NS).
+unsigned long long g_wait_ns = WAIT_NS;
 
 template <int BN, int STAGES, bool TRACE, int KC, int PLS = 1, int BKT = BK, bool SPLIT = false>
 int launch_gemm_kc(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, int K, const Terms& t,
@@ -574,7 +581,7 @@ int launch_gemm_kc(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, i
     const long tiles = (long)cf_cdiv(M, BM) * cf_cdiv(N, BN) * splits;
     const int grid = (int)(tiles < sms ? tiles : sms);
     k_umma_gemm<BN, STAGES, TRACE, KC, PLS, BKT, SPLIT><<<grid, NTHREADS, smem, st>>>(ma, mb, K, splits, t, e, tr,
-                                                                                     g_group_m, err);
+                                                                                     g_group_m, g_wait_ns, err);
     CF_CHECK_LAUNCH();
     return CF_OK;
 }
@@ -614,6 +621,29 @@ extern "C" int cf_umma_set_promotion(int kc)
     const int prev = g_promote_kc;
     if (kc == 1 || kc == 2 || kc == 4 || kc == 8 || kc == 16 || kc == 32) g_promote_kc = kc;
     return prev;
+}
+
+// Bound of every wait of the tcgen05 kernels on a pipeline barrier, in ns
+// (ns < 0 restores the default 2 s; 0 gives up at the first unsatisfied
+// try).  A wait that runs out aborts the launch: the CTA drains the copies and
+// MMAs it issued (those drains keep the 2 s bound), frees its TMEM and sets the
+// caller's error flag.  Returns the previous bound.
+extern "C" long long cf_umma_set_wait_limit(long long ns)
+{
+    const long long prev = (long long)g_wait_ns;
+    g_wait_ns = ns < 0 ? WAIT_NS : (unsigned long long)ns;
+    return prev;
+}
+
+// CF_ERR_TIMEOUT when the device error flag of a tcgen05 launch is set (a
+// wait ran out), else CF_OK; synchronises `stream` to read it.
+extern "C" int cf_umma_status(const int* err, void* stream)
+{
+    if (!err) return CF_ERR_ARG;
+    int h = 0;
+    CF_CHECK(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    CF_CHECK(cudaStreamSynchronize((cudaStream_t)stream));
+    return h ? CF_ERR_TIMEOUT : CF_OK;
 }
 
 // Row tiles per group of the persistent tile order (>= 1); returns the previous value.

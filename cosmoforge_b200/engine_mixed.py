@@ -251,8 +251,7 @@ def _fisher_core(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6", N=None, 
     if N is not None or maps is not None:
         qml = _qml_core(plan, E, Cinv, Cp, N, maps, X, pmap, ldseg, segrows, segpad)
     del X
-    if int(plan.err.item()) != 0:
-        raise RuntimeError("tensor-core kernel reported a timed-out wait")
+    check(E.lib.cf_umma_status(plan.err.data_ptr(), stream()), "tensor-core kernel")
     return F, qml
 
 

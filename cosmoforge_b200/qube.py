@@ -453,11 +453,12 @@ class Spectra(_Base):
             f.run()
         return f
 
-    def run(self) -> None:
+    def setup(self) -> None:
+        """Set-up phases of ``run()`` (qube/spectra.py:1220-1280): the Fisher run
+        (or reuse), binning, maps, and F^-1 on the device."""
         f = self._fisher()
         self.layout = f.layout
         L = self.layout
-        E = f.engine
         self.spectra_list = f.spectra_list
         self.beam_smoothing = f.beam_smoothing
         self.bins = f.bins
@@ -473,6 +474,18 @@ class Spectra(_Base):
         nsims = self.params.nsims or X.shape[1]
         if tuple(X.shape) != (L.n, nsims):
             raise ValueError(f"injected maps have shape {tuple(X.shape)}, expected ({L.n}, {nsims})")
+        self._dev_X = X
+        self._dev_invF = f.engine.spd_inverse(f._dev_F.clone())
+        self.invfisher = self._dev_invF.cpu().numpy()
+        self.fisher_normalized = f.fisher
+
+    def compute(self) -> None:
+        """Raw q, noise bias and C_hat = (q - b) F^-1 (qube/spectra.py:1124-1218);
+        runs the set-up first when it has not run."""
+        if getattr(self, "_dev_invF", None) is None:
+            self.setup()
+        f = self.fisher_instance
+        L, E, X = self.layout, f.engine, self._dev_X
         if getattr(f, "_cplan", None) is not None:
             _, _, q = f._cplan.fisher_qml(f._dev_Cinv, with_bias=False, maps=X, want_fisher=False)
             bias = f._dev_bias
@@ -486,15 +499,16 @@ class Spectra(_Base):
             _, bias, q = E.fisher_qml(f._dev_Cinv, f._dev_N, X, want_fisher=False)
         if L.remove_nb:
             q = q - bias[None, :]
-        self._dev_invF = E.spd_inverse(f._dev_F.clone())
         self._dev_q = q
         self._dev_b = bias
         self._dev_clhat = E.gemm(q, self._dev_invF)
         self._dev_nb = E.gemm(bias[None, :], self._dev_invF)[0]
         self.qml_results = q.cpu().numpy()
         self.qml_noise_bias = bias.cpu().numpy()
-        self.invfisher = self._dev_invF.cpu().numpy()
-        self.fisher_normalized = f.fisher
+
+    def run(self) -> None:
+        self.setup()
+        self.compute()
 
     # -- outputs (qube/spectra.py:1340-1733) -------------------------------
     def _inv_sqrt(self):
@@ -545,6 +559,109 @@ class Spectra(_Base):
     def get_error_bars(self, mode: str = "deconvolved", *, as_dict: bool = False):
         err = np.sqrt(np.diag(self.get_covariance(mode)))
         return self._to_dict(err) if as_dict else err
+
+    def get_effective_ells(self, use_midpoint: bool = False):
+        """Window-weighted multipole per bin (delegated to the Fisher run), or the
+        bin midpoints with ``use_midpoint`` (qube/spectra.py:1686-1711)."""
+        if use_midpoint:
+            return self.bins.lmid
+        return self._fisher().get_effective_ells()
+
+    def convolve_theory(self, cl_theory):
+        """<y> = W C_theory with the window W of the raw estimates (qube/spectra.py:2039-2097);
+        ``cl_theory`` is binned, spectrum-major, in the output convention."""
+        W = self.fisher_instance.get_window_matrix() if self.fisher_instance is not None else None
+        if W is None:
+            return None
+        return W @ np.asarray(cl_theory)
+
+    def convolve_theory_for_inference(self, cl_theory):
+        """Expected deconvolved bandpowers W_bp C_l of a per-multipole theory
+        (qube/spectra.py:1735-1878): a dict {label: C_l} or a flat array of
+        n_ell (l = lmin..lmax) or lmax + 1 (from l = 0) values per spectrum,
+        spectrum-major; unbeamed, in the output convention."""
+        f = self.fisher_instance
+        if f is None:
+            raise ValueError("convolve_theory_for_inference requires an attached Fisher instance. "
+                             "Pass fisher=fisher to Spectra() at construction.")
+        if getattr(f, "fisher", None) is None:
+            raise ValueError("Fisher matrix has not been computed. Call fisher.run() "
+                             "(and spectra.run()) before convolve_theory_for_inference().")
+        lmin, lmax = int(self.params.lmin), int(self.params.lmax)
+        n_ell = lmax - lmin + 1
+        labels = list(f.layout.labels()) if getattr(f, "layout", None) is not None else None
+        nspectra = len(labels) if labels is not None else 1
+
+        def per_ell(arr, what):
+            arr = np.asarray(arr, dtype=np.float64)
+            if arr.ndim != 1:
+                raise ValueError(f"{what} must be 1D, got shape {arr.shape}")
+            if arr.size == n_ell:
+                return arr
+            if arr.size >= lmax + 1:
+                return arr[lmin: lmax + 1]
+            raise ValueError(f"{what} length {arr.size} does not match expected {n_ell} "
+                             f"(l=lmin..lmax) or {lmax + 1} (l=0..lmax)")
+
+        if isinstance(cl_theory, dict):
+            missing = [lab for lab in labels if lab not in cl_theory]
+            if missing:
+                raise KeyError(f"cl_theory dict missing entries for: {missing}. Expected keys: {labels}")
+            vec = np.concatenate([per_ell(cl_theory[lab], lab) for lab in labels])
+        else:
+            cl = np.asarray(cl_theory, dtype=np.float64)
+            if cl.ndim != 1:
+                raise ValueError(f"cl_theory must be 1D, got shape {cl.shape}")
+            if nspectra > 1:
+                if cl.size != nspectra * n_ell:
+                    raise ValueError(f"cl_theory length {cl.size} does not match expected {nspectra * n_ell} "
+                                     f"(nspectra*n_ell, spectrum-major) for a {nspectra}-spectrum run; "
+                                     "or pass a label-keyed dict.")
+                vec = cl
+            else:
+                vec = per_ell(cl, "cl_theory")
+        W = f.get_bandpower_window_function()
+        return None if W is None else W @ vec
+
+    def write_power_spectra(self, mode: str = "deconvolved", filename: str | None = None,
+                            include_errors: bool = True) -> None:
+        """Mean spectra over simulations as a (bins x spectra) %.16e table, errors
+        beside it; ``convolved`` writes the mean raw y and the window matrix
+        (qube/spectra.py:2099-2240)."""
+        valid = ("deconvolved", "decorrelated", "convolved")
+        if mode not in valid:
+            raise ValueError(f"mode must be one of {valid}, got '{mode}'")
+        if filename is None:
+            out = getattr(self.params, "outclfile", None)
+            if out:
+                parts = str(out).rsplit(".", 1)
+                filename = f"{parts[0]}_{mode}.{parts[1] if len(parts) > 1 else 'dat'}"
+            else:
+                filename = f"spectra_{mode}.dat"
+        parts = filename.rsplit(".", 1)
+
+        def beside(tag):
+            return f"{parts[0]}_{tag}.{parts[1]}" if len(parts) > 1 else f"{filename}_{tag}"
+
+        if mode == "convolved":
+            res = self.get_power_spectra(mode="convolved")
+            if res is None:
+                return
+            y, W, _ = res
+            np.savetxt(filename, np.mean(y, axis=0), header="Raw QML estimates (y vector, mean across simulations)")
+            np.savetxt(beside("window"), W, header="Window matrix W: <y> = W @ C_true")
+            return
+        spectra = self.get_power_spectra(mode=mode)
+        if spectra is None:
+            return
+        nb = self.layout.nbins
+
+        def table(vec):
+            return np.asarray(vec).reshape(-1, nb).T  # spectrum-major vector -> (bins, spectra)
+
+        np.savetxt(filename, table(np.mean(spectra, axis=0)), fmt="%.16e")
+        if include_errors:
+            np.savetxt(beside("errors"), table(self.get_error_bars(mode=mode)), fmt="%.16e")
 
     def _to_dict(self, flat):
         sl = self.layout.bandpower_slices()

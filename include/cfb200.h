@@ -86,8 +86,10 @@ int cf_build_block(int kind, int mode, int na, const double* va, int nb, const d
  * FP64 GEMM on the DMMA tensor pipe: C = alpha op(A) op(B) + beta C, with an
  * optional transposed copy CT = C^T (NULL to skip) and a batch dimension.
  * transa / transb: 0 = A is M x K / B is K x N; 1 = A given as K x M / B as N x K.
- * lower_only: bit 0 skips output tiles strictly above the diagonal; bit 1 (with
- * transa) starts each tile's K sum at its first row (op(A) = Y^T, Y lower).
+ * lower_only: bit 0 skips output tiles strictly above the diagonal; bit 1
+ * starts each tile's K sum at its first row (op(A) upper triangular, e.g.
+ * op(A) = Y^T with Y lower); bit 2 ends it after its last row (op(A) lower
+ * triangular).  Bits 1 and 2 assume M == K (a square triangular op(A)).
  * Replaces: cosmocore/basics/linalg.py:18-32 (matrix_mult, np.matmul).
  */
 int cf_dgemm(int transa, int transb, int M, int N, int K, double alpha, const double* A, long lda,
@@ -279,6 +281,18 @@ int cf_umma_trace_bf16_mapped(int P1, int P2, int K1, int K2, int nterms, const 
                               long sYq, long ldY, long y_ps, int y_planes, double scale, double* F,
                               long ldF, const int* row_map, const int* col_map, int sym, int splits,
                               int* err, void* stream);
+
+/* Bound of every wait of the tcgen05 kernels on a pipeline barrier, in ns
+ * (default 2 s; ns < 0 restores it; 0 gives up at the first unsatisfied
+ * try).  A wait that runs out aborts the launch cleanly: issued copies and
+ * MMAs are drained (with the 2 s bound), TMEM is freed and the launch's error
+ * flag is set.  For failure-path tests and watchdogs.  Returns the previous
+ * bound.  No counterpart in the reference. */
+long long cf_umma_set_wait_limit(long long ns);
+
+/* CF_ERR_TIMEOUT if the device error flag `err` of a tcgen05 launch is set,
+ * else CF_OK.  Synchronises `stream`.  No counterpart in the reference. */
+int cf_umma_status(const int* err, void* stream);
 
 /* Promotion interval of the tensor-core kernels: k-tiles of 64 summed in one
  * FP32 TMEM accumulator before promotion (1, 2, 4, 8 or 16; default 16).

@@ -479,6 +479,49 @@ def case_picslike_tqu():
     _save("picslike_tqu_nside8", **out)
 
 
+
+def case_picslike_tqu_harmonic():
+    """The reference's PICSLike run end to end (``run()``) with ``basis="harmonic"``.
+
+    Same inputs and points as ``picslike_tqu_nside8``; the grid is given the
+    reference's way: ``params.parameters = {"idx": [0, 7, 8]}`` with one theory
+    file per point (``root_dir/root_filename_idx<i>.txt``, C_l columns) and a
+    fiducial file, as ``picslike/picslike.py:409-431`` reads them.  The harmonic
+    branch evaluates chi2 and ln|C| by Sherman-Morrison-Woodbury
+    (``picslike/picslike.py:597-622``).
+    """
+    import tempfile
+
+    from picslike import PICSLike
+
+    base = dict(np.load(HERE / "picslike_tqu_nside8.npz"))
+    pb = workloads.config3()
+    lmax_sig = int(pb.params["lmax_signal"])
+    thetas = base["thetas"]
+
+    def write(path, cls):
+        ell = np.arange(2, lmax_sig + 1, dtype=np.float64)
+        labels = sorted(cls)
+        np.savetxt(path, np.column_stack([ell] + [np.asarray(cls[k])[2:lmax_sig + 1] for k in labels]),
+                   fmt="%.18e", header="ell " + " ".join(labels))
+
+    with tempfile.TemporaryDirectory() as tmp:
+        for i, t in enumerate(thetas):
+            write(f"{tmp}/tqu_idx{float(i):.6g}.txt", workloads.model_cls(t, lmax_sig))
+        write(f"{tmp}/fid.txt", pb.cls)
+        params = dict(pb.params, input_convention="Cl", root_dir=tmp, root_filename="tqu",
+                      fiducialfile=f"{tmp}/fid.txt",
+                      parameters={"idx": [0.0, float(len(thetas) - 1), len(thetas)]})
+        pl = PICSLike(params, basis="harmonic", mask=pb.mask, noise_cov1=pb.noise, cls_data=pb.cls,
+                      fiducial_cls=pb.cls, beam=pb.beam, maps1=base["maps"])
+        t0 = time.perf_counter()
+        pl.run()
+        dt = time.perf_counter() - t0
+    out = {k: base[k] for k in base if not k.startswith("ref_")}
+    out.update(ref_chi2=np.asarray(pl.get_chi_squared()), ref_lnl=np.asarray(pl.get_log_likelihood()),
+               ref_basis=np.array("harmonic"), ref_time_s=dt)
+    _save("picslike_tqu_harmonic_nside8", **out)
+
 CASES = {
     "fortran_qube": case_fortran_qube_nside8,
     "nside4_T": lambda: case_nside4("T"),
@@ -489,6 +532,7 @@ CASES = {
     "tqu_cut": case_tqu_cut,
     "fortran_picslike": case_fortran_picslike_nside8,
     "picslike_tqu": case_picslike_tqu,
+    "picslike_tqu_harmonic": case_picslike_tqu_harmonic,
     "bandpower_tt": case_bandpower_tt,
     "bandpower_tqu": case_bandpower_tqu,
     "harmonic_tqu_cut": lambda: _harmonic_case("tqu_cut_nside4", "harmonic_tqu_cut_nside4"),
