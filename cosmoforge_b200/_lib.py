@@ -67,6 +67,9 @@ SIGNATURES = {
                                _p, _l, _l, _p, _l, _p, _p]),
     "cf_potrf_f32_workspace": (_sz, [_i, _i]),
     "cf_potrf_f32": (_i, [_i, _p, _l, _l, _i, _p, _p, _p]),
+    "cf_sgemm_bf16x6": (_i, [_i, _i, _i, _f, _p, _l, _l, _p, _l, _l, _f, _p, _l, _l, _i, _i, _p, _p]),
+    "cf_sgemm_bf16x6_set_wait_limit": (C.c_longlong, [C.c_longlong]),
+    "cf_potrf_f32_set_tensor": (_i, [_i]),
     "cf_axpby_f32": (_i, [_l, _d, _p, _l, _d, _p, _p, _l, _p, _l, _p, _l, _i, _p]),
     "cf_chi2_logdet_mixed": (_i, [_i, _p, _l, _l, _p, _l, _l, _i, _p, _l, _l, _i, _p, _p, _p]),
     "cf_mlp_dense_fwd": (_i, [_i, _i, _i, _p, _l, _p, _p, _i, _p, _p, _l, _p]),

@@ -17,11 +17,20 @@
 #include "cf_common.cuh"
 #include "potrf_diag.cuh"
 
+extern "C" int cf_sgemm_bf16x6(int M, int N, int K, float alpha, const float* A, long lda, long sA, const float* B,
+                               long ldb, long sB, float beta, float* C, long ldc, long sC, int batch, int lower_only,
+                               int* info, void* stream);
+
 namespace {
 
 constexpr int NB = cf_diag::NB;
 
 using cf_diag::k_potrf_diag_inv;
+
+// Product kernel of the FP32 factor's panel solves and trailing updates:
+// 1 = BF16x6 split products on the tensor cores (cf_sgemm_bf16x6, default),
+// 0 = the FP32 SIMT kernel below.
+int g_potrf_f32_tensor = 1;
 
 // FP32 SIMT GEMM, both operands K-contiguous (the "NT" form):
 //   C[M x N] = alpha A[M x K] B[N x K]^T + beta C, batch on blockIdx.z.
@@ -125,14 +134,22 @@ __global__ void __launch_bounds__(SNT, 2) k_sgemm_nt(int M, int N, int K, float 
     }
 }
 
-int sgemm_nt(int M, int N, int K, float alpha, const float* A, long lda, long sA, const float* B, long ldb, long sB,
-             float beta, float* C, long ldc, long sC, int batch, int lower_only, cudaStream_t st)
+int sgemm_nt_simt(int M, int N, int K, float alpha, const float* A, long lda, long sA, const float* B, long ldb,
+                  long sB, float beta, float* C, long ldc, long sC, int batch, int lower_only, cudaStream_t st)
 {
     if (M <= 0 || N <= 0) return CF_OK;
     dim3 grid(cf_cdiv(N, SBM), cf_cdiv(M, SBM), batch);
     k_sgemm_nt<<<grid, SNT, 0, st>>>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, lower_only);
     CF_CHECK_LAUNCH();
     return CF_OK;
+}
+
+int sgemm_nt(int M, int N, int K, float alpha, const float* A, long lda, long sA, const float* B, long ldb, long sB,
+             float beta, float* C, long ldc, long sC, int batch, int lower_only, int* info, cudaStream_t st)
+{
+    if (g_potrf_f32_tensor)
+        return cf_sgemm_bf16x6(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower_only, info, st);
+    return sgemm_nt_simt(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower_only, st);
 }
 
 __global__ void k_copy2d_f32(int R, int Ccols, const float* src, long lds, long ss, float* dst, long ldd, long sd)
@@ -284,12 +301,24 @@ inline size_t potrf_f32_ws(int n) { return (size_t)2 * NB * NB + (size_t)n * 2 *
 
 }  // namespace
 
+// Product kernel of cf_potrf_f32: 1 = BF16x6 tensor cores (default), 0 = FP32
+// SIMT.  Returns the previous setting.
+extern "C" int cf_potrf_f32_set_tensor(int on)
+{
+    const int prev = g_potrf_f32_tensor;
+    g_potrf_f32_tensor = on ? 1 : 0;
+    return prev;
+}
+
 extern "C" size_t cf_potrf_f32_workspace(int n, int batch) { return potrf_f32_ws(n) * sizeof(float) * (size_t)batch; }
 
 // Blocked FP32 Cholesky in place (lower factor), batched: per 64-wide panel the
-// diagonal block is factored and inverted by one CTA and L21 = A21 L11^-T is an
-// FP32 GEMM; panels go in pairs so the trailing update A22 -= L21 L21^T runs
-// once per 128 columns.  info: int[batch] zeroed by the caller.
+// diagonal block is factored and inverted by one CTA and L21 = A21 L11^-T is a
+// GEMM; panels go in pairs so the trailing update A22 -= L21 L21^T runs once
+// per 128 columns.  The GEMMs are BF16x6 split products on the tensor cores
+// (cf_sgemm_bf16x6) unless cf_potrf_f32_set_tensor(0) selects the SIMT kernel.
+// info: int[batch] zeroed by the caller; k > 0 is the first bad pivot, -3 a
+// tensor-core wait that ran out.
 extern "C" int cf_potrf_f32(int n, float* A, long lda, long strideA, int batch, void* work, int* info, void* stream)
 {
     if (n <= 0 || batch < 1 || !A || !work || lda < n) return CF_ERR_ARG;
@@ -308,10 +337,10 @@ extern "C" int cf_potrf_f32(int n, float* A, long lda, long strideA, int batch, 
         const int rest1 = n - k0 - kb1;
         if (rest1 <= 0) break;
         float* a21_1 = A + (long)(k0 + kb1) * lda + k0;
-        int rc = sgemm_nt(rest1, kb1, kb1, 1.0f, a21_1, lda, strideA, D1, kb1, ws, 0.0f, W, LDW, ws, batch, 0, st);
+        int rc = sgemm_nt(rest1, kb1, kb1, 1.0f, a21_1, lda, strideA, D1, kb1, ws, 0.0f, W, LDW, ws, batch, 0, info, st);
         if (rc) return rc;
         const int kb2 = rest1 < NB ? rest1 : NB;
-        rc = sgemm_nt(rest1, kb2, kb1, -1.0f, W, LDW, ws, W, LDW, ws, 1.0f, a21_1 + kb1, lda, strideA, batch, 0, st);
+        rc = sgemm_nt(rest1, kb2, kb1, -1.0f, W, LDW, ws, W, LDW, ws, 1.0f, a21_1 + kb1, lda, strideA, batch, 0, info, st);
         if (rc) return rc;
         k_copy2d_f32<<<dim3(cf_cdiv(kb1, 32), cf_cdiv(rest1, 8), batch), dim3(32, 8), 0, st>>>(rest1, kb1, W, LDW, ws,
                                                                                               a21_1, lda, strideA);
@@ -323,10 +352,10 @@ extern "C" int cf_potrf_f32(int n, float* A, long lda, long strideA, int batch, 
         if (rest2 <= 0) break;
         float* a21_2 = A + (long)(k1 + kb2) * lda + k1;
         float* W2 = W + (long)kb2 * LDW;
-        rc = sgemm_nt(rest2, kb2, kb2, 1.0f, a21_2, lda, strideA, D2, kb2, ws, 0.0f, W2 + kb1, LDW, ws, batch, 0, st);
+        rc = sgemm_nt(rest2, kb2, kb2, 1.0f, a21_2, lda, strideA, D2, kb2, ws, 0.0f, W2 + kb1, LDW, ws, batch, 0, info, st);
         if (rc) return rc;
         rc = sgemm_nt(rest2, rest2, kb1 + kb2, -1.0f, W2, LDW, ws, W2, LDW, ws, 1.0f, a21_2 + kb2, lda, strideA, batch,
-                      1, st);
+                      1, info, st);
         if (rc) return rc;
         k_copy2d_f32<<<dim3(cf_cdiv(kb2, 32), cf_cdiv(rest2, 8), batch), dim3(32, 8), 0, st>>>(
             rest2, kb2, W2 + kb1, LDW, ws, a21_2, lda, strideA);

@@ -1,0 +1,316 @@
+// FP32 GEMM C = alpha A B^T + beta C on the tcgen05 tensor cores with BF16
+// split products (sm_100a), for the likelihood's FP32 Cholesky.
+//
+// Each operand is split in registers into three BF16 planes,
+// a = a0 + a1 + a2 (a0 = bf16(a), a1 = bf16(a - a0), a2 = bf16(a - a0 - a1)),
+// and C += sum over the six plane pairs (0,0), (0,1), (1,0), (0,2), (1,1),
+// (2,0) (kind::f16 MMAs, FP32 accumulation in TMEM): about 24 significant
+// bits per product, the FP32 factor's own rounding level, at tensor-core
+// rate instead of the SIMT pipe's.  The leading product (0,0) and the five
+// corrections go to two TMEM accumulators, added in the epilogue, so the
+// small terms are not summed into the large one inside the tensor core.
+// Both operands are K-contiguous ("NT"), as the blocked Cholesky's panel
+// solves and trailing updates use them; batch on blockIdx.z.
+//
+// One 128 x BN output tile per CTA (128 threads).  K runs in chunks of 64
+// (one 128-byte BF16 row per operand row and plane): every thread loads its
+// share of the chunk from global memory, splits it and stores the planes in
+// the 128-byte swizzled K-major layout the MMA descriptors describe; thread 0
+// issues the 24 MMAs of the chunk and commits them to the stage's mbarrier.
+// Two stages: the loads and splits of chunk c + 1 overlap the MMAs of chunk
+// c.  The epilogue reads both accumulators with tcgen05.ld (thread = output
+// row) and writes alpha (acc0 + acc1) + beta C.  Every barrier wait is
+// bounded; a wait that runs out makes the CTA drain its MMAs, free its TMEM
+// and set info[z] = -3.
+#include <cuda_bf16.h>
+
+#include "cf_common.cuh"
+
+namespace {
+
+constexpr int BM = 128, KC = 64, NT = 128, PLANES = 3;
+constexpr uint32_t A_BYTES = BM * KC * 2;  // one BF16 plane of the A chunk (16 KB)
+constexpr unsigned long long DRAIN_NS = 2000000000ull;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(200000u)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ unsigned long long now_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Wait bounded in time; false when the bound ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned long long wait_ns)
+{
+    const unsigned long long t0 = now_ns();
+    const bool tight = wait_ns < 1000000ull;
+    for (unsigned i = 0;; ++i) {
+        if (mbar_try(bar, parity)) return true;
+        if ((tight || (i & 255) == 255) && now_ns() - t0 >= wait_ns) return false;
+    }
+}
+
+// K-major operand rows of 128 bytes, 128-byte swizzle: 8-row atoms 1024 B apart.
+__device__ __forceinline__ uint64_t smem_desc(const void* tile)
+{
+    const uint64_t addr = smem_u32(tile);
+    uint64_t d = 0;
+    d |= (addr >> 4) & 0x3FFFull;         // start address
+    d |= (uint64_t)(16 >> 4) << 16;       // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;     // stride byte offset: 8 rows of 128 B
+    d |= (uint64_t)1 << 46;               // descriptor version (sm100)
+    d |= (uint64_t)2 << 61;               // SWIZZLE_128B
+    return d;
+}
+
+template <int BN>
+__device__ __forceinline__ uint32_t instr_desc_bf16()
+{
+    // D = F32, A = B = BF16, both K-major, M = 128, N = BN.
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate)
+{
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+        ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+          "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+          "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+          "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+// Byte offset of element (r, k), k < 64, in a 128-byte-swizzled K-major BF16 tile.
+__device__ __forceinline__ uint32_t swz(int r, int k)
+{
+    return (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + ((((k >> 3) ^ (r & 7)) << 4) | ((k & 7) << 1)));
+}
+
+// rows x 64 chunk of a K-contiguous FP32 operand (row r0.., column k0..) into
+// three BF16 planes `plane` bytes apart, in two passes of 32 columns.
+template <int ROWS>
+__device__ __forceinline__ void stage_operand(const float* X, long ld, int r0, int nrows, int k0, int K, uint8_t* dst,
+                                              uint32_t plane, int tid)
+{
+    constexpr int PER = ROWS * 32 / NT;
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+        float v[PER];
+#pragma unroll
+        for (int i = 0; i < PER; ++i) {
+            const int e = i * NT + tid, r = e >> 5, k = half * 32 + (e & 31);
+            const int gr = r0 + r, gk = k0 + k;
+            v[i] = (gr < nrows && gk < K) ? X[(long)gr * ld + gk] : 0.0f;
+        }
+#pragma unroll
+        for (int i = 0; i < PER; ++i) {
+            const int e = i * NT + tid, r = e >> 5, k = half * 32 + (e & 31);
+            const __nv_bfloat16 p0 = __float2bfloat16_rn(v[i]);
+            const float r1 = v[i] - __bfloat162float(p0);
+            const __nv_bfloat16 p1 = __float2bfloat16_rn(r1);
+            const __nv_bfloat16 p2 = __float2bfloat16_rn(r1 - __bfloat162float(p1));
+            const uint32_t o = swz(r, k);
+            *reinterpret_cast<__nv_bfloat16*>(dst + o) = p0;
+            *reinterpret_cast<__nv_bfloat16*>(dst + plane + o) = p1;
+            *reinterpret_cast<__nv_bfloat16*>(dst + 2 * plane + o) = p2;
+        }
+    }
+}
+
+template <int BN>
+__global__ void __launch_bounds__(NT, 1) k_sgemm_bf16x6(int M, int N, int K, float alpha, const float* A, long lda,
+                                                        long sA, const float* B, long ldb, long sB, float beta, float* C,
+                                                        long ldc, long sC, int lower_only, unsigned long long wait_ns,
+                                                        int* info)
+{
+    constexpr uint32_t B_BYTES = BN * KC * 2;
+    constexpr uint32_t STAGE = PLANES * (A_BYTES + B_BYTES);
+    constexpr uint32_t TMEM_COLS = 2 * BN;  // leading product | corrections
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    __shared__ uint64_t done[2];
+    __shared__ uint64_t drain;
+    __shared__ uint32_t tmem_slot;
+
+    const int tile_m = blockIdx.y * BM, tile_n = blockIdx.x * BN;
+    if ((lower_only & 1) && tile_n > tile_m + BM - 1) return;  // whole CTA, before any allocation
+    const long z = blockIdx.z;
+    A += z * sA;
+    B += z * sB;
+    C += z * sC;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        mbar_init(&done[0], 1);
+        mbar_init(&done[1], 1);
+        mbar_init(&drain, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+    const uint32_t idesc = instr_desc_bf16<BN>();
+
+    const int nch = (K + KC - 1) / KC;
+    bool aborted = false;
+    for (int c = 0; c < nch; ++c) {
+        const int s = c & 1;
+        uint8_t* sa = smem + s * STAGE;  // A planes 0, 1, 2, then B planes 0, 1, 2
+        uint8_t* sb = sa + PLANES * A_BYTES;
+        // the MMAs of chunk c - 2 read this stage: wait for them before overwriting it
+        bool ok = c < 2 || mbar_wait(&done[s], (uint32_t)(((c - 2) >> 1) & 1), wait_ns);
+        if (__syncthreads_or(!ok)) {
+            aborted = true;
+            break;
+        }
+        stage_operand<BM>(A, lda, tile_m, M, c * KC, K, sa, A_BYTES, tid);
+        stage_operand<BN>(B, ldb, tile_n, N, c * KC, K, sb, B_BYTES, tid);
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            constexpr int TA[6] = {0, 0, 1, 0, 1, 2}, TB[6] = {0, 1, 0, 2, 1, 0};
+#pragma unroll
+            for (int t = 0; t < 6; ++t) {
+                const uint64_t da = smem_desc(sa + TA[t] * A_BYTES), db = smem_desc(sb + TB[t] * B_BYTES);
+                const uint32_t dst = tmem + (t > 0 ? (uint32_t)BN : 0u);
+                const bool fresh = c == 0 && t <= 1;  // first write of each accumulator
+#pragma unroll
+                for (int k = 0; k < KC / 16; ++k) {  // 16 BF16 = 32 B per MMA: advance the start address
+                    const uint64_t o = (uint64_t)((k * 32) >> 4);
+                    umma_bf16(dst, da + o, db + o, idesc, (fresh && k == 0) ? 0u : 1u);
+                }
+            }
+            umma_commit(&done[s]);
+        }
+    }
+    bool ok = !aborted;
+    if (ok && nch > 0) {
+        const int cl = nch - 1;
+        ok = mbar_wait(&done[cl & 1], (uint32_t)((cl >> 1) & 1), wait_ns);
+    }
+    if (__syncthreads_or(!ok)) {
+        // drain: every MMA issued has completed before TMEM is freed
+        if (tid == 0) {
+            umma_commit(&drain);
+            const unsigned long long t0 = now_ns();
+            while (!mbar_try(&drain, 0) && now_ns() - t0 < DRAIN_NS) {
+            }
+        }
+        if (tid == 0 && info) atomicCAS(info + z, 0, CF_ERR_TIMEOUT);
+    } else if (nch > 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        const int row = tile_m + warp * 32 + lane;
+        const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll
+        for (int g = 0; g < BN / 32; ++g) {
+            uint32_t v[32], w[32];
+            tmem_ld32(lane_addr + (uint32_t)(g * 32), v);
+            tmem_ld32(lane_addr + (uint32_t)(BN + g * 32), w);
+            if (row < M) {
+                float* pc = C + (long)row * ldc + tile_n + g * 32;
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    if (tile_n + g * 32 + j < N) {
+                        float out = alpha * (__uint_as_float(v[j]) + __uint_as_float(w[j]));
+                        if (beta != 0.0f) out += beta * pc[j];
+                        pc[j] = out;
+                    }
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TMEM_COLS));
+    }
+}
+
+unsigned long long g_sgemm_wait_ns = DRAIN_NS;
+
+template <int BN>
+int launch(int M, int N, int K, float alpha, const float* A, long lda, long sA, const float* B, long ldb, long sB,
+           float beta, float* C, long ldc, long sC, int batch, int lower_only, int* info, cudaStream_t st)
+{
+    constexpr size_t smem = 1024 + 2 * (size_t)PLANES * (A_BYTES + (size_t)BN * KC * 2);
+    static_assert(smem <= 232448, "shared memory exceeds 227 KB");
+    static std::atomic<int> attr[CF_MAX_DEVICES];
+    if (int rc = cf_smem_optin(k_sgemm_bf16x6<BN>, (int)smem, attr)) return rc;
+    dim3 grid(cf_cdiv(N, BN), cf_cdiv(M, BM), batch);
+    k_sgemm_bf16x6<BN><<<grid, NT, smem, st>>>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, lower_only,
+                                               g_sgemm_wait_ns, info);
+    CF_CHECK_LAUNCH();
+    return CF_OK;
+}
+
+}  // namespace
+
+// C_z = alpha A_z B_z^T + beta C_z (FP32, row-major, K contiguous in A and B;
+// z < batch with element strides sA, sB, sC) with six BF16 split products on
+// the tensor cores.  lower_only bit 0 skips output tiles strictly above the diagonal.
+// info (optional, int[batch]): set to -3 for a problem whose tile saw a wait
+// run out (left alone when non-zero).
+extern "C" int cf_sgemm_bf16x6(int M, int N, int K, float alpha, const float* A, long lda, long sA, const float* B,
+                               long ldb, long sB, float beta, float* C, long ldc, long sC, int batch, int lower_only,
+                               int* info, void* stream)
+{
+    if (M < 0 || N < 0 || K < 0 || batch < 1 || !C || (K > 0 && (!A || !B))) return CF_ERR_ARG;
+    if (M == 0 || N == 0) return CF_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (N <= 64)
+        return launch<64>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower_only, info, st);
+    return launch<128>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower_only, info, st);
+}
+
+// Bound of the barrier waits of cf_sgemm_bf16x6, in ns (ns < 0: the default
+// 2 s; 0: give up at the first unsatisfied try).  Returns the previous bound.
+extern "C" long long cf_sgemm_bf16x6_set_wait_limit(long long ns)
+{
+    const long long prev = (long long)g_sgemm_wait_ns;
+    g_sgemm_wait_ns = ns < 0 ? DRAIN_NS : (unsigned long long)ns;
+    return prev;
+}

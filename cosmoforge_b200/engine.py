@@ -332,29 +332,51 @@ class Engine:
               "cf_potrf")
         return info
 
-    def lnl(self, cl_tables, N: torch.Tensor, maps: torch.Tensor, noise_scale=None, precision: str = "fp64"):
+    def signal_basis(self, N: torch.Tensor) -> "SignalBasis":
+        """The per-multipole basis of C(theta) for this layout and noise (cached on N)."""
+        key = (N.data_ptr(), tuple(N.shape))
+        if getattr(self, "_basis_key", None) != key:
+            self._basis = None
+            self._basis = SignalBasis(self, N)
+            self._basis_key = key
+        return self._basis
+
+    def lnl(self, cl_tables, N: torch.Tensor, maps: torch.Tensor, noise_scale=None, precision: str = "fp64",
+            build: str = "auto"):
         """chi2 (B x nsims), ln|C| (B,), lnL (B x nsims), info (B,) for a batch of points.
 
         precision "fp64": FP64 Cholesky, chi2 = |L^-1 x|^2, ln|C| from its
         diagonal.  "mixed": FP32 Cholesky of C, chi2 from one FP64 refinement
         step against the FP64 C (second-order error), ln|C| from the FP32
         factor's diagonal summed in FP64.
+
+        build "basis" forms C(theta) = S(theta) + s N from the per-multipole
+        basis (one GEMM per block region, see SignalBasis), "direct" runs the
+        pair kernel per point, "auto" takes the basis for batches of 64 or more
+        points when it fits in 4 GB.
         """
+        if precision not in ("fp64", "mixed"):
+            raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
         cl = torch.as_tensor(cl_tables, dtype=F64, device=self.dev)
         if cl.dim() == 2:
             cl = cl[None]
         B = cl.shape[0]
         n = self.L.n
-        C = self.signal(cl)
         sc = None
         if noise_scale is not None:
             sc = torch.as_tensor(noise_scale, dtype=F64, device=self.dev).reshape(B).contiguous()
-        if precision == "mixed":
-            return self._lnl_mixed(C, N, maps, sc)
-        if precision != "fp64":
-            raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
-        check(self.lib.cf_axpby(n * n, 1.0, C.data_ptr(), n * n, 1.0, ptr(sc), N.data_ptr(), 0,
-                                C.data_ptr(), n * n, B, stream()), "cf_axpby")
+        if build == "auto":
+            build = "basis" if B >= 64 and SignalBasis.bytes_needed(self.L) <= 4 << 30 else "direct"
+        if build == "basis":
+            C = self.signal_basis(N).covariance(cl, sc)
+            if precision == "mixed":
+                return self._lnl_mixed(C, N, maps, sc, noise_added=True)
+        else:
+            C = self.signal(cl)
+            if precision == "mixed":
+                return self._lnl_mixed(C, N, maps, sc)
+            check(self.lib.cf_axpby(n * n, 1.0, C.data_ptr(), n * n, 1.0, ptr(sc), N.data_ptr(), 0,
+                                    C.data_ptr(), n * n, B, stream()), "cf_axpby")
         info = self.potrf(C)
         X = maps.to(self.dev, F64).contiguous()
         nsims = X.shape[1]
@@ -366,11 +388,15 @@ class Engine:
               "cf_chi2_logdet")
         return chi2, logdet, -0.5 * (chi2 + logdet[:, None]), info
 
-    def _lnl_mixed(self, C: torch.Tensor, N: torch.Tensor, maps: torch.Tensor, sc):
+    def _lnl_mixed(self, C: torch.Tensor, N: torch.Tensor, maps: torch.Tensor, sc, noise_added: bool = False):
         B, n = C.shape[0], self.L.n
         C32 = torch.empty((B, n, n), dtype=torch.float32, device=self.dev)
-        check(self.lib.cf_axpby_f32(n * n, 1.0, C.data_ptr(), n * n, 1.0, ptr(sc), N.data_ptr(), 0,
-                                    C.data_ptr(), n * n, C32.data_ptr(), n * n, B, stream()), "cf_axpby_f32")
+        if noise_added:  # C already holds S + s N: only its FP32 copy is made
+            check(self.lib.cf_axpby_f32(n * n, 1.0, C.data_ptr(), n * n, 0.0, None, N.data_ptr(), 0,
+                                        None, n * n, C32.data_ptr(), n * n, B, stream()), "cf_axpby_f32")
+        else:
+            check(self.lib.cf_axpby_f32(n * n, 1.0, C.data_ptr(), n * n, 1.0, ptr(sc), N.data_ptr(), 0,
+                                        C.data_ptr(), n * n, C32.data_ptr(), n * n, B, stream()), "cf_axpby_f32")
         info = torch.zeros(B, dtype=torch.int32, device=self.dev)
         work = torch.empty(self.lib.cf_potrf_f32_workspace(n, B) // 4 + 1, dtype=torch.float32, device=self.dev)
         check(self.lib.cf_potrf_f32(n, C32.data_ptr(), n, n * n, B, work.data_ptr(), info.data_ptr(), stream()),
@@ -383,6 +409,91 @@ class Engine:
                                             X.data_ptr(), nsims, 0, nsims, chi2.data_ptr(), logdet.data_ptr(),
                                             stream()), "cf_chi2_logdet_mixed")
         return chi2, logdet, -0.5 * (chi2 + logdet[:, None]), info
+
+
+class SignalBasis:
+    """C(theta) = S(theta) + s(theta) N for many points as one FP64 GEMM per block region.
+
+    The pair kernels (Legendre / spin-2 recurrences, rotation angles) do not
+    depend on the spectra: S = sum_{k, l} C~_{k,l} K_{k,l}, with K_{k,l} the
+    signal matrix of a unit table at (spectrum k, multipole l)
+    (``cosmocore/signal_kernels.py:164-502`` evaluated once per basis entry by
+    the pair kernel).  Each block region of C (a field pair and its mirror) is
+    then (points x kdim) . (kdim x region entries): the rows of the basis are
+    the region of N (weighted by the point's noise scale) followed by the
+    K_{k,l} of the region's spectra, spectrum-major.  Trailing spectra whose
+    tables are zero for every point of a batch (TB, EB in a model without
+    them) are left out of the product.  Rounding differs from the direct build
+    only in the order of the l sum.
+    """
+
+    def __init__(self, E: "Engine", N: torch.Tensor):
+        L = E.L
+        n, Lp = L.n, L.lmax_signal + 1
+        self.E, self.n, self.Lp = E, n, Lp
+        self.regions = []
+        covered = 0
+        for blk in L.blocks:
+            fa, fb = L.fields[blk.fa], L.fields[blk.fb]
+            by_mode = {L.spectra[k].mode: k for k in blk.spectra}
+            if blk.kind in (lay.KIND_00_AUTO, lay.KIND_00_CROSS):
+                sp = [blk.spectra[0]]
+            elif blk.kind == lay.KIND_22_AUTO:
+                sp = [by_mode[m] for m in (0, 1, 2) if m in by_mode]
+            else:
+                sp = [by_mode[m] for m in (0, 1) if m in by_mode]
+            spans = [(fb.offset, fa.offset, fb.nrows, fa.nrows)]
+            if blk.fa != blk.fb:
+                spans.append((fa.offset, fb.offset, fa.nrows, fb.nrows))
+            Ks = [torch.empty((1 + len(sp) * Lp, R, Cc), dtype=F64, device=E.dev) for (_, _, R, Cc) in spans]
+            for (r0, c0, R, Cc), K in zip(spans, Ks):
+                K[0] = N[r0:r0 + R, c0:c0 + Cc]
+            for j, k in enumerate(sp):
+                tab = torch.zeros((Lp, L.nspectra, Lp), dtype=F64, device=E.dev)
+                tab[torch.arange(Lp), k, torch.arange(Lp)] = 1.0
+                Sk = E.signal(tab)
+                for (r0, c0, R, Cc), K in zip(spans, Ks):
+                    K[1 + j * Lp: 1 + (j + 1) * Lp] = Sk[:, r0:r0 + R, c0:c0 + Cc]
+                del Sk
+            for (r0, c0, R, Cc), K in zip(spans, Ks):
+                self.regions.append((r0, c0, R, Cc, sp, K))
+                covered += R * Cc
+        if covered != n * n:
+            raise ValueError("the blocks of this layout do not cover the covariance matrix")
+
+    @staticmethod
+    def bytes_needed(L) -> int:
+        Lp = L.lmax_signal + 1
+        tot = 0
+        for blk in L.blocks:
+            fa, fb = L.fields[blk.fa], L.fields[blk.fb]
+            k = 1 + len(blk.spectra) * Lp
+            tot += k * fa.nrows * fb.nrows * (1 if blk.fa == blk.fb else 2)
+        return 8 * tot
+
+    def covariance(self, cl: torch.Tensor, scale: torch.Tensor | None = None, out=None) -> torch.Tensor:
+        """C (B x n x n, FP64) for beam-smoothed tables cl (B, nspectra, L+1)."""
+        E, n, Lp = self.E, self.n, self.Lp
+        B = cl.shape[0]
+        if out is None:
+            out = torch.empty((B, n, n), dtype=F64, device=E.dev)
+        s = torch.ones(B, dtype=F64, device=E.dev) if scale is None else scale.reshape(B).to(F64)
+        # leaving out the trailing all-zero spectra drops exact zeros from every
+        # sum (same bits); while a CUDA graph is being captured the host cannot
+        # read the tables, so every spectrum stays in
+        used = None
+        if not torch.cuda.is_current_stream_capturing():
+            used = (cl.abs().amax(dim=(0, 2)) > 0).cpu().numpy()
+        for r0, c0, R, Cc, sp, K in self.regions:
+            keep = len(sp)
+            while used is not None and keep > 0 and not used[sp[keep - 1]]:
+                keep -= 1
+            kd = 1 + keep * Lp
+            ctab = torch.cat([s[:, None], cl[:, sp[:keep], :].reshape(B, keep * Lp)], dim=1).contiguous()
+            check(self.E.lib.cf_dgemm(0, 0, B, Cc, kd, 1.0, ctab.data_ptr(), kd, 0, K.data_ptr(), R * Cc, Cc,
+                                      0.0, _off(out, r0 * n + c0), n * n, n, None, 0, 0, R, 0, stream()),
+                  "cf_dgemm")
+        return out
 
 
 def qml_solve(E: Engine, cls: dict, N: torch.Tensor, maps: torch.Tensor):

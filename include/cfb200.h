@@ -317,6 +317,32 @@ int cf_umma_set_group(int group_m);
 /* Bytes of workspace cf_potrf_f32 needs for `batch` problems of order n. */
 size_t cf_potrf_f32_workspace(int n, int batch);
 
+/*
+ * FP32 GEMM with BF16 split products on the tcgen05 tensor cores:
+ *   C_z = alpha A_z B_z^T + beta C_z,  A_z M x K, B_z N x K (K contiguous),
+ * each operand split into three BF16 planes and the six plane products with
+ * i + j <= 2 accumulated in FP32 (~24 significant bits).  Batch z < batch,
+ * element strides sA, sB, sC.  lower_only bit 0 skips output tiles strictly
+ * above the diagonal.  info (optional, int[batch]): -3 for a problem whose
+ * tile saw a barrier wait run out (then its C is not written).
+ * Replaces: the FP32 products of the Cholesky used by the mixed likelihood
+ * (picslike/picslike.py:643-664, cosmocore/basics/linalg.py:362-474 in FP64
+ * in the reference).
+ */
+int cf_sgemm_bf16x6(int M, int N, int K, float alpha, const float* A, long lda, long sA, const float* B, long ldb,
+                    long sB, float beta, float* C, long ldc, long sC, int batch, int lower_only, int* info,
+                    void* stream);
+
+/* Bound of the barrier waits of cf_sgemm_bf16x6 in ns (ns < 0: default 2 s;
+ * 0: give up at the first unsatisfied try).  Returns the previous bound.
+ * No counterpart in the reference. */
+long long cf_sgemm_bf16x6_set_wait_limit(long long ns);
+
+/* Product kernel of cf_potrf_f32: 1 = cf_sgemm_bf16x6 on the tensor cores
+ * (default), 0 = an FP32 SIMT kernel.  Returns the previous setting.
+ * No counterpart in the reference. */
+int cf_potrf_f32_set_tensor(int on);
+
 /* Blocked lower Cholesky in FP32, in place (batch), 64-wide panels with FP32
  * GEMM updates; info as for cf_potrf.  The factor of the mixed likelihood:
  * replaces cosmocore/basics/linalg.py:362-406 (cholesky_factor) at FP32. */

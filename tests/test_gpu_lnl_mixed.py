@@ -145,3 +145,92 @@ def test_potrf_batch_copies_bitwise_identical(dtype):
     assert int(info.abs().max()) == 0
     Lf = torch.tril(C)
     assert bool((Lf == Lf[:1]).all())
+
+
+@pytest.mark.parametrize("M,N,K,batch,lower", [(300, 300, 128, 3, 0), (1184, 1184, 128, 2, 1), (517, 64, 64, 4, 0),
+                                               (130, 200, 96, 1, 0), (64, 64, 200, 1, 0)])
+def test_sgemm_bf16x6_matches_fp64_product(M, N, K, batch, lower):
+    """cf_sgemm_bf16x6 (BF16x6 split products on tcgen05) against the product
+    of the same FP32 operands in FP64: ~24-bit products, so the error must sit
+    at the FP32 level (2e-6 of the largest |A||B| sum); alpha / beta, ragged
+    tiles, batches and skipped upper tiles included."""
+    from cosmoforge_b200 import _lib
+
+    lib = _lib.lib()
+    g = torch.Generator(device="cuda").manual_seed(M + N + K)
+    A = torch.randn((batch, M, K), device="cuda", generator=g)
+    B = A if lower else torch.randn((batch, N, K), device="cuda", generator=g)
+    C0 = torch.randn((batch, M, N), device="cuda", generator=g)
+    C = C0.clone()
+    info = torch.zeros(batch, dtype=torch.int32, device="cuda")
+    rc = lib.cf_sgemm_bf16x6(M, N, K, -1.0, A.data_ptr(), K, M * K, B.data_ptr(), K, N * K, 0.5, C.data_ptr(), N, M * N,
+                             batch, lower, info.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    assert rc == 0
+    torch.cuda.synchronize()
+    assert int(info.abs().max()) == 0
+    ref = -torch.bmm(A.double(), B.double().transpose(1, 2)) + 0.5 * C0.double()
+    scale = torch.bmm(A.double().abs(), B.double().abs().transpose(1, 2)).max()
+    if lower:  # tiles strictly above the diagonal are skipped: only rows >= the tile's columns are written
+        r = torch.arange(M, device="cuda")[:, None] // 128
+        c = torch.arange(N, device="cuda")[None, :] // 128
+        keep = (c <= r)[None]
+        err = ((C.double() - ref).abs() * keep).max()
+        assert bool((C[~keep.expand_as(C)] == C0[~keep.expand_as(C0)]).all())
+    else:
+        err = (C.double() - ref).abs().max()
+    assert float(err / scale) <= 2e-6, float(err / scale)
+
+
+def test_sgemm_bf16x6_timed_out_wait_sets_info():
+    from cosmoforge_b200 import _lib
+
+    lib = _lib.lib()
+    A = torch.randn((2, 256, 256), device="cuda")
+    C = torch.zeros((2, 256, 256), device="cuda")
+    info = torch.zeros(2, dtype=torch.int32, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    lib.cf_sgemm_bf16x6_set_wait_limit(0)
+    try:
+        assert lib.cf_sgemm_bf16x6(256, 256, 256, 1.0, A.data_ptr(), 256, 65536, A.data_ptr(), 256, 65536, 0.0,
+                                   C.data_ptr(), 256, 65536, 2, 0, info.data_ptr(), st) == 0
+        torch.cuda.synchronize()
+    finally:
+        lib.cf_sgemm_bf16x6_set_wait_limit(-1)
+    assert set(info.cpu().tolist()) == {_lib.CF_ERR_TIMEOUT}
+    info.zero_()
+    assert lib.cf_sgemm_bf16x6(256, 256, 256, 1.0, A.data_ptr(), 256, 65536, A.data_ptr(), 256, 65536, 0.0,
+                               C.data_ptr(), 256, 65536, 2, 0, info.data_ptr(), st) == 0
+    torch.cuda.synchronize()
+    assert int(info.abs().max()) == 0
+    ref = torch.bmm(A.double(), A.double().transpose(1, 2))
+    assert float((C.double() - ref).abs().max() / ref.abs().max()) <= 2e-6
+
+
+@pytest.mark.parametrize("n,batch", [(1312, 8), (200, 64)])
+def test_potrf_f32_tensor_cores_vs_simt(n, batch):
+    """The FP32 factor with tensor-core products stays as close to the FP64
+    factor as the SIMT FP32 factor does (both at FP32 rounding level)."""
+    from cosmoforge_b200 import _lib
+
+    lib = _lib.lib()
+    g = torch.Generator(device="cuda").manual_seed(n)
+    R = torch.randn((batch, n, n), dtype=torch.float64, device="cuda", generator=g)
+    A64 = R @ R.transpose(1, 2) / n + torch.eye(n, dtype=torch.float64, device="cuda")
+    L64 = torch.linalg.cholesky(A64)
+    st = torch.cuda.current_stream().cuda_stream
+    errs = {}
+    prev = lib.cf_potrf_f32_set_tensor(1)
+    try:
+        for mode in (1, 0):
+            lib.cf_potrf_f32_set_tensor(mode)
+            A = A64.float().contiguous()
+            work = torch.empty(lib.cf_potrf_f32_workspace(n, batch) // 4 + 1, dtype=torch.float32, device="cuda")
+            info = torch.zeros(batch, dtype=torch.int32, device="cuda")
+            assert lib.cf_potrf_f32(n, A.data_ptr(), n, n * n, batch, work.data_ptr(), info.data_ptr(), st) == 0
+            torch.cuda.synchronize()
+            assert int(info.abs().max()) == 0
+            Lf = torch.tril(A.double())
+            errs[mode] = float((Lf - L64).abs().max() / L64.abs().max())
+    finally:
+        lib.cf_potrf_f32_set_tensor(prev)
+    assert errs[1] <= max(4 * errs[0], 2e-6), errs
