@@ -585,7 +585,9 @@ def main():
         forms, rep = autotune.tune_fisher(E, C0, args.scheme, use_cache=False)
         torch.cuda.synchronize()
         tune_report = {"seconds": time.perf_counter() - t0,
-                       "forms": {L.spectra[k].label: {"all_planes": v[0], "kc": v[1]} for k, v in forms.items()}}
+                       "forms": {L.spectra[k].label: {"all_planes": v[0], "kc": v[1],
+                                                      "group_m": v[2] if len(v) > 2 else 16}
+                                 for k, v in forms.items()}}
         del S0, C0
     for _ in range(args.warmup):
         step()

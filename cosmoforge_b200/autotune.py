@@ -1,4 +1,5 @@
-"""Autotuner for the mixed-precision Fisher's A_b = C^-1 dC_b products.
+"""Autotuner: the mixed-precision Fisher's A_b = C^-1 dC_b products, the
+patch batches' size buckets and the batched likelihood's launch shape.
 
 For each spectrum it times the candidate forms of the split-product GEMM
 (``cf_umma_gemm_bf16``: all planes of a k-slice per stage with split
@@ -15,6 +16,11 @@ for the Fisher matrix, and keeps the fastest one within tolerance:
 * speed: CUDA-event time of the spectrum's GEMMs (second of two runs);
 * choice: the fastest candidate whose error is below ``tol`` or within
   ``slack`` of the most accurate candidate's (the split-product floor).
+
+``tune_patches`` picks the number of size buckets of ``batch.PatchBatch``
+(the fastest graph replay); ``tune_lnl`` the points per captured likelihood
+graph and the FP32 factor's product kernel (tensor-core BF16x6 or SIMT, the
+latter kept only if it is faster within the lnL tolerance).
 
 Results are cached per (scheme, problem shape, device) in-process and in a
 JSON file (``CFB200_TUNE_CACHE``, default ``~/.cache/cosmoforge_b200/
@@ -33,6 +39,7 @@ from ._lib import check, stream
 from .engine_mixed import MixedPlan, _build_planes, default_gemm_forms
 
 CANDIDATES = ((1, 16), (1, 8), (0, 16), (0, 32))
+GROUPS = (8, 16, 32)
 _MEM = {}
 
 
@@ -87,7 +94,7 @@ def _trace_AA(cols, L):
 
 def tune_fisher(E, Cinv: torch.Tensor, scheme: str = "bf16x6", tol: float = 6e-6, slack: float = 1.25,
                 candidates=CANDIDATES, probe_bins=None, use_cache: bool = True):
-    """Per-spectrum {s: (all_planes, kc)} for engine_mixed.fisher_qml, and a report."""
+    """Per-spectrum {s: (all_planes, kc, group_m)} for engine_mixed.fisher_qml, and a report."""
     key = _key(E, scheme, tol)
     if use_cache:
         got = _load(key)
@@ -107,6 +114,7 @@ def tune_fisher(E, Cinv: torch.Tensor, scheme: str = "bf16x6", tol: float = 6e-6
     lib = E.lib
     prev_ap = lib.cf_umma_set_all_planes(1)
     prev_kc = lib.cf_umma_set_promotion(16)
+    prev_gm = lib.cf_umma_set_group(16)
     forms, report = {}, {}
     try:
         for s in range(L.nspectra):
@@ -131,9 +139,10 @@ def tune_fisher(E, Cinv: torch.Tensor, scheme: str = "bf16x6", tol: float = 6e-6
             results = []
             outs = {seg: (torch.empty((Pl, npd, B.shape[1]), dtype=torch.bfloat16, device=E.dev), B.shape[1] // nb)
                     for seg, (B, K, kseg) in ops.items()}
-            for ap, kc in candidates:
+            def time_form(ap, kc, group):
                 lib.cf_umma_set_all_planes(ap)
                 lib.cf_umma_set_promotion(kc)
+                lib.cf_umma_set_group(group)
                 ms = 0.0
                 for rep in range(2):
                     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -149,6 +158,10 @@ def tune_fisher(E, Cinv: torch.Tensor, scheme: str = "bf16x6", tol: float = 6e-6
                     ev1.record()
                     torch.cuda.synchronize()
                     ms = ev0.elapsed_time(ev1)
+                return ms
+
+            for ap, kc in candidates:
+                ms = time_form(ap, kc, 16)
                 err = 0.0
                 for b, ref in refs.items():
                     cols = {}
@@ -159,18 +172,26 @@ def tune_fisher(E, Cinv: torch.Tensor, scheme: str = "bf16x6", tol: float = 6e-6
                                                for fi, fl in enumerate(L.fields)])
                     err = max(err, abs(_trace_AA(cols, L) / ref - 1.0))
                 results.append((ms, err, ap, kc))
-            del outs
-            check(lib.cf_umma_status(plan.err.data_ptr(), stream()), "tensor-core kernel while tuning")
             floor = min(r[1] for r in results)
             ok = [r for r in results if r[1] <= max(tol, slack * floor)]
             best = min(ok)
-            forms[s] = (best[2], best[3])
-            report[L.spectra[s].label] = [{"all_planes": ap, "kc": kc, "ms": round(ms, 3), "err": err}
-                                          for ms, err, ap, kc in results]
+            # the row-tile group only orders the tiles (same arithmetic per tile): timed, not re-checked
+            groups = {16: best[0]}
+            for gm in GROUPS:
+                if gm not in groups:
+                    groups[gm] = time_form(best[2], best[3], gm)
+            del outs
+            check(lib.cf_umma_status(plan.err.data_ptr(), stream()), "tensor-core kernel while tuning")
+            gbest = min(groups, key=groups.get)
+            forms[s] = (best[2], best[3], gbest)
+            report[L.spectra[s].label] = {
+                "forms": [{"all_planes": ap, "kc": kc, "ms": round(ms, 3), "err": err} for ms, err, ap, kc in results],
+                "group_ms": {str(k): round(v, 3) for k, v in groups.items()}}
             del ops
     finally:
         lib.cf_umma_set_all_planes(prev_ap)
         lib.cf_umma_set_promotion(prev_kc)
+        lib.cf_umma_set_group(prev_gm)
     _store(key, forms, report)
     return forms, report
 
@@ -184,3 +205,132 @@ def forms_for(E, Cinv, scheme: str = "bf16x6", tune: bool = False, tol: float = 
     if tune:
         return tune_fisher(E, Cinv, scheme, tol)[0]
     return default_gemm_forms(E.L)
+
+
+# ---------------------------------------------------------------------------
+# Patch batches: the number of size buckets
+# ---------------------------------------------------------------------------
+def _patch_key(sizes, dev) -> str:
+    return f"patches|{','.join(str(n) for n in sorted(int(x) for x in sizes))}|{torch.cuda.get_device_name(dev)}"
+
+
+def _load_value(key):
+    if key in _MEM:
+        return _MEM[key]
+    try:
+        d = json.loads(_cache_path().read_text())
+        if key in d:
+            _MEM[key] = d[key]["value"]
+            return _MEM[key]
+    except (OSError, ValueError, KeyError):
+        pass
+    return None
+
+
+def _store_value(key, value, report):
+    _MEM[key] = value
+    path = _cache_path()
+    try:
+        path.parent.mkdir(parents=True, exist_ok=True)
+        d = json.loads(path.read_text()) if path.exists() else {}
+        d[key] = {"value": value, "report": report}
+        path.write_text(json.dumps(d, indent=1))
+    except (OSError, ValueError):
+        pass
+
+
+def patch_buckets_for(sizes, dev, default: int = 2) -> int:
+    """The tuned bucket count for this set of patch sizes, else `default`."""
+    got = _load_value(_patch_key(sizes, dev))
+    return int(got) if got is not None else default
+
+
+def _graph_ms(fn, reps: int) -> float:
+    fn()
+    fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def tune_patches(problems, device=None, candidates=(1, 2, 3, 4, 6), reps: int = 5, use_cache: bool = True):
+    """Bucket count of batch.PatchBatch for these problems: the fastest graph
+    replay among the candidates (every candidate gives the same results, the
+    padding only adds exact zeros).  Cached per set of sizes and device."""
+    from .batch import PatchBatch
+
+    dev = torch.device(device or "cuda")
+    sizes = [int((p["mask"] > 0.5).sum()) for p in problems]
+    key = _patch_key(sizes, dev)
+    if use_cache:
+        got = _load_value(key)
+        if got is not None:
+            return int(got), None
+    times = {}
+    for k in candidates:
+        pb = PatchBatch(problems, dev, buckets=k)
+        times[k] = _graph_ms(pb.run, reps)
+        del pb
+    best = min(times, key=times.get)
+    report = {"ms_per_batch": {str(k): v for k, v in times.items()}}
+    _store_value(key, best, report)
+    return best, report
+
+
+# ---------------------------------------------------------------------------
+# Batched likelihood: points per graph replay, FP32 product kernel
+# ---------------------------------------------------------------------------
+def tune_lnl(E, N, X, precision: str = "mixed", batches=(128, 256, 512, 1024), tol: float = 0.05,
+             probe_points: int = 256, use_cache: bool = True):
+    """{"batch": B, "tensor": 0/1} for engine.LnlGraph / PICSLike on this layout.
+
+    Every candidate runs the probe points (scrambled Sobol points of the
+    five-parameter model box) through a captured LnlGraph; the mixed form's
+    FP32 product kernel (tensor-core BF16x6 or SIMT) must keep |dlnL| <= tol
+    against the FP64 evaluation of the same points.  The fastest per point
+    wins; cached per layout shape, precision and device."""
+    from . import engine as eng
+    from . import workloads
+    from .sampler import ModelTables
+
+    L = E.L
+    fields = ",".join(f"{f.spin}:{f.nrows}" for f in L.fields)
+    key = f"lnl|{precision}|n{L.n}|{fields}|L{L.lmax_signal}|{torch.cuda.get_device_name(E.dev)}"
+    if use_cache:
+        got = _load_value(key)
+        if got is not None:
+            return dict(got), None
+    th = torch.as_tensor(workloads.sobol_points(probe_points, seed=11), device=E.dev)
+    tabs = ModelTables(L, E.dev)(th)
+    sc = th[:, 4].contiguous()
+    _, _, ref, _ = E.lnl(tabs, N, X, noise_scale=sc, precision="fp64")
+    lib = E.lib
+    kernels = (1, 0) if precision == "mixed" else (1,)
+    prev = lib.cf_potrf_f32_set_tensor(1)
+    results = []
+    free = torch.cuda.mem_get_info(E.dev)[0]
+    try:
+        for tensor in kernels:
+            lib.cf_potrf_f32_set_tensor(tensor)
+            for B in batches:
+                if 4 * B * L.n * L.n * 8 > 0.6 * free:  # C, its FP32 copy and the workspaces
+                    continue
+                G = eng.LnlGraph(E, N, X, B, precision=precision)
+                got = [G(tabs[b0:b0 + B], sc[b0:b0 + B]) for b0 in range(0, probe_points, B)]
+                lnl = torch.cat([r[2] for r in got])
+                err = float((lnl - ref).abs().max())
+                ms = _graph_ms(lambda: G(tabs[:B], sc[:B]), 3)
+                results.append({"batch": B, "tensor": tensor, "us_per_point": 1e3 * ms / B, "max_abs_dlnL": err})
+                del G
+    finally:
+        lib.cf_potrf_f32_set_tensor(prev)
+    ok = [r for r in results if r["max_abs_dlnL"] <= tol] or results
+    best = min(ok, key=lambda r: r["us_per_point"])
+    choice = {"batch": best["batch"], "tensor": best["tensor"]}
+    _store_value(key, choice, {"candidates": results})
+    return choice, {"candidates": results}

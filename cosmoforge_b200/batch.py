@@ -8,11 +8,12 @@
   split-product tensor-core kernel on derivative planes emitted by the pair
   builder.
 * :class:`PatchBatch` - many independent spin-0 QML problems of uneven size
-  (sky patches) solved together: every problem is padded to a common order
-  with an identity noise block (zero signal, zero derivatives, zero map
-  entries, so F, q and the bias are unchanged), then the factorisations, the
-  A_b products, the Fisher contractions and the quadratic forms run as
-  batched device kernels, and the whole pipeline replays from one CUDA graph.
+  (sky patches) solved together: the problems are grouped by size into
+  buckets, every problem of a bucket is padded to the bucket's order with an
+  identity noise block (zero signal, zero derivatives, zero map entries, so F,
+  q and the bias are unchanged), then the factorisations, the A_b products,
+  the Fisher contractions and the quadratic forms run as batched device
+  kernels, and the whole pipeline replays from one CUDA graph.
 """
 
 from __future__ import annotations
@@ -90,14 +91,8 @@ def map_solves(E: eng.Engine, Cinv: torch.Tensor, X: torch.Tensor, precision: st
     return q
 
 
-class PatchBatch:
-    """Independent spin-0 QML problems of uneven size, solved as one padded batch.
-
-    problems: list of dicts with ``params``, ``mask`` (npix x 1), ``beam``,
-    ``cls`` ({"TT": C_l}), ``noise`` (n x n reduced noise covariance) and
-    ``maps`` (n x nsims, nsims <= 4).  All problems must share lmin / lmax /
-    lmax_signal (the same bins).
-    """
+class _PatchGroup:
+    """Spin-0 QML problems padded to the largest of them and solved as one batch."""
 
     def __init__(self, problems, device=None):
         self.dev = torch.device(device or "cuda")
@@ -205,6 +200,94 @@ class PatchBatch:
         self._dgemm(0, 0, ms, nb, nb, self.qmb.data_ptr(), nb, ms * nb, self.Finv.data_ptr(), nb, nb * nb,
                     self.clhat.data_ptr(), nb, ms * nb, P)
 
+    def results(self):
+        """Per-problem dict of numpy arrays: fisher, q (raw), bias, clhat, info flags."""
+        F, q, b, ch = (t.cpu().numpy() for t in (self.F, self.q, self.bias, self.clhat))
+        ic, jf = self.info_c.cpu().numpy(), self.info_f.cpu().numpy()
+        out = []
+        for k in range(self.P):
+            out.append(dict(fisher=F[k], q=q[k], bias=b[k], clhat=ch[k], n=self.ns[k], info_cov=int(ic[k]),
+                            info_fisher=int(jf[k])))
+        return out
+
+
+def bucket_bounds(ns, buckets: int) -> list:
+    """Split problems sorted by size into at most `buckets` contiguous groups
+    minimising the padded work sum_g |g| max_g(n)^3 (exact, by dynamic
+    programming over the sorted sizes); returns the groups' end indices."""
+    ns = sorted(int(n) for n in ns)
+    P = len(ns)
+    k = max(1, min(int(buckets), P))
+    INF = float("inf")
+    best = [[INF] * (P + 1) for _ in range(k + 1)]
+    cut = [[0] * (P + 1) for _ in range(k + 1)]
+    best[0][0] = 0.0
+    for g in range(1, k + 1):
+        for j in range(1, P + 1):
+            for i in range(g - 1, j):
+                c = best[g - 1][i] + (j - i) * float(ns[j - 1]) ** 3
+                if c < best[g][j]:
+                    best[g][j], cut[g][j] = c, i
+    g = min(range(1, k + 1), key=lambda q: best[q][P])
+    ends, j = [], P
+    while g > 0:
+        ends.append(j)
+        j = cut[g][j]
+        g -= 1
+    return sorted(ends)
+
+
+class PatchBatch:
+    """Independent spin-0 QML problems of uneven size (sky patches) solved together.
+
+    problems: list of dicts with ``params``, ``mask`` (npix x 1), ``beam``,
+    ``cls`` ({"TT": C_l}), ``noise`` (n x n reduced noise covariance) and
+    ``maps`` (n x nsims, nsims <= 4).  All problems must share lmin / lmax /
+    lmax_signal (the same bins).  The problems are sorted by size and split
+    into ``buckets`` groups (boundaries minimising the padded n^3 work), each
+    padded to its own largest problem; every group's pipeline runs as batched
+    kernels and all of them replay from one CUDA graph.  ``buckets=None``
+    takes the count the autotuner picked for this set of sizes (cached), or 1.
+    """
+
+    def __init__(self, problems, device=None, buckets: int | None = None):
+        self.dev = torch.device(device or "cuda")
+        sizes = [int((np.asarray(p["mask"]) > 0.5).sum()) for p in problems]
+        if buckets is None:
+            from .autotune import patch_buckets_for
+
+            buckets = patch_buckets_for(sizes, self.dev)
+        order = sorted(range(len(problems)), key=lambda k: sizes[k])
+        ends = bucket_bounds(sizes, buckets)
+        self.groups, self.members = [], []
+        start = 0
+        for e in ends:
+            idx = order[start:e]
+            self.groups.append(_PatchGroup([problems[k] for k in idx], self.dev))
+            self.members.append(idx)
+            start = e
+        self.buckets = len(self.groups)
+        self.P = len(problems)
+        self.nb = self.groups[0].nb
+        if any(g.nb != self.nb for g in self.groups):
+            raise ValueError("all problems must share the same bins")
+        self.ns = [0] * self.P
+        for g, idx in zip(self.groups, self.members):
+            for k, n in zip(idx, g.ns):
+                self.ns[k] = n
+        self._graph = None
+
+    @property
+    def info_f(self) -> torch.Tensor:
+        out = torch.zeros(self.P, dtype=torch.int32, device=self.dev)
+        for g, idx in zip(self.groups, self.members):
+            out[torch.as_tensor(idx, device=self.dev)] = g.info_f
+        return out
+
+    def _pipeline(self):
+        for g in self.groups:
+            g._pipeline()
+
     def run(self, graph: bool = True):
         """Solve every problem (replays one captured pipeline after the first call)."""
         if self._graph is not None:
@@ -219,11 +302,9 @@ class PatchBatch:
         return self
 
     def results(self):
-        """Per-problem dict of numpy arrays: fisher, q (raw), bias, clhat, info flags."""
-        F, q, b, ch = (t.cpu().numpy() for t in (self.F, self.q, self.bias, self.clhat))
-        ic, jf = self.info_c.cpu().numpy(), self.info_f.cpu().numpy()
-        out = []
-        for k in range(self.P):
-            out.append(dict(fisher=F[k], q=q[k], bias=b[k], clhat=ch[k], n=self.ns[k], info_cov=int(ic[k]),
-                            info_fisher=int(jf[k])))
+        """Per-problem dict of numpy arrays (input order): fisher, q (raw), bias, clhat, info flags."""
+        out = [None] * self.P
+        for g, idx in zip(self.groups, self.members):
+            for k, r in zip(idx, g.results()):
+                out[k] = r
         return out

@@ -496,6 +496,57 @@ class SignalBasis:
         return out
 
 
+class LnlGraph:
+    """The likelihood of a batch of B points as one CUDA graph replay.
+
+    Static device buffers hold the points' beam-smoothed tables and noise
+    scales; the graph records Engine.lnl on them once (C(theta) from the
+    per-multipole basis or the pair kernel, the Cholesky factor, chi2 and
+    ln|C|), and every later batch is a copy of its tables into the buffers
+    and one replay (picslike/picslike.py:479-546 run as one launch per batch).
+    A batch smaller than B fills the tail of the buffers with copies of its
+    first point and drops their results.
+    """
+
+    def __init__(self, E: Engine, N: torch.Tensor, X: torch.Tensor, B: int, precision: str = "fp64",
+                 build: str = "auto"):
+        L = E.L
+        self.E, self.B = E, int(B)
+        self.cl = torch.zeros((self.B, L.nspectra, L.lmax_signal + 1), dtype=F64, device=E.dev)
+        self.sc = torch.ones(self.B, dtype=F64, device=E.dev)
+        self.N = N
+        self.X = X.to(E.dev, F64).contiguous()
+        self.precision = precision
+        self.build = "basis" if (build == "auto" and self.B >= 64
+                                 and SignalBasis.bytes_needed(L) <= 4 << 30) else ("direct" if build == "auto"
+                                                                                     else build)
+        # eager warm-up (kernel attributes, the basis, library module loads), then the capture
+        E.lnl(self.cl, N, self.X, noise_scale=self.sc, precision=precision, build=self.build)
+        torch.cuda.synchronize(E.dev)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self.out = E.lnl(self.cl, N, self.X, noise_scale=self.sc, precision=precision, build=self.build)
+
+    def __call__(self, cl, noise_scale=None):
+        """chi2 (b, nsims), ln|C| (b,), lnL (b, nsims), info (b,) for b <= B points."""
+        cl = torch.as_tensor(cl, dtype=F64, device=self.E.dev)
+        b = cl.shape[0]
+        if b > self.B:
+            raise ValueError(f"batch of {b} points exceeds the graph's {self.B}")
+        self.cl[:b].copy_(cl)
+        if b < self.B:
+            self.cl[b:].copy_(cl[:1].expand(self.B - b, -1, -1))
+        if noise_scale is None:
+            self.sc.fill_(1.0)
+        else:
+            sc = torch.as_tensor(noise_scale, dtype=F64, device=self.E.dev).reshape(b)
+            self.sc[:b].copy_(sc)
+            self.sc[b:].copy_(sc[:1].expand(self.B - b))
+        self.graph.replay()
+        chi2, logdet, lnl, info = self.out
+        return chi2[:b].clone(), logdet[:b].clone(), lnl[:b].clone(), info[:b].clone()
+
+
 def qml_solve(E: Engine, cls: dict, N: torch.Tensor, maps: torch.Tensor):
     """S, C^-1, F, q, bias, F^-1, C_hat on the device (plain FP64)."""
     L = E.L

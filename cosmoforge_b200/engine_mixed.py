@@ -205,10 +205,13 @@ def _fisher_core(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6", N=None, 
         forms = forms_for(E, Cinv, scheme)
     prev_ap = E.lib.cf_umma_set_all_planes(1)
     prev_kc = E.lib.cf_umma_set_promotion(16)
+    prev_gm = E.lib.cf_umma_set_group(16)
     for s in range(L.nspectra):
-        ap, kc = forms.get(s, (1, 16))
+        form = tuple(forms.get(s, (1, 16)))
+        ap, kc = form[0], form[1]
         E.lib.cf_umma_set_all_planes(ap)
         E.lib.cf_umma_set_promotion(kc)
+        E.lib.cf_umma_set_group(form[2] if len(form) > 2 else 16)
         ev = E._probe_begin("build_planes")
         blk, ops = _build_planes(plan, s)
         E._probe_end("build_planes", ev, 0)
@@ -229,6 +232,7 @@ def _fisher_core(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6", N=None, 
         del ops
     E.lib.cf_umma_set_all_planes(prev_ap)
     E.lib.cf_umma_set_promotion(prev_kc)
+    E.lib.cf_umma_set_group(prev_gm)
     F = torch.zeros((P, P), dtype=torch.float64, device=E.dev)
     segs = list(X)
     for a, ss in enumerate(segs):

@@ -11,8 +11,11 @@ ln|C| and lnL = -(chi2 + ln|C|)/2 (the 2 pi constant omitted, as in the
 reference).  Results are one ``LikelihoodResult`` per simulation plus their
 mean, with the reference's accessors (``RuntimeError`` before ``compute()``).
 
-The points run in batches on the GPU: one batched build of S(theta) for all
-points of a batch, one batched Cholesky, and chi2 / ln|C| from the factor.
+The points run in batches on the GPU: C(theta) = S(theta) + s N for all
+points of a batch (one GEMM per block region against a per-multipole basis
+built once, ``engine.SignalBasis``, for batches of 64 or more), one batched
+Cholesky, and chi2 / ln|C| from the factor; a grid of more than one batch
+replays one captured CUDA graph per batch (``engine.LnlGraph``).
 ``precision="mixed"`` factors C in FP32 and refines chi2 in FP64 (one step
 against the FP64 C); ln|C| then carries the FP32 factor's rounding.
 
@@ -345,15 +348,28 @@ class PICSLike(_Base):
 
     # -- evaluation ---------------------------------------------------------
     def compute_points(self, spectra: list, noise_scale=None):
-        """chi2 (B, nsims), ln|C| (B,), lnL (B, nsims) on the device for explicit spectra dicts."""
+        """chi2 (B, nsims), ln|C| (B,), lnL (B, nsims) on the device for explicit spectra dicts.
+
+        Grids of more than one batch run every batch as a replay of one
+        captured CUDA graph (engine.LnlGraph); a single batch runs eagerly."""
         L = self.layout
         chi2s, lds, lnls = [], [], []
+        runner = None
+        if len(spectra) > self.batch_size:
+            key = (self.batch_size, self.precision)
+            if getattr(self, "_graph_key", None) != key:
+                self._graph = eng.LnlGraph(self.engine, self._dev_N, self._dev_X, self.batch_size, self.precision)
+                self._graph_key = key
+            runner = self._graph
         for b0 in range(0, len(spectra), self.batch_size):
             part = spectra[b0: b0 + self.batch_size]
             cl = np.stack([L.smoothed_cl_table(c) for c in part])
             sc = None if noise_scale is None else np.asarray(noise_scale[b0: b0 + len(part)], dtype=np.float64)
-            chi2, ld, lnl, info = self.engine.lnl(cl, self._dev_N, self._dev_X, noise_scale=sc,
-                                                  precision=self.precision)
+            if runner is not None:
+                chi2, ld, lnl, info = runner(cl, sc)
+            else:
+                chi2, ld, lnl, info = self.engine.lnl(cl, self._dev_N, self._dev_X, noise_scale=sc,
+                                                      precision=self.precision)
             bad = info.cpu().numpy()
             if np.any(bad != 0):
                 k = int(np.flatnonzero(bad)[0])

@@ -126,3 +126,45 @@ def test_picslike_in_memory_grid_and_mixed_precision():
             assert np.max(np.abs(lnl / d["ref_lnl"][:, 0] - 1)) <= tol
         else:
             assert np.max(np.abs(lnl - d["ref_lnl"][:, 0])) <= tol
+
+
+def test_graph_replayed_batches_equal_eager_batches():
+    """PICSLike grids larger than one batch replay one captured CUDA graph per
+    batch (engine.LnlGraph); the results equal a single eager batch bit for bit
+    (every point's arithmetic is independent of the other points of its batch)."""
+    from types import SimpleNamespace
+
+    from cosmoforge_b200 import engine, workloads
+    from cosmoforge_b200.layout import build_layout
+    from cosmoforge_b200.picslike import ParameterGrid, PICSLike
+
+    d = load("picslike_tqu_nside8")
+    p = params_of(d)
+    lmax_sig = int(p["lmax_signal"])
+    spectra = {(float(i),): workloads.model_cls(t, lmax_sig) for i, t in enumerate(d["thetas"])}
+    grid = ParameterGrid(SimpleNamespace(nside=8), {"idx": np.arange(len(spectra), dtype=float)},
+                         theoretical_spectra=spectra, lmax_signal=lmax_sig)
+    out = {}
+    for bs in (3, 256):
+        pl = PICSLike(p, basis=False, mask=d["mask"], noise_cov1=np.diag(d["noise_diag"]), cls_data=spectra[(0.0,)],
+                      beam=d["beam"], maps1=d["maps"], parameter_grid=grid, batch_size=bs)
+        pl.run()
+        out[bs] = (pl.get_chi_squared(), pl.get_log_likelihood())
+    assert np.array_equal(out[3][0], out[256][0]) and np.array_equal(out[3][1], out[256][1])
+
+    # config 3, 200 points through a 128-point graph (a full and a partial replay), basis build
+    pb = workloads.config3()
+    L = build_layout(pb.params, pb.mask, pb.beam)
+    E = engine.Engine(L)
+    N = torch.from_numpy(pb.noise).cuda()
+    g = torch.Generator(device="cuda").manual_seed(5)
+    X = torch.randn((L.n, 1), dtype=torch.float64, device="cuda", generator=g) * 10.0
+    th = workloads.sobol_points(200, seed=6)
+    cl = np.stack([L.smoothed_cl_table(workloads.model_cls(t, L.lmax_signal)) for t in th])
+    for prec in ("fp64", "mixed"):
+        G = engine.LnlGraph(E, N, X, 128, precision=prec)
+        got = [G(cl[b0:b0 + 128], th[b0:b0 + 128, 4]) for b0 in (0, 128)]
+        lnl_g = torch.cat([r[2] for r in got]).cpu().numpy()
+        _, _, lnl_e, info = E.lnl(cl, N, X, noise_scale=th[:, 4], precision=prec, build="basis")
+        assert int(info.abs().max()) == 0
+        assert np.array_equal(lnl_g, lnl_e.cpu().numpy()), prec
