@@ -202,63 +202,136 @@ def keep_modes(evals: np.ndarray, epsilon=None, mode_fraction=None) -> np.ndarra
 
 
 def _per_field(x, nf, what):
-    """A scalar or a per-field list of thresholds as one value per field."""
+    """A scalar or a per-field list of thresholds as one value per field; an
+    entry may be an (E, B) pair for a spin-2 field."""
     if x is None or isinstance(x, (int, float)):
         return [x] * nf
+    if isinstance(x, tuple) and len(x) == 2 and nf == 1:
+        return [x]
     x = list(x)
     if len(x) != nf:
         raise ValueError(f"{what} needs one value per field ({nf}), got {len(x)}")
-    if any(isinstance(v, (tuple, list)) for v in x):
-        raise NotImplementedError(f"{what}: separate E / B thresholds are not implemented")
-    return x
+    return [tuple(v) if isinstance(v, (tuple, list)) else v for v in x]
+
+
+def _sym_sqrt(S: torch.Tensor) -> torch.Tensor:
+    """S^1/2 of a symmetric positive semi-definite matrix from its
+    eigendecomposition, eigenvalues clipped at 1e-30 (cosmocore/basis/pixel.py:
+    339-348)."""
+    w, Q = torch.linalg.eigh(S)
+    return (Q * torch.sqrt(torch.clamp(w, min=1e-30))[None, :]) @ Q.T
 
 
 class CompressedPlan:
     """Eigen-truncated pixel basis (the reference's PixelBasis with epsilon /
     mode_fraction, cosmocore/basis/pixel.py:265-557, 965-1055, 1493-1996).
 
-    Per field f, the kept eigenvectors U_f of P_f = V_f^T V_f ("harmonic") or
-    P_f (N_eff^-1)_ff P_f ("noise_weighted", the default), with
-    N_eff = N + S_fixed when the inference window is narrower than the signal
-    band; U = diag(U_f) (n x dim).  The estimator then runs in the kept
-    subspace: C_c = U^T C U, derivatives (V U)^T E_l (V U), noise U^T N U,
-    maps U^T x, through the same harmonic contractions.  The symmetric
-    eigendecompositions are cuSOLVER's (torch.linalg.eigh, once per basis).
+    Per field f, the kept eigenvectors U_f of the compression matrix of the
+    field's rows of V (V_f, n_f columns) and its block of the effective noise
+    N_eff = N + S_fixed (N itself when the inference window covers the signal
+    band):
+
+    * "harmonic":         P_f = V_f^T V_f
+    * "noise_weighted":   P_f (N_eff^-1)_ff P_f  (the default)
+    * "total_covariance": P_f C_f^-1 P_f, C_f = (N_eff)_ff + V_f^T Lambda V_f
+    * "snr":              S_f^1/2 (N_eff^-1)_ff S_f^1/2, S_f = V_f^T Lambda V_f
+
+    Lambda holds C_l at each row's multipole (the ``C_ell`` array, or the first
+    entry of a ``C_ell`` dict).  A spin-2 field given an (E, B) pair of
+    thresholds is split: the E rows and the B rows each get their own matrix
+    (Lambda from ``C_ell["EE"]`` / ``["BB"]``) and threshold, and the two sets
+    of kept vectors are orthogonalised together by an SVD (singular values
+    above 1e-10 of the largest).  U = diag(U_f) (n x dim).  The estimator then
+    runs in the kept subspace: C_c = U^T C U, derivatives (V U)^T E_l (V U),
+    noise U^T N U, maps U^T x, through the same harmonic contractions.  The
+    symmetric eigendecompositions and the SVD are cuSOLVER's
+    (torch.linalg.eigh / svd, once per basis).
     """
 
-    TARGETS = ("harmonic", "noise_weighted")
+    TARGETS = ("harmonic", "noise_weighted", "total_covariance", "snr")
 
     def __init__(self, hp: HarmonicPlan, N: torch.Tensor, fixed_table, epsilon=None, mode_fraction=None,
-                 target: str = "noise_weighted"):
+                 target: str = "noise_weighted", C_ell=None):
         if epsilon is not None and mode_fraction is not None:
             raise ValueError("epsilon and mode_fraction are mutually exclusive")
         if target not in self.TARGETS:
-            raise NotImplementedError(f"compression_target={target!r}: only {self.TARGETS} are implemented")
+            raise ValueError(f"Unknown compression target '{target}'. Available: {list(self.TARGETS)}")
+        if target in ("total_covariance", "snr") and C_ell is None:
+            raise ValueError(f"C_ell is required for '{target}' compression_target")
         E, L = hp.E, hp.L
         nf = len(L.fields)
         eps = _per_field(epsilon, nf, "epsilon")
         mfs = _per_field(mode_fraction, nf, "mode_fraction")
         for mf in mfs:
-            if mf is not None and not (0 < mf <= 1):
-                raise ValueError(f"mode_fraction must be in (0, 1], got {mf}")
+            for v in (mf if isinstance(mf, tuple) else (mf,)):
+                if v is not None and not (0 < v <= 1):
+                    raise ValueError(f"mode_fraction must be in (0, 1], got {v}")
         if epsilon is None and mode_fraction is None:
             eps = [1e-6] * nf
         self.hp, self.E, self.L = hp, E, L
         N = N.to(E.dev, F64).contiguous()
         switch = hp.lmax < L.lmax_signal or hp.lmin > 2
         N_eff = N + E.signal(hp.outside(fixed_table)) if switch else N.clone()
-        Ninv = E.spd_inverse(N_eff) if target == "noise_weighted" else None
+        Ninv = E.spd_inverse(N_eff.clone()) if target in ("noise_weighted", "snr") else None
+        ell_of_row = hp.rowinfo[:, 1].to(torch.long)
+
+        def lam_rows(rows, cl):
+            c = torch.as_tensor(np.asarray(cl, dtype=np.float64), device=E.dev)
+            ell = ell_of_row[rows]
+            return torch.where(ell < c.numel(), c[torch.clamp(ell, max=c.numel() - 1)], torch.zeros_like(c[:1]))
+
+        def comp_matrix(Vs, cols, cl):
+            P = E.gemm(Vs, Vs, transa=True)
+            if target == "harmonic":
+                return P
+            if target == "noise_weighted":
+                return E.gemm(E.gemm(P, Ninv[cols, cols].contiguous()), P)
+            S = E.gemm(Vs, Vs * cl[:, None], transa=True)
+            if target == "total_covariance":
+                Cinv = E.spd_inverse(N_eff[cols, cols] + S)
+                return E.gemm(E.gemm(P, Cinv), P)
+            Sq = _sym_sqrt(0.5 * (S + S.T))
+            return E.gemm(E.gemm(Sq, Ninv[cols, cols].contiguous()), Sq)
+
+        def kept(M, e, mf):
+            M = 0.5 * (M + M.T)
+            ev, vec = torch.linalg.eigh(M)
+            keep = keep_modes(ev.cpu().numpy(), e, mf)
+            return vec[:, torch.from_numpy(keep.copy()).to(E.dev)]
+
+        def first_cl():
+            return next(iter(C_ell.values())) if isinstance(C_ell, dict) else C_ell
+
         blocks = []
         for fi, f in enumerate(L.fields):
             cols = slice(f.offset, f.offset + f.nrows)
             cs = [c for c, (g, _) in enumerate(hp.comps) if g == fi]
-            Vf = hp.V[cs[0] * hp.nrow:(cs[-1] + 1) * hp.nrow, cols].contiguous()
-            P = E.gemm(Vf, Vf, transa=True)
-            M = P if Ninv is None else E.gemm(E.gemm(P, Ninv[cols, cols].contiguous()), P)
-            M = 0.5 * (M + M.T)
-            ev, vec = torch.linalg.eigh(M)
-            keep = keep_modes(ev.cpu().numpy(), eps[fi], mfs[fi])
-            blocks.append((cols, vec[:, torch.from_numpy(keep.copy()).to(E.dev)]))
+            rows = torch.arange(cs[0] * hp.nrow, (cs[-1] + 1) * hp.nrow, device=E.dev)
+            e_f, m_f = eps[fi], mfs[fi]
+            split = f.spin == 2 and (isinstance(e_f, tuple) or isinstance(m_f, tuple))
+            if split:
+                parts = []
+                for j, (c, lab) in enumerate(zip(cs, ("EE", "BB"))):
+                    r = torch.arange(c * hp.nrow, (c + 1) * hp.nrow, device=E.dev)
+                    Vs = hp.V[r, cols].contiguous()
+                    cl = None
+                    if target in ("total_covariance", "snr"):
+                        src = C_ell.get(lab) if isinstance(C_ell, dict) else None
+                        if src is None:
+                            raise ValueError(f"C_ell[{lab!r}] is required for '{target}' with separate E / B "
+                                             "thresholds")
+                        cl = lam_rows(r, src)
+                    parts.append(kept(comp_matrix(Vs, cols, cl), e_f[j] if isinstance(e_f, tuple) else None,
+                                      m_f[j] if isinstance(m_f, tuple) else None))
+                Ucat = torch.cat(parts, dim=1)
+                Q, sv, _ = torch.linalg.svd(Ucat, full_matrices=False)
+                blocks.append((cols, Q[:, sv > 1e-10 * sv[0]]))
+            else:
+                Vf = hp.V[rows, cols].contiguous()
+                cl = lam_rows(rows, first_cl()) if target in ("total_covariance", "snr") else None
+                e_s = e_f[0] if isinstance(e_f, tuple) else e_f
+                m_s = None if isinstance(m_f, tuple) else m_f
+                blocks.append((cols, kept(comp_matrix(Vf, cols, cl), e_s, m_s)))
         self.dim = sum(b.shape[1] for _, b in blocks)
         self.dims = [b.shape[1] for _, b in blocks]
         self.U = torch.zeros((L.n, self.dim), dtype=F64, device=E.dev)

@@ -70,7 +70,7 @@ def _check_basis(basis):
         method = basis.get("method", "auto")
         if method not in ("auto", "harmonic", "pixel"):
             raise ValueError(f"unknown basis method {method!r}")
-        unknown = set(basis) - {"method", "epsilon", "mode_fraction", "compression_target"}
+        unknown = set(basis) - {"method", "epsilon", "mode_fraction", "compression_target", "C_ell"}
         if unknown:
             raise NotImplementedError(f"basis options {sorted(unknown)} are not implemented")
         if basis.get("epsilon") is not None or basis.get("mode_fraction") is not None:
@@ -86,7 +86,7 @@ def _compression_of(basis) -> dict:
     if not isinstance(basis, dict):
         return {}
     return dict(epsilon=basis.get("epsilon"), mode_fraction=basis.get("mode_fraction"),
-                target=basis.get("compression_target", "noise_weighted"))
+                target=basis.get("compression_target", "noise_weighted"), C_ell=basis.get("C_ell"))
 
 
 def _resolve_method(req: str, L) -> str:

@@ -345,27 +345,79 @@ def keep_modes(evals, epsilon=None, mode_fraction=None):
     return order[keep]
 
 
-def compression_basis(L, V, N_eff, lmin, lmax, epsilon=None, mode_fraction=None, target="noise_weighted"):
-    """Block-diagonal U (n x dim): per field, the kept eigenvectors of
-    P_f = V_f^T V_f ("harmonic") or P_f (N_eff^-1)_ff P_f ("noise_weighted")
-    (cosmocore/basis/pixel.py:447-557, 1493-1612)."""
+def _sym_sqrt(S):
+    """S^1/2 by eigendecomposition, eigenvalues clipped at 1e-30 (cosmocore/basis/pixel.py:339-348)."""
+    w, Q = np.linalg.eigh(S)
+    return (Q * np.sqrt(np.maximum(w, 1e-30))) @ Q.T
+
+
+def compression_basis(L, V, N_eff, lmin, lmax, epsilon=None, mode_fraction=None, target="noise_weighted",
+                      C_ell=None):
+    """Block-diagonal U (n x dim): per field, the kept eigenvectors of the
+    compression matrix of the field's rows of V (cosmocore/basis/pixel.py:
+    265-557, 965-1055, 1493-1612):
+    "harmonic" P_f = V_f^T V_f; "noise_weighted" P_f (N_eff^-1)_ff P_f;
+    "total_covariance" P_f ((N_eff)_ff + V_f^T Lam V_f)^-1 P_f; "snr"
+    S_f^1/2 (N_eff^-1)_ff S_f^1/2 with S_f = V_f^T Lam V_f, Lam = C_l at each
+    row's multipole (C_ell an array or the first value of a dict).  A spin-2
+    field with an (E, B) threshold pair builds the E rows' and the B rows'
+    matrices apart (Lam from C_ell["EE"] / ["BB"]), keeps each by its own
+    threshold, and orthogonalises the union by an economy SVD (singular
+    values above 1e-10 of the largest)."""
     comps = components(L)
-    off, _ = mode_offsets(L, lmin, lmax)
     nrow = (lmax + 1) ** 2 - lmin ** 2
+    ell_row = np.concatenate([np.repeat(np.arange(lmin, lmax + 1), 2 * np.arange(lmin, lmax + 1) + 1)] * len(comps))
     Ninv = np.linalg.inv(N_eff)
+
+    def lam(rows, cl):
+        c = np.asarray(cl, dtype=np.float64)
+        e = ell_row[rows]
+        return np.where(e < c.size, c[np.minimum(e, c.size - 1)], 0.0)
+
+    def comp_matrix(Vs, cols, cl):
+        P = Vs.T @ Vs
+        if target == "harmonic":
+            return P
+        if target == "noise_weighted":
+            return P @ Ninv[np.ix_(cols, cols)] @ P
+        S = Vs.T @ (Vs * cl[:, None])
+        if target == "total_covariance":
+            return P @ np.linalg.inv(N_eff[np.ix_(cols, cols)] + S) @ P
+        Sq = _sym_sqrt(S)
+        return Sq @ Ninv[np.ix_(cols, cols)] @ Sq
+
+    def kept(M, e, m):
+        ev, vec = np.linalg.eigh(0.5 * (M + M.T))
+        return vec[:, keep_modes(ev, e, m)]
+
+    def per_field(x, fi):
+        return x[fi] if isinstance(x, list) else x
+
     blocks = []
     for fi, f in enumerate(L.fields):
         cols = np.arange(f.offset, f.offset + f.nrows)
-        rows = np.concatenate([np.arange(ci * nrow, (ci + 1) * nrow) for ci, (g, _) in enumerate(comps) if g == fi])
-        Vf = V[np.ix_(rows, cols)]
-        P = Vf.T @ Vf
-        M = P if target == "harmonic" else P @ Ninv[np.ix_(cols, cols)] @ P
-        ev, vec = np.linalg.eigh(M)
-        e_f = epsilon[fi] if isinstance(epsilon, (list, tuple)) else epsilon
-        m_f = mode_fraction[fi] if isinstance(mode_fraction, (list, tuple)) else mode_fraction
+        cis = [ci for ci, (g, _) in enumerate(comps) if g == fi]
+        rows = np.concatenate([np.arange(ci * nrow, (ci + 1) * nrow) for ci in cis])
+        e_f, m_f = per_field(epsilon, fi), per_field(mode_fraction, fi)
         if e_f is None and m_f is None and epsilon is None and mode_fraction is None:
             e_f = 1e-6
-        blocks.append((cols, vec[:, keep_modes(ev, e_f, m_f)]))
+        if f.spin == 2 and (isinstance(e_f, tuple) or isinstance(m_f, tuple)):
+            parts = []
+            for j, (ci, lab) in enumerate(zip(cis, ("EE", "BB"))):
+                r = np.arange(ci * nrow, (ci + 1) * nrow)
+                cl = lam(r, C_ell[lab]) if target in ("total_covariance", "snr") else None
+                parts.append(kept(comp_matrix(V[np.ix_(r, cols)], cols, cl),
+                                  e_f[j] if isinstance(e_f, tuple) else None,
+                                  m_f[j] if isinstance(m_f, tuple) else None))
+            Q, sv, _ = np.linalg.svd(np.hstack(parts), full_matrices=False)
+            blocks.append((cols, Q[:, sv > 1e-10 * sv[0]]))
+        else:
+            cl = None
+            if target in ("total_covariance", "snr"):
+                cl = lam(rows, next(iter(C_ell.values())) if isinstance(C_ell, dict) else C_ell)
+            e_s = e_f[0] if isinstance(e_f, tuple) else e_f
+            m_s = None if isinstance(m_f, tuple) else m_f
+            blocks.append((cols, kept(comp_matrix(V[np.ix_(rows, cols)], cols, cl), e_s, m_s)))
     dim = sum(b.shape[1] for _, b in blocks)
     U = np.zeros((L.n, dim))
     c = 0
@@ -376,7 +428,7 @@ def compression_basis(L, V, N_eff, lmin, lmax, epsilon=None, mode_fraction=None,
 
 
 def compressed_estimator(L, N, tab, tab_fixed, maps, signal_pixel, epsilon=None, mode_fraction=None,
-                         target="noise_weighted", weights=None):
+                         target="noise_weighted", weights=None, C_ell=None):
     """F, raw bias, raw q of the compressed pixel basis: C_c = U^T C U with C
     the harmonic-basis covariance, derivatives (V U)^T E_l (V U), bias with
     U^T N U, maps U^T x (cosmocore/basis/pixel.py:1614-1996)."""
@@ -387,7 +439,7 @@ def compressed_estimator(L, N, tab, tab_fixed, maps, signal_pixel, epsilon=None,
     S_fixed = signal_pixel(_outside(tab_fixed, lmin, lmax))
     switch = lmax < L.lmax_signal or lmin > 2
     N_eff = N + S_fixed if switch else N
-    U = compression_basis(L, V, N_eff, lmin, lmax, epsilon, mode_fraction, target)
+    U = compression_basis(L, V, N_eff, lmin, lmax, epsilon, mode_fraction, target, C_ell)
     Cc = U.T @ (N + S) @ U
     Cc_inv = np.linalg.inv(Cc)
     VU = V @ U

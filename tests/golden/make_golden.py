@@ -363,8 +363,25 @@ def _compressed_case(src: str, name: str, basis: dict):
     out.update(ref_fisher=np.asarray(f.get_fisher_matrix()), ref_q_raw=np.asarray(s.qml_results),
                ref_noise_bias_raw=np.asarray(s.qml_noise_bias), ref_clhat=np.asarray(s.get_power_spectra()),
                ref_noise_bias=np.asarray(s.get_noise_bias()), ref_invfisher=np.asarray(s.invfisher),
-               ref_basis=np.array(repr(basis)), ref_dim=int(f.basis_manager.dim))
+               ref_basis=np.array(repr({k: v for k, v in basis.items() if k != "C_ell"})),
+               ref_dim=int(f.basis_manager.dim))
     _save(name, **out)
+
+
+def _smoothed_cl(src: str) -> dict:
+    """{label: C_l b_l^2} of a fixture's spectra with its beam (T, E, B rows): the
+    beam-smoothed C_l a user passes as a compressed basis's ``C_ell``."""
+    d = np.load(HERE / f"{src}.npz")
+    beam = d["beam"]
+    row = {"T": 0, "E": 1, "B": 2}
+    out = {}
+    for k in d.files:
+        if k.startswith("cl_"):
+            lab = k[3:]
+            c = np.asarray(d[k], dtype=np.float64)
+            n = min(c.size, beam.shape[1])
+            out[lab] = c[:n] * beam[row[lab[0]], :n] * beam[row[lab[1]], :n]
+    return out
 
 
 def _harmonic_case(src: str, name: str):
@@ -547,6 +564,20 @@ CASES = {
     "compressed_h_config0": lambda: _compressed_case(
         "config0_tt_nside8", "compressed_h_config0_tt_nside8",
         {"method": "pixel", "epsilon": 1e-2, "compression_target": "harmonic"}),
+    "compressed_tc_config0": lambda: _compressed_case(
+        "config0_tt_nside8", "compressed_tc_config0_tt_nside8",
+        {"method": "pixel", "epsilon": 1e-3, "compression_target": "total_covariance",
+         "C_ell": _smoothed_cl("config0_tt_nside8")["TT"]}),
+    "compressed_snr_config0": lambda: _compressed_case(
+        "config0_tt_nside8", "compressed_snr_config0_tt_nside8",
+        {"method": "pixel", "epsilon": 1e-4, "compression_target": "snr",
+         "C_ell": _smoothed_cl("config0_tt_nside8")["TT"]}),
+    "compressed_eb_tqu_cut": lambda: _compressed_case(
+        "tqu_cut_nside4", "compressed_eb_tqu_cut_nside4", {"method": "pixel", "epsilon": [1e-3, (1e-3, 1e-2)]}),
+    "compressed_tc_eb_tqu_cut": lambda: _compressed_case(
+        "tqu_cut_nside4", "compressed_tc_eb_tqu_cut_nside4",
+        {"method": "pixel", "epsilon": [1e-3, (2e-3, 1e-2)], "compression_target": "total_covariance",
+         "C_ell": {k: _smoothed_cl("tqu_cut_nside4")[k] for k in ("TT", "EE", "BB")}}),
 }
 
 if __name__ == "__main__":

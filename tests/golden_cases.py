@@ -38,3 +38,17 @@ def noise_of(d: dict) -> np.ndarray:
 
 QML_CASES = ["fortran_qube_nside8_B", "nside4_T", "nside4_QU", "nside4_TQU", "nside4_TEB",
              "config0_tt_nside8", "tqu_cut_nside4"]
+
+
+def smoothed_cls(d: dict) -> dict:
+    """{label: C_l b_l^2} with the fixture's beam rows (T, E, B): the
+    beam-smoothed spectra passed as a compressed basis's ``C_ell``
+    (tests/golden/make_golden.py builds the same arrays)."""
+    beam = d["beam"]
+    row = {"T": 0, "E": 1, "B": 2}
+    out = {}
+    for lab, c in cls_of(d).items():
+        c = np.asarray(c, dtype=np.float64)
+        n = min(c.size, beam.shape[1])
+        out[lab] = c[:n] * beam[row[lab[0]], :n] * beam[row[lab[1]], :n]
+    return out

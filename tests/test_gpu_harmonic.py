@@ -21,7 +21,7 @@ import torch
 
 from cosmoforge_b200 import workloads
 from cosmoforge_b200.layout import build_layout
-from golden_cases import cls_of, load, noise_of, params_of
+from golden_cases import cls_of, load, noise_of, params_of, smoothed_cls
 
 pytestmark = pytest.mark.gpu
 
@@ -107,7 +107,14 @@ def test_harmonic_matches_pixel_at_config1_size():
     ("compressed_tqu_cut_nside4", {"method": "pixel", "epsilon": 1e-3}),
     ("compressed_config0_tt_nside8", {"method": "pixel", "epsilon": 1e-3}),
     ("compressed_mf_tqu_cut_nside4", {"method": "pixel", "mode_fraction": [0.7, 0.6]}),
-    ("compressed_h_config0_tt_nside8", {"method": "pixel", "epsilon": 1e-2, "compression_target": "harmonic"})])
+    ("compressed_h_config0_tt_nside8", {"method": "pixel", "epsilon": 1e-2, "compression_target": "harmonic"}),
+    ("compressed_tc_config0_tt_nside8", {"method": "pixel", "epsilon": 1e-3, "compression_target": "total_covariance",
+                                         "C_ell": "TT"}),
+    ("compressed_snr_config0_tt_nside8", {"method": "pixel", "epsilon": 1e-4, "compression_target": "snr",
+                                          "C_ell": "TT"}),
+    ("compressed_eb_tqu_cut_nside4", {"method": "pixel", "epsilon": [1e-3, (1e-3, 1e-2)]}),
+    ("compressed_tc_eb_tqu_cut_nside4", {"method": "pixel", "epsilon": [1e-3, (2e-3, 1e-2)],
+                                         "compression_target": "total_covariance", "C_ell": ("TT", "EE", "BB")})])
 def test_compressed_dropin_matches_reference(name, basis):
     """The eigen-truncated pixel basis (cuSOLVER eigenvectors) through the
     drop-in classes against the reference's run with the same basis dict:
@@ -116,6 +123,12 @@ def test_compressed_dropin_matches_reference(name, basis):
 
     d = load(name)
     p = params_of(d)
+    basis = dict(basis)
+    if isinstance(basis.get("C_ell"), str):  # the fixture's beam-smoothed spectra, as the reference run got them
+        basis["C_ell"] = smoothed_cls(d)[basis["C_ell"]]
+    elif isinstance(basis.get("C_ell"), tuple):
+        sm = smoothed_cls(d)
+        basis["C_ell"] = {k: sm[k] for k in basis["C_ell"]}
     f = qube.Fisher(p, basis=basis, mask=d["mask"], noise_cov1=noise_of(d), cls_data=cls_of(d), beam=d["beam"])
     f.run()
     assert f.method == "compressed" and f.dim == int(d["ref_dim"])

@@ -19,7 +19,7 @@ import numpy as np
 import pytest
 
 from cosmoforge_b200.layout import build_layout
-from golden_cases import cls_of, load, noise_of, params_of
+from golden_cases import cls_of, load, noise_of, params_of, smoothed_cls
 from oracle import harmonic_oracle as ho
 from oracle import oracle as orc
 
@@ -72,7 +72,24 @@ def test_harmonic_estimator_matches_reference(src, hname):
 COMPRESSED = [("compressed_tqu_cut_nside4", dict(epsilon=1e-3)),
               ("compressed_config0_tt_nside8", dict(epsilon=1e-3)),
               ("compressed_mf_tqu_cut_nside4", dict(mode_fraction=[0.7, 0.6])),
-              ("compressed_h_config0_tt_nside8", dict(epsilon=1e-2, target="harmonic"))]
+              ("compressed_h_config0_tt_nside8", dict(epsilon=1e-2, target="harmonic")),
+              ("compressed_tc_config0_tt_nside8", dict(epsilon=1e-3, target="total_covariance", C_ell="TT")),
+              ("compressed_snr_config0_tt_nside8", dict(epsilon=1e-4, target="snr", C_ell="TT")),
+              ("compressed_eb_tqu_cut_nside4", dict(epsilon=[1e-3, (1e-3, 1e-2)])),
+              ("compressed_tc_eb_tqu_cut_nside4", dict(epsilon=[1e-3, (2e-3, 1e-2)], target="total_covariance",
+                                                       C_ell=("TT", "EE", "BB")))]
+
+
+def _with_cell(d, kw):
+    """The test's keyword arguments with C_ell named by label(s) replaced by the
+    fixture's beam-smoothed spectra (an array, or a dict in the given order)."""
+    kw = dict(kw)
+    if isinstance(kw.get("C_ell"), str):
+        kw["C_ell"] = smoothed_cls(d)[kw["C_ell"]]
+    elif isinstance(kw.get("C_ell"), tuple):
+        sm = smoothed_cls(d)
+        kw["C_ell"] = {k: sm[k] for k in kw["C_ell"]}
+    return kw
 
 
 @pytest.mark.parametrize("name,kw", COMPRESSED)
@@ -88,7 +105,7 @@ def test_compressed_estimator_matches_reference(name, kw):
     L = build_layout(params_of(d), d["mask"], d["beam"])
     tab = L.smoothed_cl_table(cls_of(d))
     F, b, q, dim = ho.compressed_estimator(L, noise_of(d), tab, tab, d["maps"],
-                                           lambda t: orc.signal_matrix(L, t), **kw)
+                                           lambda t: orc.signal_matrix(L, t), **_with_cell(d, kw))
     if L.remove_nb:
         q = q - b[None, :]
     assert dim == int(d["ref_dim"])
