@@ -32,7 +32,10 @@ def test_basis_rejects(basis, exc):
 
 def test_compression_options():
     c = _compression_of({"method": "pixel", "epsilon": 1e-3})
-    assert c == {"epsilon": 1e-3, "mode_fraction": None, "target": "noise_weighted"}
+    assert c == {"epsilon": 1e-3, "mode_fraction": None, "target": "noise_weighted", "C_ell": None}
+    c = _compression_of({"method": "pixel", "epsilon": [1e-3, (1e-3, 1e-2)], "compression_target": "snr",
+                         "C_ell": [0.0, 1.0]})
+    assert c["target"] == "snr" and c["epsilon"] == [1e-3, (1e-3, 1e-2)] and c["C_ell"] == [0.0, 1.0]
     assert _compression_of("harmonic") == {}
 
 
