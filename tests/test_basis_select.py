@@ -68,8 +68,9 @@ def test_per_field_thresholds():
     assert harmonic._per_field([0.7, 0.6], 2, "mode_fraction") == [0.7, 0.6]
     with pytest.raises(ValueError):
         harmonic._per_field([0.7], 2, "mode_fraction")
-    with pytest.raises(NotImplementedError):
-        harmonic._per_field([(0.7, 0.5), 0.6], 2, "mode_fraction")
+    # an (E, B) pair per spin-2 field (cosmocore/basis/pixel.py:447-557)
+    assert harmonic._per_field([0.6, (0.7, 0.5)], 2, "mode_fraction") == [0.6, (0.7, 0.5)]
+    assert harmonic._per_field([1e-3, [1e-3, 1e-2]], 2, "epsilon") == [1e-3, (1e-3, 1e-2)]
 
 
 def test_auto_falls_back_to_pixel_for_unsupported_layouts():
