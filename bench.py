@@ -744,6 +744,7 @@ KERNEL_DOC = """Single-kernel timing cases (``python bench.py kernel CASE SHAPE`
     python bench.py kernel spd_inverse N
     python bench.py kernel harmonic 1        (config-1 harmonic-basis solve)
     python bench.py kernel map_solves NMAPS [--precision fp64|mixed]
+    python bench.py kernel lnl POINTS [--precision fp64|mixed]      (config-3 likelihood batch)
 
 Each case fills seeded random operands on cuda:0, runs two untimed launches,
 then times `reps` launches with CUDA events on the launching stream and prints
@@ -914,6 +915,28 @@ def map_solves_case(nmaps, precision="mixed"):
     return fn, 0.0, None
 
 
+def lnl_case(points, precision="mixed", build="auto"):
+    """Batched likelihood of `points` Sobol points of the config-3 problem (TQU
+    nside 8, n = 1312): C(theta), Cholesky factor, chi2 and ln|C| per call."""
+    from cosmoforge_b200 import engine, qube, sampler, workloads
+    from cosmoforge_b200.layout import build_layout
+
+    pb = workloads.config3()
+    L = build_layout(pb.params, pb.mask, pb.beam)
+    E = engine.Engine(L)
+    N = torch.from_numpy(pb.noise).cuda()
+    x = qube.draw_maps(L, pb.cls, N, 1, seed=0)
+    th = torch.as_tensor(workloads.sobol_points(points), device="cuda")
+    cl = sampler.ModelTables(L, "cuda")(th)
+    s = th[:, 4].contiguous()
+
+    def fn():
+        E.lnl(cl, N, x, noise_scale=s, precision=precision, build=build)
+
+    fn._keep = (E, N, x, cl, s)
+    return fn, float(points) * L.n ** 3 / 3.0, None
+
+
 def kernel_main(argv=None):
     global torch, _lib
     import torch
@@ -922,13 +945,13 @@ def kernel_main(argv=None):
     ap = argparse.ArgumentParser(prog="bench.py kernel", description=KERNEL_DOC,
                                  formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("case", choices=["umma_gemm", "umma_trace", "dgemm", "spd_inverse", "harmonic",
-                                           "map_solves"])
+                                           "map_solves", "lnl"])
     ap.add_argument("shape", help="comma-separated sizes")
     ap.add_argument("--planes", type=int, default=3)
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--kc", type=int, default=16, help="promotion interval of the tensor-core kernels")
     ap.add_argument("--splits", type=int, default=0)
-    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed", help="map_solves only")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed", help="map_solves and lnl")
     a = ap.parse_args(argv)
     dims = [int(x) for x in a.shape.split(",")]
     lib = _lib.lib()
@@ -943,6 +966,8 @@ def kernel_main(argv=None):
         fn, fl, err = harmonic_case(*dims)
     elif a.case == "map_solves":
         fn, fl, err = map_solves_case(*dims, precision=a.precision)
+    elif a.case == "lnl":
+        fn, fl, err = lnl_case(*dims, precision=a.precision)
     else:
         fn, fl, err = spd_inverse_case(*dims)
     ms = time_launches(fn, a.reps)
