@@ -50,6 +50,18 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity)
     return ok != 0;
 }
 
+// Non-blocking probe of a barrier phase (no suspend hint).
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
 __device__ __forceinline__ unsigned long long now_ns()
 {
     unsigned long long t;
@@ -57,13 +69,15 @@ __device__ __forceinline__ unsigned long long now_ns()
     return t;
 }
 
-// Wait bounded in time; false when the bound ran out.
+// Wait bounded in time; false when the bound ran out.  Bounds under 1 ms
+// probe without suspending (try_wait may sleep up to its hint) and read the
+// clock on every probe, so a bound of 0 gives up at the first unsatisfied one.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned long long wait_ns)
 {
     const unsigned long long t0 = now_ns();
     const bool tight = wait_ns < 1000000ull;
     for (unsigned i = 0;; ++i) {
-        if (mbar_try(bar, parity)) return true;
+        if (tight ? mbar_test(bar, parity) : mbar_try(bar, parity)) return true;
         if ((tight || (i & 255) == 255) && now_ns() - t0 >= wait_ns) return false;
     }
 }

@@ -84,6 +84,18 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity)
         : "memory");
     return ok != 0;
 }
+// Non-blocking probe of a barrier phase (no suspend hint).
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
 __device__ __forceinline__ unsigned long long now_ns()
 {
     unsigned long long t;
@@ -98,9 +110,9 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
                                           unsigned long long wait_ns)
 {
     const unsigned long long t0 = now_ns();
-    const bool tight = wait_ns < 1000000ull;
+    const bool tight = wait_ns < 1000000ull;  // probe without suspending (try_wait may sleep up to its hint)
     for (unsigned i = 0;; ++i) {
-        if (mbar_try(bar, parity)) return true;
+        if (tight ? mbar_test(bar, parity) : mbar_try(bar, parity)) return true;
         if (*abort_flag) return false;
         if ((tight || (i & 255) == 255) && now_ns() - t0 >= wait_ns) break;
     }

@@ -455,8 +455,9 @@ class SignalBasis:
                 for (r0, c0, R, Cc), K in zip(spans, Ks):
                     K[1 + j * Lp: 1 + (j + 1) * Lp] = Sk[:, r0:r0 + R, c0:c0 + Cc]
                 del Sk
+            sp_dev = torch.tensor(sp, dtype=torch.long, device=E.dev)
             for (r0, c0, R, Cc), K in zip(spans, Ks):
-                self.regions.append((r0, c0, R, Cc, sp, K))
+                self.regions.append((r0, c0, R, Cc, sp, sp_dev, K))
                 covered += R * Cc
         if covered != n * n:
             raise ValueError("the blocks of this layout do not cover the covariance matrix")
@@ -484,12 +485,14 @@ class SignalBasis:
         used = None
         if not torch.cuda.is_current_stream_capturing():
             used = (cl.abs().amax(dim=(0, 2)) > 0).cpu().numpy()
-        for r0, c0, R, Cc, sp, K in self.regions:
+        for r0, c0, R, Cc, sp, sp_dev, K in self.regions:
             keep = len(sp)
             while used is not None and keep > 0 and not used[sp[keep - 1]]:
                 keep -= 1
             kd = 1 + keep * Lp
-            ctab = torch.cat([s[:, None], cl[:, sp[:keep], :].reshape(B, keep * Lp)], dim=1).contiguous()
+            # spectra picked with a device index (no host-to-device copy: capturable)
+            ctab = torch.cat([s[:, None], cl.index_select(1, sp_dev[:keep]).reshape(B, keep * Lp)],
+                             dim=1).contiguous()
             check(self.E.lib.cf_dgemm(0, 0, B, Cc, kd, 1.0, ctab.data_ptr(), kd, 0, K.data_ptr(), R * Cc, Cc,
                                       0.0, _off(out, r0 * n + c0), n * n, n, None, 0, 0, R, 0, stream()),
                   "cf_dgemm")

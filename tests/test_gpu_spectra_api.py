@@ -1,6 +1,6 @@
 """The Spectra drop-in's methods beyond run() (qube/spectra.py:1206-2240).
 
-* ``compute()`` after ``setup()`` gives exactly what ``run()`` gives;
+* ``compute()`` after ``setup()`` gives what ``run()`` gives (to rounding: atomics);
 * ``convolve_theory_for_inference`` is W_bp C_l with the reference's own
   bandpower window (fixture ``bandpower_*``: the window
   ``get_bandpower_window_function`` returned in the reference run), for every
@@ -43,10 +43,12 @@ def runs(request):
 
 
 def test_compute_after_setup_equals_run(runs):
+    """Same kernels on the same inputs; the build-and-reduce kernel adds its
+    per-block partial sums with atomics, so the two agree to rounding."""
     _, _, _, s1, s2 = runs
-    assert np.array_equal(s1.get_power_spectra(), s2.get_power_spectra())
-    assert np.array_equal(s1.get_noise_bias(), s2.get_noise_bias())
-    assert np.array_equal(s1.qml_results, s2.qml_results)
+    assert _rel(s2.get_power_spectra(), s1.get_power_spectra()) <= 1e-13
+    assert _rel(s2.get_noise_bias(), s1.get_noise_bias()) <= 1e-13
+    assert _rel(s2.qml_results, s1.qml_results) <= 1e-13
 
 
 def test_convolve_theory_for_inference_all_input_forms(runs):
