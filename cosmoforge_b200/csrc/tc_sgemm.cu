@@ -12,14 +12,15 @@
 // Both operands are K-contiguous ("NT"), as the blocked Cholesky's panel
 // solves and trailing updates use them; batch on blockIdx.z.
 //
-// One 128 x BN output tile per CTA (128 threads).  K runs in chunks of 64
+// One 128 x BN output tile per CTA (256 threads).  K runs in chunks of 64
 // (one 128-byte BF16 row per operand row and plane): every thread loads its
 // share of the chunk from global memory, splits it and stores the planes in
 // the 128-byte swizzled K-major layout the MMA descriptors describe; thread 0
 // issues the 24 MMAs of the chunk and commits them to the stage's mbarrier.
-// Two stages: the loads and splits of chunk c + 1 overlap the MMAs of chunk
-// c.  The epilogue reads both accumulators with tcgen05.ld (thread = output
-// row) and writes alpha (acc0 + acc1) + beta C.  Every barrier wait is
+// One stage (two CTAs per SM, one CTA's loads overlapping the other's MMAs)
+// or two (the loads and splits of chunk c + 1 overlap the MMAs of chunk c).  The epilogue reads both accumulators with tcgen05.ld (thread = output
+// row), turns each warp's 32 x 32 pieces around in shared memory and writes
+// alpha (acc0 + acc1) + beta C in coalesced row segments.  Every barrier wait is
 // bounded; a wait that runs out makes the CTA drain its MMAs, free its TMEM
 // and set info[z] = -3.
 #include <cuda_bf16.h>
@@ -28,7 +29,7 @@
 
 namespace {
 
-constexpr int BM = 128, KC = 64, NT = 128, PLANES = 3;
+constexpr int BM = 128, KC = 64, NT = 256, PLANES = 3;
 constexpr uint32_t A_BYTES = BM * KC * 2;  // one BF16 plane of the A chunk (16 KB)
 constexpr unsigned long long DRAIN_NS = 2000000000ull;
 
@@ -169,8 +170,8 @@ __device__ __forceinline__ void stage_operand(const float* X, long ld, int r0, i
     }
 }
 
-template <int BN>
-__global__ void __launch_bounds__(NT, 1) k_sgemm_bf16x6(int M, int N, int K, float alpha, const float* A, long lda,
+template <int BN, int STAGES>
+__global__ void __launch_bounds__(NT, STAGES == 1 ? 2 : 1) k_sgemm_bf16x6(int M, int N, int K, float alpha, const float* A, long lda,
                                                         long sA, const float* B, long ldb, long sB, float beta, float* C,
                                                         long ldc, long sC, int lower_only, unsigned long long wait_ns,
                                                         int* info)
@@ -211,11 +212,11 @@ __global__ void __launch_bounds__(NT, 1) k_sgemm_bf16x6(int M, int N, int K, flo
     const int nch = (K + KC - 1) / KC;
     bool aborted = false;
     for (int c = 0; c < nch; ++c) {
-        const int s = c & 1;
+        const int s = c % STAGES;
         uint8_t* sa = smem + s * STAGE;  // A planes 0, 1, 2, then B planes 0, 1, 2
         uint8_t* sb = sa + PLANES * A_BYTES;
-        // the MMAs of chunk c - 2 read this stage: wait for them before overwriting it
-        bool ok = c < 2 || mbar_wait(&done[s], (uint32_t)(((c - 2) >> 1) & 1), wait_ns);
+        // the MMAs of chunk c - STAGES read this stage: wait for them before overwriting it
+        bool ok = c < STAGES || mbar_wait(&done[s], (uint32_t)(((c - STAGES) / STAGES) & 1), wait_ns);
         if (__syncthreads_or(!ok)) {
             aborted = true;
             break;
@@ -244,7 +245,7 @@ __global__ void __launch_bounds__(NT, 1) k_sgemm_bf16x6(int M, int N, int K, flo
     bool ok = !aborted;
     if (ok && nch > 0) {
         const int cl = nch - 1;
-        ok = mbar_wait(&done[cl & 1], (uint32_t)((cl >> 1) & 1), wait_ns);
+        ok = mbar_wait(&done[cl % STAGES], (uint32_t)((cl / STAGES) & 1), wait_ns);
     }
     if (__syncthreads_or(!ok)) {
         // drain: every MMA issued has completed before TMEM is freed
@@ -256,25 +257,34 @@ __global__ void __launch_bounds__(NT, 1) k_sgemm_bf16x6(int M, int N, int K, flo
         }
         if (tid == 0 && info) atomicCAS(info + z, 0, CF_ERR_TIMEOUT);
     } else if (nch > 0) {
+        // Thread = output row in TMEM; each warp turns its 32 x 32 pieces around
+        // in shared memory (the operand stages are free now: every MMA has
+        // completed) so that C is read and written in 128-byte row segments.
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-        const int row = tile_m + warp * 32 + lane;
-        const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
-#pragma unroll
-        for (int g = 0; g < BN / 32; ++g) {
+        const int quad = warp & 3;  // a warp reads TMEM lanes 32 (warp % 4) .. + 31
+        const uint32_t lane_addr = tmem + ((uint32_t)(quad * 32) << 16);
+        float* T = reinterpret_cast<float*>(smem) + warp * 32 * 33;
+        const int col = lane;
+#pragma unroll 1
+        for (int g = warp >> 2; g < BN / 32; g += NT / 128) {  // the two warps of a quadrant split the columns
             uint32_t v[32], w[32];
             tmem_ld32(lane_addr + (uint32_t)(g * 32), v);
             tmem_ld32(lane_addr + (uint32_t)(BN + g * 32), w);
-            if (row < M) {
-                float* pc = C + (long)row * ldc + tile_n + g * 32;
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    if (tile_n + g * 32 + j < N) {
-                        float out = alpha * (__uint_as_float(v[j]) + __uint_as_float(w[j]));
-                        if (beta != 0.0f) out += beta * pc[j];
-                        pc[j] = out;
-                    }
+            for (int j = 0; j < 32; ++j) T[lane * 33 + j] = __uint_as_float(v[j]) + __uint_as_float(w[j]);
+            __syncwarp();
+            const int c = tile_n + g * 32 + col;
+#pragma unroll 4
+            for (int r = 0; r < 32; ++r) {
+                const int row = tile_m + quad * 32 + r;
+                if (row < M && c < N) {
+                    float* pc = C + (long)row * ldc + c;
+                    float out = alpha * T[r * 33 + col];
+                    if (beta != 0.0f) out += beta * *pc;
+                    *pc = out;
                 }
             }
+            __syncwarp();
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -285,18 +295,21 @@ __global__ void __launch_bounds__(NT, 1) k_sgemm_bf16x6(int M, int N, int K, flo
 }
 
 unsigned long long g_sgemm_wait_ns = DRAIN_NS;
+// Operand stages: 2 (double buffer, one CTA per SM) or 1 (two CTAs per SM
+// overlap each other's loads and MMAs).
+int g_sgemm_stages = 1;
 
-template <int BN>
+template <int BN, int STAGES>
 int launch(int M, int N, int K, float alpha, const float* A, long lda, long sA, const float* B, long ldb, long sB,
            float beta, float* C, long ldc, long sC, int batch, int lower_only, int* info, cudaStream_t st)
 {
-    constexpr size_t smem = 1024 + 2 * (size_t)PLANES * (A_BYTES + (size_t)BN * KC * 2);
+    constexpr size_t smem = 1024 + STAGES * (size_t)PLANES * (A_BYTES + (size_t)BN * KC * 2);
     static_assert(smem <= 232448, "shared memory exceeds 227 KB");
     static std::atomic<int> attr[CF_MAX_DEVICES];
-    if (int rc = cf_smem_optin(k_sgemm_bf16x6<BN>, (int)smem, attr)) return rc;
+    if (int rc = cf_smem_optin(k_sgemm_bf16x6<BN, STAGES>, (int)smem, attr)) return rc;
     dim3 grid(cf_cdiv(N, BN), cf_cdiv(M, BM), batch);
-    k_sgemm_bf16x6<BN><<<grid, NT, smem, st>>>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, lower_only,
-                                               g_sgemm_wait_ns, info);
+    k_sgemm_bf16x6<BN, STAGES><<<grid, NT, smem, st>>>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC,
+                                                       lower_only, g_sgemm_wait_ns, info);
     CF_CHECK_LAUNCH();
     return CF_OK;
 }
@@ -315,9 +328,23 @@ extern "C" int cf_sgemm_bf16x6(int M, int N, int K, float alpha, const float* A,
     if (M < 0 || N < 0 || K < 0 || batch < 1 || !C || (K > 0 && (!A || !B))) return CF_ERR_ARG;
     if (M == 0 || N == 0) return CF_OK;
     cudaStream_t st = (cudaStream_t)stream;
+    if (g_sgemm_stages == 2) {
+        if (N <= 64)
+            return launch<64, 2>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower_only, info, st);
+        return launch<128, 2>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower_only, info, st);
+    }
     if (N <= 64)
-        return launch<64>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower_only, info, st);
-    return launch<128>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower_only, info, st);
+        return launch<64, 1>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower_only, info, st);
+    return launch<128, 1>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower_only, info, st);
+}
+
+// Operand stages of cf_sgemm_bf16x6: 1 (default; two CTAs per SM) or 2 (one
+// CTA per SM, double-buffered).  Returns the previous setting.
+extern "C" int cf_sgemm_bf16x6_set_stages(int stages)
+{
+    const int prev = g_sgemm_stages;
+    if (stages == 1 || stages == 2) g_sgemm_stages = stages;
+    return prev;
 }
 
 // Bound of the barrier waits of cf_sgemm_bf16x6, in ns (ns < 0: the default

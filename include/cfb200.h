@@ -338,6 +338,11 @@ int cf_sgemm_bf16x6(int M, int N, int K, float alpha, const float* A, long lda, 
  * No counterpart in the reference. */
 long long cf_sgemm_bf16x6_set_wait_limit(long long ns);
 
+/* Operand stages of cf_sgemm_bf16x6: 1 (default: two CTAs per SM) or 2 (one
+ * CTA per SM, double-buffered).  Returns the previous setting.
+ * No counterpart in the reference. */
+int cf_sgemm_bf16x6_set_stages(int stages);
+
 /* Product kernel of cf_potrf_f32: 1 = cf_sgemm_bf16x6 on the tensor cores
  * (default), 0 = an FP32 SIMT kernel.  Returns the previous setting.
  * No counterpart in the reference. */

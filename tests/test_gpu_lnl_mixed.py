@@ -161,24 +161,30 @@ def test_sgemm_bf16x6_matches_fp64_product(M, N, K, batch, lower):
     A = torch.randn((batch, M, K), device="cuda", generator=g)
     B = A if lower else torch.randn((batch, N, K), device="cuda", generator=g)
     C0 = torch.randn((batch, M, N), device="cuda", generator=g)
-    C = C0.clone()
-    info = torch.zeros(batch, dtype=torch.int32, device="cuda")
-    rc = lib.cf_sgemm_bf16x6(M, N, K, -1.0, A.data_ptr(), K, M * K, B.data_ptr(), K, N * K, 0.5, C.data_ptr(), N, M * N,
-                             batch, lower, info.data_ptr(), torch.cuda.current_stream().cuda_stream)
-    assert rc == 0
-    torch.cuda.synchronize()
-    assert int(info.abs().max()) == 0
     ref = -torch.bmm(A.double(), B.double().transpose(1, 2)) + 0.5 * C0.double()
     scale = torch.bmm(A.double().abs(), B.double().abs().transpose(1, 2)).max()
-    if lower:  # tiles strictly above the diagonal are skipped: only rows >= the tile's columns are written
-        r = torch.arange(M, device="cuda")[:, None] // 128
-        c = torch.arange(N, device="cuda")[None, :] // 128
-        keep = (c <= r)[None]
-        err = ((C.double() - ref).abs() * keep).max()
-        assert bool((C[~keep.expand_as(C)] == C0[~keep.expand_as(C0)]).all())
-    else:
-        err = (C.double() - ref).abs().max()
-    assert float(err / scale) <= 2e-6, float(err / scale)
+    prev = lib.cf_sgemm_bf16x6_set_stages(1)
+    try:
+        for stages in (1, 2):
+            lib.cf_sgemm_bf16x6_set_stages(stages)
+            C = C0.clone()
+            info = torch.zeros(batch, dtype=torch.int32, device="cuda")
+            rc = lib.cf_sgemm_bf16x6(M, N, K, -1.0, A.data_ptr(), K, M * K, B.data_ptr(), K, N * K, 0.5, C.data_ptr(),
+                                     N, M * N, batch, lower, info.data_ptr(), torch.cuda.current_stream().cuda_stream)
+            assert rc == 0
+            torch.cuda.synchronize()
+            assert int(info.abs().max()) == 0
+            if lower:  # tiles strictly above the diagonal are skipped: only rows >= the tile's columns are written
+                r = torch.arange(M, device="cuda")[:, None] // 128
+                c = torch.arange(N, device="cuda")[None, :] // 128
+                keep = (c <= r)[None]
+                err = ((C.double() - ref).abs() * keep).max()
+                assert bool((C[~keep.expand_as(C)] == C0[~keep.expand_as(C0)]).all())
+            else:
+                err = (C.double() - ref).abs().max()
+            assert float(err / scale) <= 2e-6, (stages, float(err / scale))
+    finally:
+        lib.cf_sgemm_bf16x6_set_stages(prev)
 
 
 def test_sgemm_bf16x6_timed_out_wait_sets_info():
