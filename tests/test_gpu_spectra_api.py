@@ -44,11 +44,12 @@ def runs(request):
 
 def test_compute_after_setup_equals_run(runs):
     """Same kernels on the same inputs; the build-and-reduce kernel adds its
-    per-block partial sums with atomics, so the two agree to rounding."""
+    per-block partial sums with atomics, so the two agree to rounding (q to
+    1e-13; C_hat through F^-1 to the parity bar, 1e-10)."""
     _, _, _, s1, s2 = runs
-    assert _rel(s2.get_power_spectra(), s1.get_power_spectra()) <= 1e-13
-    assert _rel(s2.get_noise_bias(), s1.get_noise_bias()) <= 1e-13
     assert _rel(s2.qml_results, s1.qml_results) <= 1e-13
+    assert _rel(s2.get_power_spectra(), s1.get_power_spectra()) <= 1e-10
+    assert _rel(s2.get_noise_bias(), s1.get_noise_bias()) <= 1e-10
 
 
 def test_convolve_theory_for_inference_all_input_forms(runs):
