@@ -16,10 +16,14 @@
 // factor's first-order error.
 #include "cf_common.cuh"
 #include "potrf_diag.cuh"
+#include "tri_solve.cuh"
 
 extern "C" int cf_sgemm_bf16x6(int M, int N, int K, float alpha, const float* A, long lda, long sA, const float* B,
                                long ldb, long sB, float beta, float* C, long ldc, long sC, int batch, int lower_only,
                                int* info, void* stream);
+int cf_sgemm_bf16x6_dual(int M, int N, int K, float alpha, const float* A, long lda, long sA, const float* B,
+                         long ldb, long sB, float beta, float* C, long ldc, long sC, float* C2, long ldc2, long sC2,
+                         int batch, int lower_only, int* info, void* stream);
 
 namespace {
 
@@ -152,6 +156,24 @@ int sgemm_nt(int M, int N, int K, float alpha, const float* A, long lda, long sA
     return sgemm_nt_simt(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower_only, st);
 }
 
+__global__ void k_copy2d_f32(int R, int Ccols, const float* src, long lds, long ss, float* dst, long ldd, long sd);
+
+// Panel solve W = A21 Dinv^T (M x kb, K = kb) written to the work buffer W and
+// into the matrix at A21 itself: one pass with the tensor-core GEMM's second
+// destination, or the SIMT GEMM and a copy.
+int panel_nt(int M, int kb, float* a21, long lda, long sA, const float* D, long sD, float* W, long ldw, long sW,
+             int batch, int* info, cudaStream_t st)
+{
+    if (g_potrf_f32_tensor)
+        return cf_sgemm_bf16x6_dual(M, kb, kb, 1.0f, a21, lda, sA, D, kb, sD, 0.0f, W, ldw, sW, a21, lda, sA, batch, 0,
+                                    info, st);
+    int rc = sgemm_nt_simt(M, kb, kb, 1.0f, a21, lda, sA, D, kb, sD, 0.0f, W, ldw, sW, batch, 0, st);
+    if (rc) return rc;
+    k_copy2d_f32<<<dim3(cf_cdiv(kb, 32), cf_cdiv(M, 8), batch), dim3(32, 8), 0, st>>>(M, kb, W, ldw, sW, a21, lda, sA);
+    CF_CHECK_LAUNCH();
+    return CF_OK;
+}
+
 __global__ void k_copy2d_f32(int R, int Ccols, const float* src, long lds, long ss, float* dst, long ldd, long sd)
 {
     src += blockIdx.z * ss;
@@ -182,10 +204,17 @@ constexpr int CNT = 256;
 
 // One CTA per (problem b, map m): w = L^-1 x, v = L^-T w (FP64 arithmetic on
 // the FP32 factor, both vectors in shared memory), then
-// chi2 = 2 w.w - v^T C v with C read from its FP64 lower triangle.
-__global__ void __launch_bounds__(CNT) k_chi2_refined(int n, const float* L, long lda, long sL, const double* C,
-                                                      long ldc, long sC, const double* X, long ldx, long sX,
-                                                      int nrhs, double* chi2)
+// chi2 = 2 w.w - v^T C v with C read from its FP64 lower triangle.  Both
+// solves run over 32-row blocks (cf_tri): warp 0 solves the diagonal block,
+// then the CTA applies the block's 32-wide segments - forward, one row
+// segment of L per thread below the block; backward, one column of the block
+// row per thread to its left, while the threads on rows at or below the block
+// add that block's 32 columns of the lower triangle of C to v^T C v (every v
+// they need is final by then), so C is read once, in row segments.
+template <bool VL, bool VC>
+__global__ void __launch_bounds__(CNT, 2) k_chi2_refined(int n, const float* L, long lda, long sL, const double* C,
+                                                         long ldc, long sC, const double* X, long ldx, long sX,
+                                                         int nrhs, double* chi2)
 {
     extern __shared__ double sh[];
     double* w = sh;
@@ -198,79 +227,39 @@ __global__ void __launch_bounds__(CNT) k_chi2_refined(int n, const float* L, lon
     __shared__ double red[CNT / 32];
     for (int i = tid; i < n; i += CNT) w[i] = X[(long)i * ldx + m];
     __syncthreads();
-    // forward substitution, 32 rows per block
     for (int b0 = 0; b0 < n; b0 += 32) {
         const int kb = n - b0 < 32 ? n - b0 : 32;
-        if (warp == 0) {
-            // lane i holds row b0 + i of the diagonal block (independent loads)
-            float lrow[32];
-#pragma unroll
-            for (int k = 0; k < 32; ++k) lrow[k] = (lane < kb && k < kb) ? L[(long)(b0 + lane) * lda + b0 + k] : 1.0f;
-            double zi = lane < kb ? w[b0 + lane] : 0.0;
-#pragma unroll
-            for (int r = 0; r < 32; ++r) {
-                if (r < kb) {
-                    if (lane == r) zi /= (double)lrow[r];
-                    const double zr = __shfl_sync(0xffffffffu, zi, r);
-                    if (lane > r) zi -= (double)lrow[r] * zr;
-                }
-            }
-            if (lane < kb) w[b0 + lane] = zi;
-        }
+        if (warp == 0) cf_tri::diag_forward(L, lda, b0, kb, w, lane);
         __syncthreads();
-        // rows below: 8 coalesced row loads in flight per warp, then the reductions
-        const double zl = lane < kb ? w[b0 + lane] : 0.0;
-        for (int r0 = b0 + kb + warp * 8; r0 < n; r0 += (CNT / 32) * 8) {
-            double t[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i)
-                t[i] = (r0 + i < n && lane < kb) ? (double)L[(long)(r0 + i) * lda + b0 + lane] * zl : 0.0;
-#pragma unroll
-            for (int i = 0; i < 8; ++i)
-                for (int o = 16; o; o >>= 1) t[i] += __shfl_xor_sync(0xffffffffu, t[i], o);
-            if (lane == 0)
-#pragma unroll
-                for (int i = 0; i < 8; ++i)
-                    if (r0 + i < n) w[r0 + i] -= t[i];
-        }
+        for (int r = b0 + kb + tid; r < n; r += CNT) w[r] -= cf_tri::seg_dot<VL>(L + (long)r * lda + b0, w + b0, kb);
         __syncthreads();
     }
-    for (int i = tid; i < n; i += CNT) v[i] = w[i];
-    __syncthreads();
-    // back substitution L^T v = w, 32 rows per block from the bottom
-    const int nblk = (n + 31) / 32;
-    for (int blk = nblk - 1; blk >= 0; --blk) {
-        const int b0 = blk * 32;
-        const int kb = n - b0 < 32 ? n - b0 : 32;
-        if (warp == 0) {
-            double vi = lane < kb ? v[b0 + lane] : 0.0;
-            for (int r = kb - 1; r >= 0; --r) {
-                if (lane == r) vi /= (double)L[(long)(b0 + r) * lda + b0 + r];
-                const double vr = __shfl_sync(0xffffffffu, vi, r);
-                if (lane < r) vi -= (double)L[(long)(b0 + r) * lda + b0 + lane] * vr;
-            }
-            if (lane < kb) v[b0 + lane] = vi;
-        }
-        __syncthreads();
-        // rows above the block: v[i] -= sum_k L[b0 + k, i] v[b0 + k]
-        for (int i = tid; i < b0; i += CNT) {
-            double t = 0.0;
-            for (int k = 0; k < kb; ++k) t += (double)L[(long)(b0 + k) * lda + i] * v[b0 + k];
-            v[i] -= t;
-        }
-        __syncthreads();
-    }
-    // 2 w.w - v^T C v, C from its lower triangle
     double s = 0.0;
-    for (int i = tid; i < n; i += CNT) s += 2.0 * w[i] * w[i];
-    for (int r = warp; r < n; r += CNT / 32) {
-        const double* cr = C + (long)r * ldc;
-        double t = 0.0;
-        for (int c = lane; c < r; c += 32) t += cr[c] * v[c];
-        t = 2.0 * t;
-        if (lane == 0) t += cr[r] * v[r];
-        s -= t * v[r];
+    for (int i = tid; i < n; i += CNT) {
+        v[i] = w[i];
+        s += 2.0 * w[i] * w[i];
     }
+    __syncthreads();
+    double qf = 0.0;  // this thread's share of v^T C v
+    for (int b0 = ((n - 1) / 32) * 32; b0 >= 0; b0 -= 32) {
+        const int kb = n - b0 < 32 ? n - b0 : 32;
+        if (warp == 0) cf_tri::diag_backward(L, lda, b0, kb, v, lane);
+        __syncthreads();
+        for (int q = tid; q < n; q += CNT) {
+            if (q < b0) {
+                v[q] -= cf_tri::col_dot(L, lda, b0, q, v + b0, kb);
+            } else if (q >= b0 + kb) {
+                qf += 2.0 * v[q] * cf_tri::seg_dot<VC>(C + (long)q * ldc + b0, v + b0, kb);
+            } else {
+                const double* cr = C + (long)q * ldc;
+                double t = cr[q] * v[q];
+                for (int c = b0; c < q; ++c) t += 2.0 * cr[c] * v[c];
+                qf += v[q] * t;
+            }
+        }
+        __syncthreads();
+    }
+    s -= qf;
     for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) red[warp] = s;
     __syncthreads();
@@ -337,14 +326,11 @@ extern "C" int cf_potrf_f32(int n, float* A, long lda, long strideA, int batch, 
         const int rest1 = n - k0 - kb1;
         if (rest1 <= 0) break;
         float* a21_1 = A + (long)(k0 + kb1) * lda + k0;
-        int rc = sgemm_nt(rest1, kb1, kb1, 1.0f, a21_1, lda, strideA, D1, kb1, ws, 0.0f, W, LDW, ws, batch, 0, info, st);
+        int rc = panel_nt(rest1, kb1, a21_1, lda, strideA, D1, ws, W, LDW, ws, batch, info, st);
         if (rc) return rc;
         const int kb2 = rest1 < NB ? rest1 : NB;
         rc = sgemm_nt(rest1, kb2, kb1, -1.0f, W, LDW, ws, W, LDW, ws, 1.0f, a21_1 + kb1, lda, strideA, batch, 0, info, st);
         if (rc) return rc;
-        k_copy2d_f32<<<dim3(cf_cdiv(kb1, 32), cf_cdiv(rest1, 8), batch), dim3(32, 8), 0, st>>>(rest1, kb1, W, LDW, ws,
-                                                                                              a21_1, lda, strideA);
-        CF_CHECK_LAUNCH();
         const int k1 = k0 + kb1;
         k_potrf_diag_inv<float><<<batch, cf_diag::NTHREADS, cf_diag::smem_bytes<float>(), st>>>(A, lda, strideA, k1, kb2, D2, ws, info);
         CF_CHECK_LAUNCH();
@@ -352,14 +338,11 @@ extern "C" int cf_potrf_f32(int n, float* A, long lda, long strideA, int batch, 
         if (rest2 <= 0) break;
         float* a21_2 = A + (long)(k1 + kb2) * lda + k1;
         float* W2 = W + (long)kb2 * LDW;
-        rc = sgemm_nt(rest2, kb2, kb2, 1.0f, a21_2, lda, strideA, D2, kb2, ws, 0.0f, W2 + kb1, LDW, ws, batch, 0, info, st);
+        rc = panel_nt(rest2, kb2, a21_2, lda, strideA, D2, ws, W2 + kb1, LDW, ws, batch, info, st);
         if (rc) return rc;
         rc = sgemm_nt(rest2, rest2, kb1 + kb2, -1.0f, W2, LDW, ws, W2, LDW, ws, 1.0f, a21_2 + kb2, lda, strideA, batch,
                       1, info, st);
         if (rc) return rc;
-        k_copy2d_f32<<<dim3(cf_cdiv(kb2, 32), cf_cdiv(rest2, 8), batch), dim3(32, 8), 0, st>>>(
-            rest2, kb2, W2 + kb1, LDW, ws, a21_2, lda, strideA);
-        CF_CHECK_LAUNCH();
     }
     return CF_OK;
 }
@@ -395,11 +378,14 @@ extern "C" int cf_chi2_logdet_mixed(int n, const float* L, long lda, long stride
     if (nrhs > 0) {
         if (!X || !C || !chi2) return CF_ERR_ARG;
         const size_t smem = 2 * (size_t)n * sizeof(double);
-        static std::atomic<int> attr[CF_MAX_DEVICES];
-        int rc = cf_smem_optin(k_chi2_refined, 2 * 12288 * (int)sizeof(double), attr);
+        const bool vl = ((uintptr_t)L & 15) == 0 && (lda & 3) == 0 && (batch == 1 || (strideL & 3) == 0);
+        const bool vc = ((uintptr_t)C & 15) == 0 && (ldc & 1) == 0 && (batch == 1 || (strideC & 1) == 0);
+        auto kern = vl ? (vc ? k_chi2_refined<true, true> : k_chi2_refined<true, false>)
+                       : (vc ? k_chi2_refined<false, true> : k_chi2_refined<false, false>);
+        static std::atomic<int> attr[4][CF_MAX_DEVICES];
+        int rc = cf_smem_optin(kern, 2 * 12288 * (int)sizeof(double), attr[2 * vl + vc]);
         if (rc) return rc;
-        k_chi2_refined<<<batch * nrhs, CNT, smem, st>>>(n, L, lda, strideL, C, ldc, strideC, X, ldx, strideX, nrhs,
-                                                       chi2);
+        kern<<<batch * nrhs, CNT, smem, st>>>(n, L, lda, strideL, C, ldc, strideC, X, ldx, strideX, nrhs, chi2);
         CF_CHECK_LAUNCH();
     }
     if (logdet) {

@@ -80,16 +80,119 @@ inline int nblocks(int n) { return (n + NB - 1) / NB; }
 // doubles of potrf workspace per problem: every diagonal-block inverse + one
 // double-width panel (two 64-column panels side by side)
 inline size_t potrf_ws(int n) { return (size_t)nblocks(n) * NB * NB + (size_t)n * 2 * NB; }
+// A single matrix above this order is factored with a look-ahead (a second
+// panel buffer, the bulk of each trailing update on a second stream).
+constexpr int LOOKAHEAD_MIN_N = 1024;
+inline bool use_lookahead(int n, int batch) { return batch == 1 && n > LOOKAHEAD_MIN_N; }
+inline size_t potrf_ws_total(int n, int batch)
+{
+    return potrf_ws(n) * (size_t)batch + (use_lookahead(n, batch) ? (size_t)n * 2 * NB : 0);
+}
+
+// Per-device side stream (highest priority: it carries the factorisation's
+// critical path) and the events of the look-ahead fork / join.  The mutex
+// keeps one caller's event records from interleaving with another's.
+struct Lookahead {
+    std::mutex mu;
+    bool ready = false;
+    cudaStream_t chain = nullptr;
+    cudaEvent_t fork = nullptr, panel = nullptr, bulk = nullptr, join = nullptr;
+};
+Lookahead g_la[CF_MAX_DEVICES];
+
+int lookahead_state(Lookahead** out)
+{
+    int dev = -1;
+    CF_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= CF_MAX_DEVICES) return CF_ERR_UNSUPPORTED;
+    Lookahead& la = g_la[dev];
+    *out = &la;
+    return CF_OK;
+}
+
+int lookahead_init(Lookahead& la)
+{
+    if (la.ready) return CF_OK;
+    int least = 0, greatest = 0;
+    CF_CHECK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    CF_CHECK(cudaStreamCreateWithPriority(&la.chain, cudaStreamNonBlocking, greatest));
+    for (cudaEvent_t* e : {&la.fork, &la.panel, &la.bulk, &la.join})
+        CF_CHECK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    la.ready = true;
+    return CF_OK;
+}
 }  // namespace
 
-extern "C" size_t cf_potrf_workspace(int n, int batch) { return potrf_ws(n) * sizeof(double) * (size_t)batch; }
+extern "C" size_t cf_potrf_workspace(int n, int batch) { return potrf_ws_total(n, batch) * sizeof(double); }
+
+namespace {
+// One 128-column step of the factorisation up to the trailing update: factor
+// the two diagonal blocks (keeping their inverses), solve both panels into W
+// and write them back.  Returns the K = 128 panel W2 the trailing update
+// A22 -= W2 W2^T needs through *w2 (nullptr when no trailing matrix is left).
+int potrf_step(int n, int k0, double* A, long lda, long strideA, int batch, double* Dinv, int blk, double* W,
+               long ws, int* info, cudaStream_t st, const double** w2, int* rest2_out)
+{
+    constexpr size_t DIAG_SMEM = cf_diag::smem_bytes<double>();
+    constexpr int LDW = 2 * NB;
+    void* stream = (void*)st;
+    *w2 = nullptr;
+    *rest2_out = 0;
+    const int kb1 = n - k0 < NB ? n - k0 : NB;
+    double* D1 = Dinv + (long)blk * NB * NB;
+    k_potrf_diag_inv<double><<<batch, cf_diag::NTHREADS, DIAG_SMEM, st>>>(A, lda, strideA, k0, kb1, D1, ws, info);
+    CF_CHECK_LAUNCH();
+    const int rest1 = n - k0 - kb1;
+    if (rest1 <= 0) return CF_OK;
+    double* a21_1 = A + (long)(k0 + kb1) * lda + k0;
+    // T1 = A21 L11^-T into W[:, 0:kb1]
+    int rc = cf_dgemm(0, 1, rest1, kb1, kb1, 1.0, a21_1, lda, strideA, D1, kb1, ws, 0.0, W, LDW, ws, nullptr, 0, 0,
+                      batch, 0, stream);
+    if (rc) return rc;
+    const int kb2 = rest1 < NB ? rest1 : NB;
+    // panel 2's columns, every row below panel 1: A -= T1 T1[0:kb2]^T
+    rc = cf_dgemm(0, 1, rest1, kb2, kb1, -1.0, W, LDW, ws, W, LDW, ws, 1.0, a21_1 + kb1, lda, strideA, nullptr, 0, 0,
+                  batch, 0, stream);
+    if (rc) return rc;
+    k_copy2d<<<dim3(cf_cdiv(kb1, 32), cf_cdiv(rest1, 8), batch), dim3(32, 8), 0, st>>>(rest1, kb1, W, LDW, ws, a21_1,
+                                                                                      lda, strideA);
+    CF_CHECK_LAUNCH();
+    const int k1 = k0 + kb1;
+    double* D2 = Dinv + (long)(blk + 1) * NB * NB;
+    k_potrf_diag_inv<double><<<batch, cf_diag::NTHREADS, DIAG_SMEM, st>>>(A, lda, strideA, k1, kb2, D2, ws, info);
+    CF_CHECK_LAUNCH();
+    const int rest2 = rest1 - kb2;
+    if (rest2 <= 0) return CF_OK;
+    double* a21_2 = A + (long)(k1 + kb2) * lda + k1;
+    double* W2 = W + (long)kb2 * LDW;  // rows of W at and below the trailing matrix
+    // T2 = A21_2 L22^-T into W[kb2:, kb1:kb1+kb2]
+    rc = cf_dgemm(0, 1, rest2, kb2, kb2, 1.0, a21_2, lda, strideA, D2, kb2, ws, 0.0, W2 + kb1, LDW, ws, nullptr, 0, 0,
+                  batch, 0, stream);
+    if (rc) return rc;
+    k_copy2d<<<dim3(cf_cdiv(kb2, 32), cf_cdiv(rest2, 8), batch), dim3(32, 8), 0, st>>>(rest2, kb2, W2 + kb1, LDW, ws,
+                                                                                      a21_2, lda, strideA);
+    CF_CHECK_LAUNCH();
+    *w2 = W2;
+    *rest2_out = rest2;
+    return CF_OK;
+}
+}  // namespace
 
 // Right-looking blocked Cholesky: per 64-wide panel, the diagonal block is
 // factored (and inverted) by one CTA and the panel below is L21 = A21 L11^-T
-// (DMMA GEMM against the inverted block); panels go in pairs with a
-// look-ahead so that the trailing update A22 -= L21 L21^T (lower-only DMMA
-// GEMM) runs once per 128 columns.  `work` holds cf_potrf_workspace(n, batch)
-// bytes and keeps every L11^-1 for cf_trtri_lower.
+// (DMMA GEMM against the inverted block); panels go in pairs so that the
+// trailing update A22 -= L21 L21^T (lower-only DMMA GEMM) runs once per 128
+// columns.  `work` holds cf_potrf_workspace(n, batch) bytes and keeps every
+// L11^-1 for cf_trtri_lower.
+//
+// A single matrix of order above 1024 is factored with a look-ahead: the
+// next step's 128 columns of each trailing update go first, on a
+// high-priority side stream that carries the whole critical path (diagonal
+// blocks, panels, those columns), while the rest of the update (the bulk of
+// the FLOPs) runs on the caller's stream; two panel buffers alternate so a
+// step's panels never overwrite the ones the previous bulk update still
+// reads.  The side stream forks from and joins the caller's stream through
+// events, so the routine stays stream-ordered and capturable.
 extern "C" int cf_potrf(int n, double* A, long lda, long strideA, int batch, void* work, int* info, void* stream)
 {
     if (n <= 0 || batch < 1 || !A || !work) return CF_ERR_ARG;
@@ -101,55 +204,75 @@ extern "C" int cf_potrf(int n, double* A, long lda, long strideA, int batch, voi
     double* Dinv = (double*)work;                   // [batch][nblocks][NB][NB]
     double* W = Dinv + (long)nblocks(n) * NB * NB;  // [batch][n][2 NB] (same stride ws)
     constexpr int LDW = 2 * NB;
-    // Two 64-column panels per pass (look-ahead): factor panel 1, update only
-    // panel 2's columns with it, factor panel 2, then one trailing update of
-    // K = 128 with both, so the trailing matrix is read and written once per
-    // 128 columns.
-    int blk = 0;
-    for (int k0 = 0; k0 < n; k0 += 2 * NB) {
-        const int kb1 = n - k0 < NB ? n - k0 : NB;
-        k_potrf_diag_inv<double><<<batch, cf_diag::NTHREADS, DIAG_SMEM, st>>>(A, lda, strideA, k0, kb1, Dinv + (long)blk * NB * NB, ws,
-                                                        info);
-        CF_CHECK_LAUNCH();
-        const double* D1 = Dinv + (long)blk * NB * NB;
-        ++blk;
-        const int rest1 = n - k0 - kb1;
-        if (rest1 <= 0) break;
-        double* a21_1 = A + (long)(k0 + kb1) * lda + k0;
-        // T1 = A21 L11^-T into W[:, 0:kb1]
-        int rc = cf_dgemm(0, 1, rest1, kb1, kb1, 1.0, a21_1, lda, strideA, D1, kb1, ws, 0.0, W, LDW, ws, nullptr, 0,
-                          0, batch, 0, stream);
-        if (rc) return rc;
-        const int kb2 = rest1 < NB ? rest1 : NB;
-        // panel 2's columns, every row below panel 1: A -= T1 T1[0:kb2]^T
-        rc = cf_dgemm(0, 1, rest1, kb2, kb1, -1.0, W, LDW, ws, W, LDW, ws, 1.0, a21_1 + kb1, lda, strideA, nullptr,
-                      0, 0, batch, 0, stream);
-        if (rc) return rc;
-        k_copy2d<<<dim3(cf_cdiv(kb1, 32), cf_cdiv(rest1, 8), batch), dim3(32, 8), 0, st>>>(rest1, kb1, W, LDW, ws,
-                                                                                          a21_1, lda, strideA);
-        CF_CHECK_LAUNCH();
-        const int k1 = k0 + kb1;
-        k_potrf_diag_inv<double><<<batch, cf_diag::NTHREADS, DIAG_SMEM, st>>>(A, lda, strideA, k1, kb2, Dinv + (long)blk * NB * NB, ws,
-                                                        info);
-        CF_CHECK_LAUNCH();
-        const double* D2 = Dinv + (long)blk * NB * NB;
-        ++blk;
-        const int rest2 = rest1 - kb2;
-        if (rest2 <= 0) break;
-        double* a21_2 = A + (long)(k1 + kb2) * lda + k1;
-        double* W2 = W + (long)kb2 * LDW;  // rows of W at and below the trailing matrix
-        // T2 = A21_2 L22^-T into W[kb2:, kb1:kb1+kb2]
-        rc = cf_dgemm(0, 1, rest2, kb2, kb2, 1.0, a21_2, lda, strideA, D2, kb2, ws, 0.0, W2 + kb1, LDW, ws, nullptr,
-                      0, 0, batch, 0, stream);
-        if (rc) return rc;
-        // trailing update with both panels (kb1 == NB here): A22 -= [T1 T2] [T1 T2]^T, lower tiles
-        rc = cf_dgemm(0, 1, rest2, rest2, kb1 + kb2, -1.0, W2, LDW, ws, W2, LDW, ws, 1.0, a21_2 + kb2, lda, strideA,
-                      nullptr, 0, 0, batch, 1, stream);
-        if (rc) return rc;
-        k_copy2d<<<dim3(cf_cdiv(kb2, 32), cf_cdiv(rest2, 8), batch), dim3(32, 8), 0, st>>>(rest2, kb2, W2 + kb1, LDW,
-                                                                                          ws, a21_2, lda, strideA);
-        CF_CHECK_LAUNCH();
+    if (!use_lookahead(n, batch)) {
+        int blk = 0;
+        for (int k0 = 0; k0 < n; k0 += 2 * NB, blk += 2) {
+            const double* W2 = nullptr;
+            int rest2 = 0;
+            int rc = potrf_step(n, k0, A, lda, strideA, batch, Dinv, blk, W, ws, info, st, &W2, &rest2);
+            if (rc) return rc;
+            if (!W2) break;
+            double* a22 = A + (long)(k0 + 2 * NB) * (lda + 1);
+            rc = cf_dgemm(0, 1, rest2, rest2, 2 * NB, -1.0, W2, LDW, ws, W2, LDW, ws, 1.0, a22, lda, strideA, nullptr,
+                          0, 0, batch, 1, stream);
+            if (rc) return rc;
+        }
+        return CF_OK;
     }
+    Lookahead* la = nullptr;
+    if (int rc = lookahead_state(&la)) return rc;
+    std::lock_guard<std::mutex> lock(la->mu);
+    if (int rc = lookahead_init(*la)) return rc;
+    cudaStream_t ch = la->chain;
+    double* Wbuf[2] = {W, W + (long)n * LDW};  // the second buffer follows the first problem's workspace
+    CF_CHECK(cudaEventRecord(la->fork, st));
+    CF_CHECK(cudaStreamWaitEvent(ch, la->fork, 0));
+    int rc = CF_OK;
+    bool bulk_pending = false;
+    int blk = 0;
+    for (int k0 = 0, it = 0; k0 < n && rc == CF_OK; k0 += 2 * NB, blk += 2, ++it) {
+        const double* W2 = nullptr;
+        int rest2 = 0;
+        rc = potrf_step(n, k0, A, lda, strideA, 1, Dinv, blk, Wbuf[it & 1], ws, info, ch, &W2, &rest2);
+        if (rc || !W2) break;
+        // every earlier update of the next step's columns is done before they are updated again
+        if (bulk_pending) {
+            if (cudaStreamWaitEvent(ch, la->bulk, 0) != cudaSuccess) {
+                rc = CF_ERR_CUDA;
+                break;
+            }
+        }
+        double* a22 = A + (long)(k0 + 2 * NB) * (lda + 1);
+        const int nn = rest2 < 2 * NB ? rest2 : 2 * NB;
+        // the next step's columns, every row below: critical path
+        rc = cf_dgemm(0, 1, rest2, nn, 2 * NB, -1.0, W2, LDW, 0, W2, LDW, 0, 1.0, a22, lda, 0, nullptr, 0, 0, 1, 1,
+                      (void*)ch);
+        if (rc) break;
+        const int rest3 = rest2 - nn;
+        if (rest3 > 0) {
+            // the rest of the trailing matrix on the caller's stream
+            if (cudaEventRecord(la->panel, ch) != cudaSuccess || cudaStreamWaitEvent(st, la->panel, 0) != cudaSuccess) {
+                rc = CF_ERR_CUDA;
+                break;
+            }
+            const double* w3 = W2 + (long)nn * LDW;
+            rc = cf_dgemm(0, 1, rest3, rest3, 2 * NB, -1.0, w3, LDW, 0, w3, LDW, 0, 1.0, a22 + (long)nn * (lda + 1),
+                          lda, 0, nullptr, 0, 0, 1, 1, stream);
+            if (rc) break;
+            if (cudaEventRecord(la->bulk, st) != cudaSuccess) {
+                rc = CF_ERR_CUDA;
+                break;
+            }
+            bulk_pending = true;
+        } else {
+            bulk_pending = false;
+        }
+    }
+    // join: the caller's stream waits for the side stream's last work (on every path)
+    const cudaError_t e1 = cudaEventRecord(la->join, ch);
+    const cudaError_t e2 = cudaStreamWaitEvent(st, la->join, 0);
+    if (rc) return rc;
+    if (e1 != cudaSuccess || e2 != cudaSuccess) return CF_ERR_CUDA;
     return CF_OK;
 }
 
@@ -245,7 +368,7 @@ extern "C" int cf_trtri_lower(int n, const double* L, long lda, long strideL, do
 
 extern "C" size_t cf_spd_inverse_workspace(int n, int batch)
 {
-    return ((size_t)n * n + (size_t)n + potrf_ws(n)) * sizeof(double) * (size_t)batch;
+    return (((size_t)n * n + (size_t)n) * (size_t)batch + potrf_ws_total(n, batch)) * sizeof(double);
 }
 
 // In place inverse of symmetric positive-definite matrices (row-major,

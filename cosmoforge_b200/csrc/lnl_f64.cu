@@ -5,60 +5,37 @@
 // log-determinant (picslike/picslike.py:643-664, cosmocore/basics/
 // linalg.py:430-474); both numbers follow from the one factor.
 //
-// One CTA per (problem, map): blocked forward substitution, 32 rows at a
-// time - warp 0 solves the 32 x 32 diagonal block with shuffles, then all
-// warps apply the panel to the rows below (one warp per row, coalesced reads
-// of L).
+// One CTA per (problem, map), z = L^-1 x in shared memory (global scratch for
+// n above the shared-memory limit).  Blocked forward substitution, 32 rows at a
+// time: warp 0 solves the 32 x 32 diagonal block (lane = row, registers and
+// shuffles, reciprocal pivots), then every thread takes one row below it and
+// subtracts its 32-column segment of L times the block's z (one 256-byte row
+// segment per thread, 16 loads in flight, no reductions).
 #include "cf_common.cuh"
+#include "tri_solve.cuh"
 
 namespace {
 
 constexpr int NT = 256;
+constexpr int SMEM_MAX_N = 24576;  // z in shared memory up to 192 KB
 
-__global__ void __launch_bounds__(NT) k_chi2(int n, const double* L, long lda, long sL, const double* X,
+template <bool VEC>
+__global__ void __launch_bounds__(NT, 2) k_chi2(int n, const double* L, long lda, long sL, const double* X,
                                              long ldx, long sX, int nrhs, double* z_work, double* chi2)
 {
+    extern __shared__ double zsh[];
     const int b = blockIdx.x / nrhs, m = blockIdx.x % nrhs;
     L += (long)b * sL;
     X += (long)b * sX;
-    double* z = z_work + (long)blockIdx.x * n;
+    double* z = z_work ? z_work + (long)blockIdx.x * n : zsh;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int i = tid; i < n; i += NT) z[i] = X[(long)i * ldx + m];
     __syncthreads();
     for (int b0 = 0; b0 < n; b0 += 32) {
         const int kb = n - b0 < 32 ? n - b0 : 32;
-        if (warp == 0) {
-            // lane i holds row b0 + i of the diagonal block (independent loads)
-            double lrow[32];
-#pragma unroll
-            for (int k = 0; k < 32; ++k) lrow[k] = (lane < kb && k < kb) ? L[(long)(b0 + lane) * lda + b0 + k] : 1.0;
-            double zi = lane < kb ? z[b0 + lane] : 0.0;
-#pragma unroll
-            for (int r = 0; r < 32; ++r) {
-                if (r < kb) {
-                    if (lane == r) zi /= lrow[r];
-                    const double zr = __shfl_sync(0xffffffffu, zi, r);
-                    if (lane > r) zi -= lrow[r] * zr;
-                }
-            }
-            if (lane < kb) z[b0 + lane] = zi;
-        }
+        if (warp == 0) cf_tri::diag_forward(L, lda, b0, kb, z, lane);
         __syncthreads();
-        // rows below: 8 coalesced row loads in flight per warp, then the reductions
-        const double zl = lane < kb ? z[b0 + lane] : 0.0;
-        for (int r0 = b0 + kb + warp * 8; r0 < n; r0 += (NT / 32) * 8) {
-            double v[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i)
-                v[i] = (r0 + i < n && lane < kb) ? L[(long)(r0 + i) * lda + b0 + lane] * zl : 0.0;
-#pragma unroll
-            for (int i = 0; i < 8; ++i)
-                for (int o = 16; o; o >>= 1) v[i] += __shfl_xor_sync(0xffffffffu, v[i], o);
-            if (lane == 0)
-#pragma unroll
-                for (int i = 0; i < 8; ++i)
-                    if (r0 + i < n) z[r0 + i] -= v[i];
-        }
+        for (int r = b0 + kb + tid; r < n; r += NT) z[r] -= cf_tri::seg_dot<VEC>(L + (long)r * lda + b0, z + b0, kb);
         __syncthreads();
     }
     double s = 0.0;
@@ -93,7 +70,7 @@ __global__ void __launch_bounds__(NT) k_logdet(int n, const double* L, long lda,
 }  // namespace
 
 // chi2[b * nrhs + m] = |L_b^-1 x_{b,m}|^2, logdet[b] = 2 sum ln (L_b)_ii.
-// z_work holds batch * nrhs * n doubles.  strideX = 0 shares X across the batch.
+// z_work holds batch * nrhs * n doubles (read only for n > 24576; may be NULL below).  strideX = 0 shares X across the batch.
 extern "C" int cf_chi2_logdet(int n, const double* L, long lda, long strideL, int batch, const double* X,
                               long ldx, long strideX, int nrhs, double* z_work, double* chi2,
                               double* logdet, void* stream)
@@ -101,8 +78,14 @@ extern "C" int cf_chi2_logdet(int n, const double* L, long lda, long strideL, in
     if (n <= 0 || batch < 1 || nrhs < 0 || !L) return CF_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     if (nrhs > 0) {
-        if (!X || !z_work || !chi2) return CF_ERR_ARG;
-        k_chi2<<<batch * nrhs, NT, 0, st>>>(n, L, lda, strideL, X, ldx, strideX, nrhs, z_work, chi2);
+        if (!X || !chi2 || (n > SMEM_MAX_N && !z_work)) return CF_ERR_ARG;
+        const bool vec = ((uintptr_t)L & 15) == 0 && (lda & 1) == 0 && (batch == 1 || (strideL & 1) == 0);
+        const bool sh = n <= SMEM_MAX_N;
+        const int smem = sh ? n * (int)sizeof(double) : 0;
+        auto kern = vec ? k_chi2<true> : k_chi2<false>;
+        static std::atomic<int> attr[2][CF_MAX_DEVICES];
+        if (int rc = cf_smem_optin(kern, SMEM_MAX_N * (int)sizeof(double), attr[vec])) return rc;
+        kern<<<batch * nrhs, NT, smem, st>>>(n, L, lda, strideL, X, ldx, strideX, nrhs, sh ? nullptr : z_work, chi2);
         CF_CHECK_LAUNCH();
     }
     if (logdet) {

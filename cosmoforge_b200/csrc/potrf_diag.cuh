@@ -4,8 +4,8 @@
 //
 // The block is factored right-looking in 16-column panels:
 //   (a) warp 0 factors the panel's 16 x 16 diagonal tile in registers (lane i
-//       holds row i; pivots are broadcast by shuffles, one square root and
-//       one reciprocal per column);
+//       holds row i; pivots are broadcast by shuffles, one reciprocal square
+//       root per column, l_kk = d rsqrt(d));
 //   (b) every row below the tile is solved against it by one thread
 //       (x_k = a_k / l_kk, then a_j -= x_k l_jk for the later columns j);
 //   (c) the trailing lower triangle takes the rank-16 update, 3 x 3 entries
@@ -13,7 +13,8 @@
 // Three barriers per panel instead of one per column.  The inverse X = L^-1 is
 // formed by 16-row block rows: each warp t inverts diagonal tile t by forward
 // substitution (lane c = column c), then block row I takes
-// X_I = T_I^-1 (-sum_{K<I} L_IK X_K) with T_I^-1 the tile inverse.
+// X_I = T_I^-1 (-sum_{K<I} L_IK X_K) with T_I^-1 the tile inverse (four
+// independent partial sums per dot product, to shorten the dependent chains).
 //
 // Per-problem status follows LAPACK: info = k0 + j + 1 for the first
 // non-positive (or NaN) pivot j of this block, left unchanged when the
@@ -48,13 +49,20 @@ __global__ void __launch_bounds__(NTHREADS) k_potrf_diag_inv(T* A, long lda, lon
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned FULL = 0xffffffffu;
 
-    // load the lower triangle (columns fastest: coalesced), zero the rest
+    // load the lower triangle (columns fastest: coalesced; every load in
+    // flight before the first store), zero the rest
     {
         const int c = tid & 63;
-        for (int r = tid >> 6; r < NB; r += NTHREADS / 64) {
-            T v = T(0);
-            if (r < kb && c <= r) v = A[(long)(k0 + r) * lda + k0 + c];
-            S[r * LDS + c] = v;
+        T v[NB / (NTHREADS / 64)];
+#pragma unroll
+        for (int i = 0; i < NB / (NTHREADS / 64); ++i) {
+            const int r = (tid >> 6) + i * (NTHREADS / 64);
+            v[i] = (r < kb && c <= r) ? A[(long)(k0 + r) * lda + k0 + c] : T(0);
+        }
+#pragma unroll
+        for (int i = 0; i < NB / (NTHREADS / 64); ++i) {
+            const int r = (tid >> 6) + i * (NTHREADS / 64);
+            S[r * LDS + c] = v[i];
             X[r * LDS + c] = T(0);
         }
     }
@@ -76,8 +84,8 @@ __global__ void __launch_bounds__(NTHREADS) k_potrf_diag_inv(T* A, long lda, lon
                         if (lane == 0 && bad == 0) bad = k0 + p + k + 1;
                         d = T(1);
                     }
-                    const T lkk = sqrt(d);
-                    const T rl = T(1) / lkk;
+                    const T rl = rsqrt(d);
+                    const T lkk = d * rl;
                     if (lane == k) r[k] = lkk;
                     else if (lane > k) r[k] *= rl;
                     if (lane == 0) rdg[p + k] = rl;
@@ -186,18 +194,28 @@ __global__ void __launch_bounds__(NTHREADS) k_potrf_diag_inv(T* A, long lda, lon
         const int rows = kb - I0 < PW ? kb - I0 : PW;
         for (int e = tid; e < PW * I0; e += NTHREADS) {
             const int r = e / I0, c = e - (e / I0) * I0;
-            T acc = T(0);
-            if (r < rows)
-                for (int mm = c; mm < I0; ++mm) acc -= S[(I0 + r) * LDS + mm] * X[mm * LDS + c];
-            Tb[r * NB + c] = acc;
+            T acc[4] = {T(0), T(0), T(0), T(0)};  // four independent chains over mm
+            if (r < rows) {
+                const T* lr = S + (I0 + r) * LDS;
+                int mm = c;
+                for (; mm + 3 < I0; mm += 4) {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) acc[u] -= lr[mm + u] * X[(mm + u) * LDS + c];
+                }
+                for (; mm < I0; ++mm) acc[0] -= lr[mm] * X[mm * LDS + c];
+            }
+            Tb[r * NB + c] = (acc[0] + acc[1]) + (acc[2] + acc[3]);
         }
         __syncthreads();
         for (int e = tid; e < PW * I0; e += NTHREADS) {
             const int r = e / I0, c = e - (e / I0) * I0;
             if (r < rows) {
-                T acc = T(0);
-                for (int j = 0; j <= r; ++j) acc += X[(I0 + r) * LDS + I0 + j] * Tb[j * NB + c];
-                X[(I0 + r) * LDS + c] = acc;
+                const T* xr = X + (I0 + r) * LDS + I0;
+                T acc[4] = {T(0), T(0), T(0), T(0)};
+#pragma unroll
+                for (int j = 0; j < PW; ++j)
+                    if (j <= r) acc[j & 3] += xr[j] * Tb[j * NB + c];
+                X[(I0 + r) * LDS + c] = (acc[0] + acc[1]) + (acc[2] + acc[3]);
             }
         }
         __syncthreads();

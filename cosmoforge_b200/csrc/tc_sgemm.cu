@@ -13,16 +13,18 @@
 // solves and trailing updates use them; batch on blockIdx.z.
 //
 // One 128 x BN output tile per CTA (256 threads).  K runs in chunks of 64
-// (one 128-byte BF16 row per operand row and plane): every thread loads its
-// share of the chunk from global memory, splits it and stores the planes in
-// the 128-byte swizzled K-major layout the MMA descriptors describe; thread 0
-// issues the 24 MMAs of the chunk and commits them to the stage's mbarrier.
-// One stage (two CTAs per SM, one CTA's loads overlapping the other's MMAs)
-// or two (the loads and splits of chunk c + 1 overlap the MMAs of chunk c).  The epilogue reads both accumulators with tcgen05.ld (thread = output
-// row), turns each warp's 32 x 32 pieces around in shared memory and writes
-// alpha (acc0 + acc1) + beta C in coalesced row segments.  Every barrier wait is
-// bounded; a wait that runs out makes the CTA drain its MMAs, free its TMEM
-// and set info[z] = -3.
+// (one 128-byte BF16 row per operand row and plane).  Every thread holds its
+// share of a chunk in registers (float4 loads, two 256-byte row segments per
+// warp), splits it and stores the planes in the 128-byte swizzled K-major
+// layout the MMA descriptors describe; thread 0 issues the 24 MMAs of the
+// chunk and commits them to the stage's mbarrier, and the threads go on to
+// load chunk c + 1 while those MMAs run.  One stage (two CTAs per SM) or two
+// (one CTA per SM).  The epilogue reads both accumulators with tcgen05.ld
+// (thread = output row), turns each warp's 32 x 32 pieces around in shared
+// memory and writes alpha (acc0 + acc1) + beta C in coalesced row segments;
+// a warp's 32 C segments are all in flight at once, the first piece's before
+// the last MMA wait.  Every barrier wait is bounded; a wait that runs out
+// makes the CTA drain its MMAs, free its TMEM and set info[z] = -3.
 #include <cuda_bf16.h>
 
 #include "cf_common.cuh"
@@ -139,42 +141,68 @@ __device__ __forceinline__ uint32_t swz(int r, int k)
     return (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + ((((k >> 3) ^ (r & 7)) << 4) | ((k & 7) << 1)));
 }
 
-// rows x 64 chunk of a K-contiguous FP32 operand (row r0.., column k0..) into
-// three BF16 planes `plane` bytes apart, in two passes of 32 columns.
-template <int ROWS>
-__device__ __forceinline__ void stage_operand(const float* X, long ld, int r0, int nrows, int k0, int K, uint8_t* dst,
-                                              uint32_t plane, int tid)
+// rows x 64 chunk of a K-contiguous FP32 operand (row r0.., column k0..) in
+// registers: thread tid holds float4 i at row (i NT + tid) / 16, columns
+// 4 ((i NT + tid) % 16) ..  + 3, so a warp reads two 256-byte row segments.
+// VEC: rows start on 16-byte boundaries (ld, base and batch stride multiples
+// of 4 floats), float4 loads; otherwise (or at the K edge) scalar loads.
+template <int ROWS, bool VEC>
+__device__ __forceinline__ void load_operand(const float* X, long ld, int r0, int nrows, int k0, int K,
+                                             float4 (&v)[ROWS / 16], int tid)
 {
-    constexpr int PER = ROWS * 32 / NT;
 #pragma unroll
-    for (int half = 0; half < 2; ++half) {
-        float v[PER];
-#pragma unroll
-        for (int i = 0; i < PER; ++i) {
-            const int e = i * NT + tid, r = e >> 5, k = half * 32 + (e & 31);
-            const int gr = r0 + r, gk = k0 + k;
-            v[i] = (gr < nrows && gk < K) ? X[(long)gr * ld + gk] : 0.0f;
-        }
-#pragma unroll
-        for (int i = 0; i < PER; ++i) {
-            const int e = i * NT + tid, r = e >> 5, k = half * 32 + (e & 31);
-            const __nv_bfloat16 p0 = __float2bfloat16_rn(v[i]);
-            const float r1 = v[i] - __bfloat162float(p0);
-            const __nv_bfloat16 p1 = __float2bfloat16_rn(r1);
-            const __nv_bfloat16 p2 = __float2bfloat16_rn(r1 - __bfloat162float(p1));
-            const uint32_t o = swz(r, k);
-            *reinterpret_cast<__nv_bfloat16*>(dst + o) = p0;
-            *reinterpret_cast<__nv_bfloat16*>(dst + plane + o) = p1;
-            *reinterpret_cast<__nv_bfloat16*>(dst + 2 * plane + o) = p2;
+    for (int i = 0; i < ROWS / 16; ++i) {
+        const int e = i * NT + tid, r = e >> 4, k = (e & 15) * 4;
+        const int gr = r0 + r, gk = k0 + k;
+        const float* p = X + (long)gr * ld + gk;
+        if (VEC && gr < nrows && gk + 3 < K) {
+            v[i] = *reinterpret_cast<const float4*>(p);
+        } else {
+            v[i].x = (gr < nrows && gk < K) ? p[0] : 0.0f;
+            v[i].y = (gr < nrows && gk + 1 < K) ? p[1] : 0.0f;
+            v[i].z = (gr < nrows && gk + 2 < K) ? p[2] : 0.0f;
+            v[i].w = (gr < nrows && gk + 3 < K) ? p[3] : 0.0f;
         }
     }
 }
 
-template <int BN, int STAGES>
+__device__ __forceinline__ void split3(float x, __nv_bfloat16& p0, __nv_bfloat16& p1, __nv_bfloat16& p2)
+{
+    p0 = __float2bfloat16_rn(x);
+    const float r1 = x - __bfloat162float(p0);
+    p1 = __float2bfloat16_rn(r1);
+    p2 = __float2bfloat16_rn(r1 - __bfloat162float(p1));
+}
+
+// The registers of load_operand as three BF16 planes `plane` bytes apart, in
+// the 128-byte-swizzled K-major layout (4 consecutive k share one 8-byte word).
+template <int ROWS>
+__device__ __forceinline__ void store_operand(const float4 (&v)[ROWS / 16], uint8_t* dst, uint32_t plane, int tid)
+{
+#pragma unroll
+    for (int i = 0; i < ROWS / 16; ++i) {
+        const int e = i * NT + tid, r = e >> 4, k = (e & 15) * 4;
+        __nv_bfloat16 a[3][4];
+        split3(v[i].x, a[0][0], a[1][0], a[2][0]);
+        split3(v[i].y, a[0][1], a[1][1], a[2][1]);
+        split3(v[i].z, a[0][2], a[1][2], a[2][2]);
+        split3(v[i].w, a[0][3], a[1][3], a[2][3]);
+        const uint32_t o = swz(r, k);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            uint2 w;
+            w.x = (uint32_t)__bfloat16_as_ushort(a[q][0]) | ((uint32_t)__bfloat16_as_ushort(a[q][1]) << 16);
+            w.y = (uint32_t)__bfloat16_as_ushort(a[q][2]) | ((uint32_t)__bfloat16_as_ushort(a[q][3]) << 16);
+            *reinterpret_cast<uint2*>(dst + q * plane + o) = w;
+        }
+    }
+}
+
+template <int BN, int STAGES, bool VEC>
 __global__ void __launch_bounds__(NT, STAGES == 1 ? 2 : 1) k_sgemm_bf16x6(int M, int N, int K, float alpha, const float* A, long lda,
                                                         long sA, const float* B, long ldb, long sB, float beta, float* C,
-                                                        long ldc, long sC, int lower_only, unsigned long long wait_ns,
-                                                        int* info)
+                                                        long ldc, long sC, float* C2, long ldc2, long sC2,
+                                                        int lower_only, unsigned long long wait_ns, int* info)
 {
     constexpr uint32_t B_BYTES = BN * KC * 2;
     constexpr uint32_t STAGE = PLANES * (A_BYTES + B_BYTES);
@@ -191,7 +219,15 @@ __global__ void __launch_bounds__(NT, STAGES == 1 ? 2 : 1) k_sgemm_bf16x6(int M,
     A += z * sA;
     B += z * sB;
     C += z * sC;
+    if (C2) C2 += z * sC2;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nch = (K + KC - 1) / KC;
+    // chunk 0's operands are in flight while the barriers and TMEM are set up
+    float4 ra[BM / 16], rb[BN / 16];
+    if (nch > 0) {
+        load_operand<BM, VEC>(A, lda, tile_m, M, 0, K, ra, tid);
+        load_operand<BN, VEC>(B, ldb, tile_n, N, 0, K, rb, tid);
+    }
     if (tid == 0) {
         mbar_init(&done[0], 1);
         mbar_init(&done[1], 1);
@@ -209,7 +245,6 @@ __global__ void __launch_bounds__(NT, STAGES == 1 ? 2 : 1) k_sgemm_bf16x6(int M,
     const uint32_t tmem = tmem_slot;
     const uint32_t idesc = instr_desc_bf16<BN>();
 
-    const int nch = (K + KC - 1) / KC;
     bool aborted = false;
     for (int c = 0; c < nch; ++c) {
         const int s = c % STAGES;
@@ -221,8 +256,8 @@ __global__ void __launch_bounds__(NT, STAGES == 1 ? 2 : 1) k_sgemm_bf16x6(int M,
             aborted = true;
             break;
         }
-        stage_operand<BM>(A, lda, tile_m, M, c * KC, K, sa, A_BYTES, tid);
-        stage_operand<BN>(B, ldb, tile_n, N, c * KC, K, sb, B_BYTES, tid);
+        store_operand<BM>(ra, sa, A_BYTES, tid);
+        store_operand<BN>(rb, sb, B_BYTES, tid);
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         __syncthreads();
         if (tid == 0) {
@@ -241,7 +276,28 @@ __global__ void __launch_bounds__(NT, STAGES == 1 ? 2 : 1) k_sgemm_bf16x6(int M,
             }
             umma_commit(&done[s]);
         }
+        // the next chunk's loads overlap this chunk's MMAs
+        if (c + 1 < nch) {
+            load_operand<BM, VEC>(A, lda, tile_m, M, (c + 1) * KC, K, ra, tid);
+            load_operand<BN, VEC>(B, ldb, tile_n, N, (c + 1) * KC, K, rb, tid);
+        }
     }
+    // Thread = output row in TMEM; each warp turns its 32 x 32 pieces around in
+    // shared memory so that C is read and written in 128-byte row segments.
+    // The C segments of the warp's first piece are read before the last wait.
+    const int quad = warp & 3;  // a warp reads TMEM lanes 32 (warp % 4) .. + 31
+    const int col = lane;
+    float cv[32];
+    auto load_c = [&](int g) {
+        const int c = tile_n + g * 32 + col;
+#pragma unroll
+        for (int r = 0; r < 32; ++r) {
+            const int row = tile_m + quad * 32 + r;
+            cv[r] = (beta != 0.0f && row < M && c < N) ? C[(long)row * ldc + c] : 0.0f;
+        }
+    };
+    const int g0 = warp >> 2;
+    if (!aborted) load_c(g0);
     bool ok = !aborted;
     if (ok && nch > 0) {
         const int cl = nch - 1;
@@ -257,31 +313,31 @@ __global__ void __launch_bounds__(NT, STAGES == 1 ? 2 : 1) k_sgemm_bf16x6(int M,
         }
         if (tid == 0 && info) atomicCAS(info + z, 0, CF_ERR_TIMEOUT);
     } else if (nch > 0) {
-        // Thread = output row in TMEM; each warp turns its 32 x 32 pieces around
-        // in shared memory (the operand stages are free now: every MMA has
-        // completed) so that C is read and written in 128-byte row segments.
+        // the operand stages are free now: every MMA has completed
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-        const int quad = warp & 3;  // a warp reads TMEM lanes 32 (warp % 4) .. + 31
         const uint32_t lane_addr = tmem + ((uint32_t)(quad * 32) << 16);
         float* T = reinterpret_cast<float*>(smem) + warp * 32 * 33;
-        const int col = lane;
 #pragma unroll 1
-        for (int g = warp >> 2; g < BN / 32; g += NT / 128) {  // the two warps of a quadrant split the columns
-            uint32_t v[32], w[32];
-            tmem_ld32(lane_addr + (uint32_t)(g * 32), v);
-            tmem_ld32(lane_addr + (uint32_t)(BN + g * 32), w);
+        for (int g = g0; g < BN / 32; g += NT / 128) {  // the two warps of a quadrant split the columns
+            if (g != g0) load_c(g);
+            {
+                uint32_t v[32];
+                tmem_ld32(lane_addr + (uint32_t)(g * 32), v);
 #pragma unroll
-            for (int j = 0; j < 32; ++j) T[lane * 33 + j] = __uint_as_float(v[j]) + __uint_as_float(w[j]);
+                for (int j = 0; j < 32; ++j) T[lane * 33 + j] = __uint_as_float(v[j]);
+                tmem_ld32(lane_addr + (uint32_t)(BN + g * 32), v);
+#pragma unroll
+                for (int j = 0; j < 32; ++j) T[lane * 33 + j] += __uint_as_float(v[j]);
+            }
             __syncwarp();
             const int c = tile_n + g * 32 + col;
-#pragma unroll 4
+#pragma unroll
             for (int r = 0; r < 32; ++r) {
                 const int row = tile_m + quad * 32 + r;
                 if (row < M && c < N) {
-                    float* pc = C + (long)row * ldc + c;
-                    float out = alpha * T[r * 33 + col];
-                    if (beta != 0.0f) out += beta * *pc;
-                    *pc = out;
+                    const float out = alpha * T[r * 33 + col] + beta * cv[r];
+                    C[(long)row * ldc + c] = out;
+                    if (C2) C2[(long)row * ldc2 + c] = out;
                 }
             }
             __syncwarp();
@@ -299,22 +355,65 @@ unsigned long long g_sgemm_wait_ns = DRAIN_NS;
 // overlap each other's loads and MMAs).
 int g_sgemm_stages = 1;
 
-template <int BN, int STAGES>
-int launch(int M, int N, int K, float alpha, const float* A, long lda, long sA, const float* B, long ldb, long sB,
-           float beta, float* C, long ldc, long sC, int batch, int lower_only, int* info, cudaStream_t st)
+template <int BN, int STAGES, bool VEC>
+int launch_t(int M, int N, int K, float alpha, const float* A, long lda, long sA, const float* B, long ldb, long sB,
+             float beta, float* C, long ldc, long sC, float* C2, long ldc2, long sC2, int batch, int lower_only,
+             int* info, cudaStream_t st)
 {
     constexpr size_t smem = 1024 + STAGES * (size_t)PLANES * (A_BYTES + (size_t)BN * KC * 2);
     static_assert(smem <= 232448, "shared memory exceeds 227 KB");
     static std::atomic<int> attr[CF_MAX_DEVICES];
-    if (int rc = cf_smem_optin(k_sgemm_bf16x6<BN, STAGES>, (int)smem, attr)) return rc;
+    if (int rc = cf_smem_optin(k_sgemm_bf16x6<BN, STAGES, VEC>, (int)smem, attr)) return rc;
     dim3 grid(cf_cdiv(N, BN), cf_cdiv(M, BM), batch);
-    k_sgemm_bf16x6<BN, STAGES><<<grid, NT, smem, st>>>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC,
-                                                       lower_only, g_sgemm_wait_ns, info);
+    k_sgemm_bf16x6<BN, STAGES, VEC><<<grid, NT, smem, st>>>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC,
+                                                            C2, ldc2, sC2, lower_only, g_sgemm_wait_ns, info);
     CF_CHECK_LAUNCH();
     return CF_OK;
 }
 
+inline bool aligned16(const float* p, long ld, long stride, int batch)
+{
+    return ((uintptr_t)p & 15) == 0 && (ld & 3) == 0 && (batch == 1 || (stride & 3) == 0);
+}
+
+template <int BN, int STAGES>
+int launch(int M, int N, int K, float alpha, const float* A, long lda, long sA, const float* B, long ldb, long sB,
+           float beta, float* C, long ldc, long sC, float* C2, long ldc2, long sC2, int batch, int lower_only,
+           int* info, cudaStream_t st)
+{
+    if (aligned16(A, lda, sA, batch) && aligned16(B, ldb, sB, batch))
+        return launch_t<BN, STAGES, true>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, C2, ldc2, sC2,
+                                          batch, lower_only, info, st);
+    return launch_t<BN, STAGES, false>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, C2, ldc2, sC2, batch,
+                                       lower_only, info, st);
+}
+
 }  // namespace
+
+// Same product with an optional second destination C2 (same values; NULL for
+// none), for the FP32 Cholesky's panel solves, which write the panel to its
+// work buffer and into the matrix in one pass.  C2 must not overlap C, nor
+// operand rows read by another CTA.
+int cf_sgemm_bf16x6_dual(int M, int N, int K, float alpha, const float* A, long lda, long sA, const float* B,
+                         long ldb, long sB, float beta, float* C, long ldc, long sC, float* C2, long ldc2, long sC2,
+                         int batch, int lower_only, int* info, void* stream)
+{
+    if (M < 0 || N < 0 || K < 0 || batch < 1 || !C || (K > 0 && (!A || !B))) return CF_ERR_ARG;
+    if (M == 0 || N == 0) return CF_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (g_sgemm_stages == 2) {
+        if (N <= 64)
+            return launch<64, 2>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, C2, ldc2, sC2, batch,
+                                 lower_only, info, st);
+        return launch<128, 2>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, C2, ldc2, sC2, batch,
+                              lower_only, info, st);
+    }
+    if (N <= 64)
+        return launch<64, 1>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, C2, ldc2, sC2, batch,
+                             lower_only, info, st);
+    return launch<128, 1>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, C2, ldc2, sC2, batch, lower_only,
+                          info, st);
+}
 
 // C_z = alpha A_z B_z^T + beta C_z (FP32, row-major, K contiguous in A and B;
 // z < batch with element strides sA, sB, sC) with six BF16 split products on
@@ -325,17 +424,8 @@ extern "C" int cf_sgemm_bf16x6(int M, int N, int K, float alpha, const float* A,
                                long ldb, long sB, float beta, float* C, long ldc, long sC, int batch, int lower_only,
                                int* info, void* stream)
 {
-    if (M < 0 || N < 0 || K < 0 || batch < 1 || !C || (K > 0 && (!A || !B))) return CF_ERR_ARG;
-    if (M == 0 || N == 0) return CF_OK;
-    cudaStream_t st = (cudaStream_t)stream;
-    if (g_sgemm_stages == 2) {
-        if (N <= 64)
-            return launch<64, 2>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower_only, info, st);
-        return launch<128, 2>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower_only, info, st);
-    }
-    if (N <= 64)
-        return launch<64, 1>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower_only, info, st);
-    return launch<128, 1>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower_only, info, st);
+    return cf_sgemm_bf16x6_dual(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, nullptr, 0, 0, batch,
+                                lower_only, info, stream);
 }
 
 // Operand stages of cf_sgemm_bf16x6: 1 (default; two CTAs per SM) or 2 (one

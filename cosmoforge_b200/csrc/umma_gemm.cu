@@ -148,18 +148,19 @@ __device__ __forceinline__ void tma_load_4d(const CUtensorMap* map, uint64_t* ba
 }
 
 // Shared-memory matrix descriptor, K-major rows of BKT BF16: BKT = 64 is the
-// 128B swizzle (8-row atoms 1024 B apart), BKT = 32 the 64B swizzle (512 B).
+// 128B swizzle (8-row atoms 1024 B apart), BKT = 32 the 64B swizzle (512 B),
+// BKT = 16 the 32B swizzle (256 B).
 template <int BKT>
 __device__ __forceinline__ uint64_t smem_desc(const void* tile)
 {
-    static_assert(BKT == 64 || BKT == 32, "k-tile of 64 or 32 BF16");
+    static_assert(BKT == 64 || BKT == 32 || BKT == 16, "k-tile of 64, 32 or 16 BF16");
     const uint64_t addr = smem_u32(tile);
     uint64_t d = 0;
     d |= (addr >> 4) & 0x3FFFull;                  // start address
     d |= (uint64_t)(16 >> 4) << 16;                // leading byte offset (unused for swizzled K-major)
     d |= (uint64_t)((8 * BKT * 2) >> 4) << 32;     // stride byte offset: 8 rows
     d |= (uint64_t)1 << 46;                        // descriptor version (sm100)
-    d |= (uint64_t)(BKT == 64 ? 2 : 4) << 61;      // SWIZZLE_128B / SWIZZLE_64B
+    d |= (uint64_t)(BKT == 64 ? 2 : (BKT == 32 ? 4 : 6)) << 61;  // SWIZZLE_128B / 64B / 32B
     return d;
 }
 
@@ -535,7 +536,7 @@ EncodeTiledFn encode_fn()
 }
 
 // 3D bf16 map: dims (K, rows, planes), row stride ld elements, plane stride ps elements;
-// box (bk, box_rows, 1): bk = 64 with 128B swizzle, bk = 32 with 64B swizzle.
+// box (bk, box_rows, 1): bk = 64 with 128B swizzle, bk = 32 with 64B, bk = 16 with 32B.
 int make_map(CUtensorMap* map, const void* base, long K, long rows, long ld, int planes, long ps, int box_rows,
              int bk = BK)
 {
@@ -547,7 +548,8 @@ int make_map(CUtensorMap* map, const void* base, long K, long rows, long ld, int
     cuuint32_t box[3] = {(cuuint32_t)bk, (cuuint32_t)box_rows, 1};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides, box, estr,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, bk == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    bk == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : (bk == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B),
                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? CF_OK : CF_ERR_ARG;
@@ -599,7 +601,10 @@ int launch_gemm_kc(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, i
 }
 
 // GEMM mode: 1 = all planes of a 32-wide k-slice per stage with split
-// accumulators where the planes allow it, 0 = 64-wide k-tiles term by term.
+// accumulators where the planes allow it (3 stages of 72 KB for three
+// planes), 2 = the same with 16-wide k-slices (6 stages of 36 KB: the same
+// ring in finer steps, so a stage is refilled sooner), 0 = 64-wide k-tiles
+// term by term.
 int g_all_planes = 1;
 
 template <int BN, int STAGES, bool TRACE, int PLS = 1, int BKT = BK, bool SPLIT = false>
@@ -666,11 +671,12 @@ extern "C" int cf_umma_set_group(int group_m)
     return prev;
 }
 
-// Select the GEMM form (1 = all planes per stage, 0 = term by term); returns the previous one.
+// Select the GEMM form (1 = all planes per stage in 32-wide k-slices, 2 = in
+// 16-wide k-slices, 0 = term by term); returns the previous one.
 extern "C" int cf_umma_set_all_planes(int on)
 {
     const int prev = g_all_planes;
-    g_all_planes = on ? 1 : 0;
+    g_all_planes = (on == 0 || on == 1 || on == 2) ? on : 1;
     return prev;
 }
 
@@ -704,10 +710,15 @@ extern "C" int cf_umma_gemm_bf16(int M, int N, int K, int nterms, const int* ta,
     bool all_planes = g_all_planes && (pls == 2 || pls == 3) && t.a[0] == 0 && t.b[0] == 0;
     for (int i = 1; i < nterms && all_planes; ++i) all_planes = !(t.a[i] == 0 && t.b[i] == 0);
     if (all_planes) {
-        int rc = make_map(&ma, A, K, M, lda, a_planes, a_ps, BM, 32);
+        const int bk = g_all_planes == 2 ? 16 : 32;
+        int rc = make_map(&ma, A, K, M, lda, a_planes, a_ps, BM, bk);
         if (rc) return rc;
-        rc = make_map(&mb, B, K, N, ldb, b_planes, b_ps, 256, 32);
+        rc = make_map(&mb, B, K, N, ldb, b_planes, b_ps, 256, bk);
         if (rc) return rc;
+        if (bk == 16) {
+            if (pls == 3) return launch_gemm<256, 6, false, 3, 16, true>(ma, mb, M, N, K, t, e, tr, 1, err, st);
+            return launch_gemm<256, 8, false, 2, 16, true>(ma, mb, M, N, K, t, e, tr, 1, err, st);
+        }
         if (pls == 3) return launch_gemm<256, 3, false, 3, 32, true>(ma, mb, M, N, K, t, e, tr, 1, err, st);
         return launch_gemm<256, 4, false, 2, 32, true>(ma, mb, M, N, K, t, e, tr, 1, err, st);
     }

@@ -103,9 +103,13 @@ size_t cf_potrf_workspace(int n, int batch);
 /*
  * Blocked lower Cholesky factorisation in place (batch of n x n matrices):
  * 64-wide panels, diagonal block factored and inverted by one CTA, panel and
- * trailing updates as DMMA GEMMs.  work: cf_potrf_workspace(n, batch) bytes
- * (keeps the diagonal-block inverses for cf_trtri_lower).  info: int[batch],
- * zeroed by the caller.
+ * trailing updates as DMMA GEMMs.  A single matrix (batch 1) of order above
+ * 1024 is factored with a look-ahead: the critical path runs on an internal
+ * high-priority stream forked from and joined back to `stream` by events
+ * (stream-ordered, capturable into a CUDA graph), the bulk of each trailing
+ * update on `stream`.  work: cf_potrf_workspace(n, batch) bytes (keeps the
+ * diagonal-block inverses for cf_trtri_lower; one more panel buffer for the
+ * look-ahead).  info: int[batch], zeroed by the caller.
  * Replaces: cosmocore/basics/linalg.py:362-406 (cholesky_factor, LAPACK dpotrf).
  */
 int cf_potrf(int n, double* A, long lda, long strideA, int batch, void* work, int* info, void* stream);
@@ -179,7 +183,9 @@ int cf_qml_reduce_f64(int P, int R, int Ccols, const double* D, long ldD, long s
 /*
  * chi2[b nrhs + m] = |L_b^-1 x_{b,m}|^2 and logdet[b] = 2 sum ln (L_b)_ii
  * from lower Cholesky factors (batch).  X: n x nrhs (ldx), strideX = 0 shares
- * it across the batch; z_work: batch * nrhs * n doubles.
+ * it across the batch; z_work: batch * nrhs * n doubles, used (and required)
+ * only for n > 24576, may be NULL below (the solve vector lives in shared
+ * memory).
  * Replaces: picslike/picslike.py:643-664 (chi2 einsum with C^-1) and
  * cosmocore/basics/linalg.py:430-474 (matrix_slogdet_symm).
  */
@@ -302,8 +308,9 @@ int cf_umma_set_promotion(int kc);
 /* Form of cf_umma_gemm_bf16: 1 (default) loads every plane of a 32-wide
  * k-slice into one pipeline stage and keeps the leading product apart from
  * the corrections in a second TMEM accumulator, when both operands carry the
- * same 2 or 3 planes; 0 walks 64-wide k-tiles term by term.  Returns the
- * previous setting.  No counterpart in the reference. */
+ * same 2 or 3 planes; 2 does the same with 16-wide k-slices (twice the
+ * stages of the same ring); 0 walks 64-wide k-tiles term by term.  Returns
+ * the previous setting.  No counterpart in the reference. */
 int cf_umma_set_all_planes(int on);
 
 /* Row tiles per group in the persistent tile order of the tcgen05 kernels

@@ -54,3 +54,30 @@ def test_large_inverse_reports_pivot(bad):
     C[bad, bad] = -1.0
     _, info = _inverse(lib, C, 1)
     assert int(info.item()) == bad + 1
+
+
+def test_large_inverse_in_a_cuda_graph():
+    """Above order 1024 the factorisation forks a side stream for its
+    look-ahead and joins it back; the call must capture into a CUDA graph and
+    replay to the eager result bit for bit."""
+    from cosmoforge_b200 import _lib
+
+    lib = _lib.lib()
+    n = 1500
+    C = _spd(n, 11)
+    eager, _ = _inverse(lib, C, 1)
+    A = C.clone()
+    work = torch.empty(lib.cf_spd_inverse_workspace(n, 1) // 8 + 1, dtype=torch.float64, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            rc = lib.cf_spd_inverse(n, A.data_ptr(), n, n * n, 1, work.data_ptr(), info.data_ptr(), s.cuda_stream)
+    assert rc == 0
+    for _ in range(2):
+        A.copy_(C)
+        g.replay()
+        torch.cuda.synchronize()
+        assert int(info.item()) == 0
+        assert torch.equal(A, eager)
