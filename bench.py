@@ -747,7 +747,7 @@ def main():
 # --------------------------------------------------------------------------
 KERNEL_DOC = """Single-kernel timing cases (``python bench.py kernel CASE SHAPE``).
 
-    python bench.py kernel umma_gemm M,N,K [--planes 3] [--reps 5] [--kc 16]
+    python bench.py kernel umma_gemm M,N,K [--planes 3] [--reps 5] [--kc 16] [--form 1|0]
     python bench.py kernel umma_trace P1,P2,K1,K2 [--planes 3]
     python bench.py kernel dgemm M,N,K
     python bench.py kernel spd_inverse N
@@ -961,10 +961,13 @@ def kernel_main(argv=None):
     ap.add_argument("--kc", type=int, default=16, help="promotion interval of the tensor-core kernels")
     ap.add_argument("--splits", type=int, default=0)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed", help="map_solves and lnl")
+    ap.add_argument("--form", type=int, choices=[0, 1], default=1,
+                    help="tensor-core GEMM form: 1 = all planes per 32-wide k-slice, 0 = term by term")
     a = ap.parse_args(argv)
     dims = [int(x) for x in a.shape.split(",")]
     lib = _lib.lib()
     lib.cf_umma_set_promotion(a.kc)
+    lib.cf_umma_set_all_planes(a.form)
     if a.case == "umma_gemm":
         fn, fl, err = umma_gemm_case(*dims, planes=a.planes)
     elif a.case == "umma_trace":

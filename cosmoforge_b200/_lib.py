@@ -65,6 +65,8 @@ SIGNATURES = {
     "cf_split_bf16": (_i, [_i, _i, _p, _l, _i, _p, _l, _l, _p]),
     "cf_umma_gemm_bf16": (_i, [_i, _i, _i, _i, _p, _p, _p, _l, _l, _i, _p, _l, _l, _i, _p, _l, _l, _i,
                                _p, _l, _l, _p, _l, _p, _p]),
+    "cf_umma_gemm_bf16_scatter": (_i, [_i, _i, _i, _i, _p, _p, _p, _l, _l, _i, _p, _l, _l, _i, _p, _p, _l, _i,
+                                       _l, _p, _p]),
     "cf_potrf_f32_workspace": (_sz, [_i, _i]),
     "cf_potrf_f32": (_i, [_i, _p, _l, _l, _i, _p, _p, _p]),
     "cf_sgemm_bf16x6": (_i, [_i, _i, _i, _f, _p, _l, _l, _p, _l, _l, _f, _p, _l, _l, _i, _i, _p, _p]),
@@ -73,6 +75,7 @@ SIGNATURES = {
     "cf_potrf_f32_set_tensor": (_i, [_i]),
     "cf_axpby_f32": (_i, [_l, _d, _p, _l, _d, _p, _p, _l, _p, _l, _p, _l, _i, _p]),
     "cf_chi2_logdet_mixed": (_i, [_i, _p, _l, _l, _p, _l, _l, _i, _p, _l, _l, _i, _p, _p, _p]),
+    "cf_chi2_logdet_mixed_c32": (_i, [_i, _p, _l, _l, _p, _l, _l, _i, _p, _l, _l, _i, _p, _p, _p]),
     "cf_mlp_dense_fwd": (_i, [_i, _i, _i, _p, _l, _p, _p, _i, _p, _p, _l, _p]),
     "cf_mlp_dense_bwd_data": (_i, [_i, _i, _i, _p, _p, _p, _p, _p]),
     "cf_mlp_dense_bwd_weight": (_i, [_i, _i, _i, _p, _p, _l, _p, _p, _p]),

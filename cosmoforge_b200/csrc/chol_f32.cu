@@ -18,12 +18,7 @@
 #include "potrf_diag.cuh"
 #include "tri_solve.cuh"
 
-extern "C" int cf_sgemm_bf16x6(int M, int N, int K, float alpha, const float* A, long lda, long sA, const float* B,
-                               long ldb, long sB, float beta, float* C, long ldc, long sC, int batch, int lower_only,
-                               int* info, void* stream);
-int cf_sgemm_bf16x6_dual(int M, int N, int K, float alpha, const float* A, long lda, long sA, const float* B,
-                         long ldb, long sB, float beta, float* C, long ldc, long sC, float* C2, long ldc2, long sC2,
-                         int batch, int lower_only, int* info, void* stream);
+#include "tc_sgemm.cuh"
 
 namespace {
 
@@ -32,7 +27,7 @@ constexpr int NB = cf_diag::NB;
 using cf_diag::k_potrf_diag_inv;
 
 // Product kernel of the FP32 factor's panel solves and trailing updates:
-// 1 = BF16x6 split products on the tensor cores (cf_sgemm_bf16x6, default),
+// 1 = BF16x6 split products on the tensor cores (tc_sgemm.cu, default),
 // 0 = the FP32 SIMT kernel below.
 int g_potrf_f32_tensor = 1;
 
@@ -148,30 +143,56 @@ int sgemm_nt_simt(int M, int N, int K, float alpha, const float* A, long lda, lo
     return CF_OK;
 }
 
-int sgemm_nt(int M, int N, int K, float alpha, const float* A, long lda, long sA, const float* B, long ldb, long sB,
-             float beta, float* C, long ldc, long sC, int batch, int lower_only, int* info, cudaStream_t st)
-{
-    if (g_potrf_f32_tensor)
-        return cf_sgemm_bf16x6(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower_only, info, st);
-    return sgemm_nt_simt(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower_only, st);
-}
-
 __global__ void k_copy2d_f32(int R, int Ccols, const float* src, long lds, long ss, float* dst, long ldd, long sd);
 
-// Panel solve W = A21 Dinv^T (M x kb, K = kb) written to the work buffer W and
-// into the matrix at A21 itself: one pass with the tensor-core GEMM's second
-// destination, or the SIMT GEMM and a copy.
-int panel_nt(int M, int kb, float* a21, long lda, long sA, const float* D, long sD, float* W, long ldw, long sW,
-             int batch, int* info, cudaStream_t st)
+// The factor's work panel W (n rows x 2 NB columns per problem): FP32 for the
+// SIMT kernel, or, for the tensor cores, the three BF16 split planes of the
+// FP32 panel (split once, where the panel is solved, instead of in every
+// output tile that reads it).  `ws` floats per problem hold either form.
+struct Panel {
+    float* f;
+    long ws;
+    int n;
+    static constexpr int LD = 2 * NB;
+    __nv_bfloat16* planes() const { return reinterpret_cast<__nv_bfloat16*>(f); }
+    long plane_stride() const { return (long)n * LD; }
+};
+
+// Panel solve: W[r0.., c0..c0+kb) = A21 Dinv^T (M x kb, K = kb), written to W
+// and into the matrix at A21 in one pass (tensor cores: W as split planes), or
+// by the SIMT GEMM and a copy.
+int panel_solve(int M, int kb, float* a21, long lda, long sA, const float* D, const Panel& W, int r0, int c0,
+                int batch, int* info, cudaStream_t st)
 {
-    if (g_potrf_f32_tensor)
-        return cf_sgemm_bf16x6_dual(M, kb, kb, 1.0f, a21, lda, sA, D, kb, sD, 0.0f, W, ldw, sW, a21, lda, sA, batch, 0,
-                                    info, st);
-    int rc = sgemm_nt_simt(M, kb, kb, 1.0f, a21, lda, sA, D, kb, sD, 0.0f, W, ldw, sW, batch, 0, st);
+    if (g_potrf_f32_tensor) {
+        const cf_sg::Opnd a{a21, lda, sA, 0}, d{D, kb, W.ws, 0};
+        const cf_sg::Out o{nullptr, 0, 0, a21, lda, sA, W.planes() + (long)r0 * Panel::LD + c0, Panel::LD, 2 * W.ws,
+                           W.plane_stride()};
+        return cf_sg::sgemm(M, kb, kb, 1.0f, a, d, 0.0f, o, false, batch, 0, info, st);
+    }
+    float* w = W.f + (long)r0 * Panel::LD + c0;
+    int rc = sgemm_nt_simt(M, kb, kb, 1.0f, a21, lda, sA, D, kb, W.ws, 0.0f, w, Panel::LD, W.ws, batch, 0, st);
     if (rc) return rc;
-    k_copy2d_f32<<<dim3(cf_cdiv(kb, 32), cf_cdiv(M, 8), batch), dim3(32, 8), 0, st>>>(M, kb, W, ldw, sW, a21, lda, sA);
+    k_copy2d_f32<<<dim3(cf_cdiv(kb, 32), cf_cdiv(M, 8), batch), dim3(32, 8), 0, st>>>(M, kb, w, Panel::LD, W.ws, a21,
+                                                                                      lda, sA);
     CF_CHECK_LAUNCH();
     return CF_OK;
+}
+
+// C -= W[ra.., 0:K) W[rb.., 0:K)^T (M x N), lower_only as in the GEMMs.
+int panel_update(int M, int N, int K, const Panel& W, int ra, int rb, float* C, long ldc, long sC, int batch,
+                 int lower_only, int* info, cudaStream_t st)
+{
+    if (g_potrf_f32_tensor) {
+        const cf_sg::Opnd a{W.planes() + (long)ra * Panel::LD, Panel::LD, 2 * W.ws, W.plane_stride()};
+        const cf_sg::Opnd b{W.planes() + (long)rb * Panel::LD, Panel::LD, 2 * W.ws, W.plane_stride()};
+        const cf_sg::Out o{C, ldc, sC, nullptr, 0, 0, nullptr, 0, 0, 0};
+        return cf_sg::sgemm(M, N, K, -1.0f, a, b, 1.0f, o, true, batch, lower_only, info, st);
+    }
+    const float* wa = W.f + (long)ra * Panel::LD;
+    const float* wb = W.f + (long)rb * Panel::LD;
+    return sgemm_nt_simt(M, N, K, -1.0f, wa, Panel::LD, W.ws, wb, Panel::LD, W.ws, 1.0f, C, ldc, sC, batch,
+                         lower_only, st);
 }
 
 __global__ void k_copy2d_f32(int R, int Ccols, const float* src, long lds, long ss, float* dst, long ldd, long sd)
@@ -211,8 +232,8 @@ constexpr int CNT = 256;
 // row per thread to its left, while the threads on rows at or below the block
 // add that block's 32 columns of the lower triangle of C to v^T C v (every v
 // they need is final by then), so C is read once, in row segments.
-template <bool VL, bool VC>
-__global__ void __launch_bounds__(CNT, 2) k_chi2_refined(int n, const float* L, long lda, long sL, const double* C,
+template <bool VL, bool VC, typename TC>
+__global__ void __launch_bounds__(CNT, 2) k_chi2_refined(int n, const float* L, long lda, long sL, const TC* C,
                                                          long ldc, long sC, const double* X, long ldx, long sX,
                                                          int nrhs, double* chi2)
 {
@@ -251,9 +272,9 @@ __global__ void __launch_bounds__(CNT, 2) k_chi2_refined(int n, const float* L, 
             } else if (q >= b0 + kb) {
                 qf += 2.0 * v[q] * cf_tri::seg_dot<VC>(C + (long)q * ldc + b0, v + b0, kb);
             } else {
-                const double* cr = C + (long)q * ldc;
-                double t = cr[q] * v[q];
-                for (int c = b0; c < q; ++c) t += 2.0 * cr[c] * v[c];
+                const TC* cr = C + (long)q * ldc;
+                double t = (double)cr[q] * v[q];
+                for (int c = b0; c < q; ++c) t += 2.0 * (double)cr[c] * v[c];
                 qf += v[q] * t;
             }
         }
@@ -286,7 +307,9 @@ __global__ void __launch_bounds__(CNT) k_logdet_f32(int n, const float* L, long 
     }
 }
 
-inline size_t potrf_f32_ws(int n) { return (size_t)2 * NB * NB + (size_t)n * 2 * NB; }
+// floats per problem: two diagonal-block inverses and the work panel (FP32, or
+// three BF16 planes of it: 3 n 2 NB BF16 = 3 n NB floats)
+inline size_t potrf_f32_ws(int n) { return (size_t)2 * NB * NB + (size_t)3 * n * NB; }
 
 }  // namespace
 
@@ -305,7 +328,9 @@ extern "C" size_t cf_potrf_f32_workspace(int n, int batch) { return potrf_f32_ws
 // diagonal block is factored and inverted by one CTA and L21 = A21 L11^-T is a
 // GEMM; panels go in pairs so the trailing update A22 -= L21 L21^T runs once
 // per 128 columns.  The GEMMs are BF16x6 split products on the tensor cores
-// (cf_sgemm_bf16x6) unless cf_potrf_f32_set_tensor(0) selects the SIMT kernel.
+// unless cf_potrf_f32_set_tensor(0) selects the SIMT kernel: each panel solve
+// writes its panel into the matrix (FP32) and into the work panel as three
+// BF16 split planes, which the updates then copy straight into shared memory.
 // info: int[batch] zeroed by the caller; k > 0 is the first bad pivot, -3 a
 // tensor-core wait that ran out.
 extern "C" int cf_potrf_f32(int n, float* A, long lda, long strideA, int batch, void* work, int* info, void* stream)
@@ -313,35 +338,37 @@ extern "C" int cf_potrf_f32(int n, float* A, long lda, long strideA, int batch, 
     if (n <= 0 || batch < 1 || !A || !work || lda < n) return CF_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     const long ws = (long)potrf_f32_ws(n);
-    float* D1 = (float*)work;             // [batch][NB][NB]
-    float* D2 = D1 + (long)NB * NB;       // [batch][NB][NB]
-    float* W = D2 + (long)NB * NB;        // [batch][n][2 NB]
-    constexpr int LDW = 2 * NB;
+    float* D1 = (float*)work;        // [batch][NB][NB]
+    float* D2 = D1 + (long)NB * NB;  // [batch][NB][NB]
+    const Panel W{D2 + (long)NB * NB, ws, n};
+    constexpr size_t DSM = cf_diag::smem_bytes<float>();
     // Panels in pairs with a look-ahead (see cf_potrf): one K = 128 trailing
     // update per 128 columns.
     for (int k0 = 0; k0 < n; k0 += 2 * NB) {
         const int kb1 = n - k0 < NB ? n - k0 : NB;
-        k_potrf_diag_inv<float><<<batch, cf_diag::NTHREADS, cf_diag::smem_bytes<float>(), st>>>(A, lda, strideA, k0, kb1, D1, ws, info);
+        k_potrf_diag_inv<float><<<batch, cf_diag::NTHREADS, DSM, st>>>(A, lda, strideA, k0, kb1, D1, ws, info);
         CF_CHECK_LAUNCH();
         const int rest1 = n - k0 - kb1;
         if (rest1 <= 0) break;
         float* a21_1 = A + (long)(k0 + kb1) * lda + k0;
-        int rc = panel_nt(rest1, kb1, a21_1, lda, strideA, D1, ws, W, LDW, ws, batch, info, st);
+        // panel 1 into W rows 0.., columns 0..kb1
+        int rc = panel_solve(rest1, kb1, a21_1, lda, strideA, D1, W, 0, 0, batch, info, st);
         if (rc) return rc;
         const int kb2 = rest1 < NB ? rest1 : NB;
-        rc = sgemm_nt(rest1, kb2, kb1, -1.0f, W, LDW, ws, W, LDW, ws, 1.0f, a21_1 + kb1, lda, strideA, batch, 0, info, st);
+        // panel 2's columns, every row below panel 1
+        rc = panel_update(rest1, kb2, kb1, W, 0, 0, a21_1 + kb1, lda, strideA, batch, 0, info, st);
         if (rc) return rc;
         const int k1 = k0 + kb1;
-        k_potrf_diag_inv<float><<<batch, cf_diag::NTHREADS, cf_diag::smem_bytes<float>(), st>>>(A, lda, strideA, k1, kb2, D2, ws, info);
+        k_potrf_diag_inv<float><<<batch, cf_diag::NTHREADS, DSM, st>>>(A, lda, strideA, k1, kb2, D2, ws, info);
         CF_CHECK_LAUNCH();
         const int rest2 = rest1 - kb2;
         if (rest2 <= 0) break;
         float* a21_2 = A + (long)(k1 + kb2) * lda + k1;
-        float* W2 = W + (long)kb2 * LDW;
-        rc = panel_nt(rest2, kb2, a21_2, lda, strideA, D2, ws, W2 + kb1, LDW, ws, batch, info, st);
+        // panel 2 into W rows kb2.., columns kb1..kb1+kb2
+        rc = panel_solve(rest2, kb2, a21_2, lda, strideA, D2, W, kb2, kb1, batch, info, st);
         if (rc) return rc;
-        rc = sgemm_nt(rest2, rest2, kb1 + kb2, -1.0f, W2, LDW, ws, W2, LDW, ws, 1.0f, a21_2 + kb2, lda, strideA, batch,
-                      1, info, st);
+        // trailing update with both panels, lower tiles
+        rc = panel_update(rest2, rest2, kb1 + kb2, W, kb2, kb2, a21_2 + kb2, lda, strideA, batch, 1, info, st);
         if (rc) return rc;
     }
     return CF_OK;
@@ -364,24 +391,21 @@ extern "C" int cf_axpby_f32(long count, double a, const double* X, long strideX,
     return CF_OK;
 }
 
-// chi2[b nrhs + m] = 2 |L_b^-1 x|^2 - v^T C_b v with v = (L_b L_b^T)^-1 x (one
-// FP64 refinement step on the FP32 factor L_b of C_b), logdet[b] = 2 sum ln
-// (L_b)_ii.  C: FP64 matrices (lower triangle read); X: n x nrhs (ldx),
-// strideX = 0 shares it.  n <= 12288 (two FP64 vectors in shared memory).
-extern "C" int cf_chi2_logdet_mixed(int n, const float* L, long lda, long strideL, const double* C, long ldc,
-                                    long strideC, int batch, const double* X, long ldx, long strideX, int nrhs,
-                                    double* chi2, double* logdet, void* stream)
+namespace {
+template <typename TC>
+int chi2_mixed(int n, const float* L, long lda, long strideL, const TC* C, long ldc, long strideC, int batch,
+               const double* X, long ldx, long strideX, int nrhs, double* chi2, double* logdet, cudaStream_t st)
 {
     if (n <= 0 || batch < 1 || nrhs < 0 || !L) return CF_ERR_ARG;
     if (n > 12288) return CF_ERR_UNSUPPORTED;
-    cudaStream_t st = (cudaStream_t)stream;
     if (nrhs > 0) {
         if (!X || !C || !chi2) return CF_ERR_ARG;
         const size_t smem = 2 * (size_t)n * sizeof(double);
+        constexpr long VW = 16 / sizeof(TC);  // elements per 16-byte vector
         const bool vl = ((uintptr_t)L & 15) == 0 && (lda & 3) == 0 && (batch == 1 || (strideL & 3) == 0);
-        const bool vc = ((uintptr_t)C & 15) == 0 && (ldc & 1) == 0 && (batch == 1 || (strideC & 1) == 0);
-        auto kern = vl ? (vc ? k_chi2_refined<true, true> : k_chi2_refined<true, false>)
-                       : (vc ? k_chi2_refined<false, true> : k_chi2_refined<false, false>);
+        const bool vc = ((uintptr_t)C & 15) == 0 && (ldc % VW) == 0 && (batch == 1 || (strideC % VW) == 0);
+        auto kern = vl ? (vc ? k_chi2_refined<true, true, TC> : k_chi2_refined<true, false, TC>)
+                       : (vc ? k_chi2_refined<false, true, TC> : k_chi2_refined<false, false, TC>);
         static std::atomic<int> attr[4][CF_MAX_DEVICES];
         int rc = cf_smem_optin(kern, 2 * 12288 * (int)sizeof(double), attr[2 * vl + vc]);
         if (rc) return rc;
@@ -393,4 +417,27 @@ extern "C" int cf_chi2_logdet_mixed(int n, const float* L, long lda, long stride
         CF_CHECK_LAUNCH();
     }
     return CF_OK;
+}
+}  // namespace
+
+// chi2[b nrhs + m] = 2 |L_b^-1 x|^2 - v^T C_b v with v = (L_b L_b^T)^-1 x (one
+// FP64 refinement step on the FP32 factor L_b of C_b), logdet[b] = 2 sum ln
+// (L_b)_ii.  C: FP64 matrices (lower triangle read); X: n x nrhs (ldx),
+// strideX = 0 shares it.  n <= 12288 (two FP64 vectors in shared memory).
+extern "C" int cf_chi2_logdet_mixed(int n, const float* L, long lda, long strideL, const double* C, long ldc,
+                                    long strideC, int batch, const double* X, long ldx, long strideX, int nrhs,
+                                    double* chi2, double* logdet, void* stream)
+{
+    return chi2_mixed<double>(n, L, lda, strideL, C, ldc, strideC, batch, X, ldx, strideX, nrhs, chi2, logdet,
+                              (cudaStream_t)stream);
+}
+
+// The same with C in FP32 (the matrices the FP32 factor was computed from, as
+// the tensor-core build writes them); the refinement arithmetic stays FP64.
+extern "C" int cf_chi2_logdet_mixed_c32(int n, const float* L, long lda, long strideL, const float* C, long ldc,
+                                        long strideC, int batch, const double* X, long ldx, long strideX, int nrhs,
+                                        double* chi2, double* logdet, void* stream)
+{
+    return chi2_mixed<float>(n, L, lda, strideL, C, ldc, strideC, batch, X, ldx, strideX, nrhs, chi2, logdet,
+                             (cudaStream_t)stream);
 }

@@ -11,8 +11,9 @@
 //   (c) the trailing lower triangle takes the rank-16 update, 3 x 3 entries
 //       per thread.
 // Three barriers per panel instead of one per column.  The inverse X = L^-1 is
-// formed by 16-row block rows: each warp t inverts diagonal tile t by forward
-// substitution (lane c = column c), then block row I takes
+// formed by 16-row block rows: a spare warp inverts each diagonal tile by
+// forward substitution (lane c = column c) while the rows below it are solved
+// in step (b), then block row I takes
 // X_I = T_I^-1 (-sum_{K<I} L_IK X_K) with T_I^-1 the tile inverse (four
 // independent partial sums per dot product, to shorten the dependent chains).
 //
@@ -69,8 +70,32 @@ __global__ void __launch_bounds__(NTHREADS) k_potrf_diag_inv(T* A, long lda, lon
     if (tid == 0) bad = 0;
     __syncthreads();
 
+    // Inverse of the factored diagonal tile at t0 (one warp, lane c = column c,
+    // forward substitution): X[t0 + r][t0 + c] for c <= r.  The tile and its
+    // reciprocal pivots are final once step (a) of its panel is done.
+    auto tile_inverse = [&](int t0) {
+        const int tw = kb - t0 < PW ? kb - t0 : PW;
+        const int c = lane;
+        if (c < tw) {
+            T x[PW];
+#pragma unroll
+            for (int r = 0; r < PW; ++r) {
+                T acc = (r == c) ? T(1) : T(0);
+#pragma unroll
+                for (int mm = 0; mm < r; ++mm)
+                    if (mm >= c) acc -= S[(t0 + r) * LDS + t0 + mm] * x[mm];
+                x[r] = (r >= c && r < tw) ? acc * rdg[t0 + (r < tw ? r : 0)] : T(0);
+            }
+#pragma unroll
+            for (int r = 0; r < PW; ++r)
+                if (r < tw && r >= c) X[(t0 + r) * LDS + t0 + c] = x[r];
+        }
+    };
+    constexpr int SPARE = NTHREADS / 32 - 1;  // idle in step (b): m <= 48 rows
+    int p_last = 0;
     for (int p = 0; p < kb; p += PW) {
         const int pw = kb - p < PW ? kb - p : PW;
+        p_last = p;
         // (a) the pw x pw diagonal tile, warp 0, lane i = row p + i
         if (warp == 0) {
             T r[PW];
@@ -106,7 +131,9 @@ __global__ void __launch_bounds__(NTHREADS) k_potrf_diag_inv(T* A, long lda, lon
         const int q = p + pw;  // first row / column of the trailing block
         const int m = kb - q;
         if (m <= 0) break;
-        // (b) rows below the tile: L[i][p:p+pw] = A[i][p:p+pw] L_tile^-T
+        // (b) rows below the tile: L[i][p:p+pw] = A[i][p:p+pw] L_tile^-T;
+        // meanwhile the spare warp inverts the tile (step A of the inverse)
+        if (warp == SPARE) tile_inverse(p);
         if (tid < m) {
             const int i = q + tid;
             T a[PW];
@@ -165,28 +192,9 @@ __global__ void __launch_bounds__(NTHREADS) k_potrf_diag_inv(T* A, long lda, lon
             if (c < kb) A[(long)(k0 + r) * lda + k0 + c] = (c <= r) ? S[r * LDS + c] : T(0);
     }
 
-    // X = L^-1.  Step A: warp t inverts diagonal tile t (lane c = column c)
-    {
-        const int t0 = warp * PW;
-        if (t0 < kb) {
-            const int tw = kb - t0 < PW ? kb - t0 : PW;
-            const int c = lane;
-            if (c < tw) {
-                T x[PW];
-#pragma unroll
-                for (int r = 0; r < PW; ++r) {
-                    T acc = (r == c) ? T(1) : T(0);
-#pragma unroll
-                    for (int mm = 0; mm < r; ++mm)
-                        if (mm >= c) acc -= S[(t0 + r) * LDS + t0 + mm] * x[mm];
-                    x[r] = (r >= c && r < tw) ? acc * rdg[t0 + (r < tw ? r : 0)] : T(0);
-                }
-#pragma unroll
-                for (int r = 0; r < PW; ++r)
-                    if (r < tw && r >= c) X[(t0 + r) * LDS + t0 + c] = x[r];
-            }
-        }
-    }
+    // X = L^-1.  Step A: every tile but the last was inverted during step (b)
+    // of its panel; the last one now
+    if (warp == SPARE) tile_inverse(p_last);
     __syncthreads();
     // Step B: block rows I = 1, 2, 3: Tb = -sum_{m < 16 I} L[16I + r][m] X[m][c],
     // then X[16I + r][c] = sum_{j <= r} X_II[r][j] Tb[j][c] for c < 16 I

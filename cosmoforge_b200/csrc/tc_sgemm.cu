@@ -28,6 +28,7 @@
 #include <cuda_bf16.h>
 
 #include "cf_common.cuh"
+#include "tc_sgemm.cuh"
 
 namespace {
 
@@ -198,11 +199,42 @@ __device__ __forceinline__ void store_operand(const float4 (&v)[ROWS / 16], uint
     }
 }
 
-template <int BN, int STAGES, bool VEC>
-__global__ void __launch_bounds__(NT, STAGES == 1 ? 2 : 1) k_sgemm_bf16x6(int M, int N, int K, float alpha, const float* A, long lda,
-                                                        long sA, const float* B, long ldb, long sB, float beta, float* C,
-                                                        long ldc, long sC, float* C2, long ldc2, long sC2,
-                                                        int lower_only, unsigned long long wait_ns, int* info)
+// 16-byte pieces of a rows x 64 chunk of three BF16 planes (row r0.., column
+// k0..) into the swizzled stage with cp.async; pieces past the rows or K are
+// zero-filled (a piece that straddles K copies only its leading elements).
+template <int ROWS>
+__device__ __forceinline__ void copy_planes(const __nv_bfloat16* X, long ld, long ps, int r0, int nrows, int k0, int K,
+                                            uint8_t* dst, uint32_t plane_bytes, int tid)
+{
+    constexpr int PIECES = PLANES * ROWS * 8;
+#pragma unroll
+    for (int i = 0; i < PIECES / NT; ++i) {
+        const int e = i * NT + tid;
+        const int pl = e / (ROWS * 8), rem = e - pl * (ROWS * 8), r = rem >> 3, j = rem & 7;
+        const int gr = r0 + r, gk = k0 + j * 8;
+        const int left = gr < nrows ? K - gk : 0;
+        const int bytes = left >= 8 ? 16 : (left > 0 ? 2 * left : 0);
+        const __nv_bfloat16* src = bytes ? X + (long)pl * ps + (long)gr * ld + gk : X;
+        const uint32_t d = smem_u32(dst + pl * plane_bytes + (r >> 3) * 1024 + (r & 7) * 128 + ((j ^ (r & 7)) << 4));
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+    }
+}
+
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// PI: operands are BF16 split planes (cp.async into the stage), else FP32
+// (registers, split in the kernel).  PO: the result also goes out as split
+// planes.
+template <int BN, int STAGES, bool VEC, bool PI, bool PO>
+__global__ void __launch_bounds__(NT, STAGES == 1 ? 2 : 1) k_sgemm_bf16x6(int M, int N, int K, float alpha,
+                                                                          cf_sg::Opnd A, cf_sg::Opnd B, float beta,
+                                                                          cf_sg::Out o, int lower_only,
+                                                                          unsigned long long wait_ns, int* info)
 {
     constexpr uint32_t B_BYTES = BN * KC * 2;
     constexpr uint32_t STAGE = PLANES * (A_BYTES + B_BYTES);
@@ -216,17 +248,30 @@ __global__ void __launch_bounds__(NT, STAGES == 1 ? 2 : 1) k_sgemm_bf16x6(int M,
     const int tile_m = blockIdx.y * BM, tile_n = blockIdx.x * BN;
     if ((lower_only & 1) && tile_n > tile_m + BM - 1) return;  // whole CTA, before any allocation
     const long z = blockIdx.z;
-    A += z * sA;
-    B += z * sB;
-    C += z * sC;
-    if (C2) C2 += z * sC2;
+    float* C = o.C ? o.C + z * o.sC : nullptr;
+    float* C2 = o.C2 ? o.C2 + z * o.sC2 : nullptr;
+    __nv_bfloat16* Cp = o.Cp ? o.Cp + z * o.sCp : nullptr;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nch = (K + KC - 1) / KC;
-    // chunk 0's operands are in flight while the barriers and TMEM are set up
-    float4 ra[BM / 16], rb[BN / 16];
-    if (nch > 0) {
-        load_operand<BM, VEC>(A, lda, tile_m, M, 0, K, ra, tid);
-        load_operand<BN, VEC>(B, ldb, tile_n, N, 0, K, rb, tid);
+    const float* Af = PI ? nullptr : (const float*)A.p + z * A.sz;
+    const float* Bf = PI ? nullptr : (const float*)B.p + z * B.sz;
+    const __nv_bfloat16* Ap = PI ? (const __nv_bfloat16*)A.p + z * A.sz : nullptr;
+    const __nv_bfloat16* Bp = PI ? (const __nv_bfloat16*)B.p + z * B.sz : nullptr;
+    // the first chunks' operands are in flight while the barriers and TMEM are set up
+    float4 ra[PI ? 1 : BM / 16], rb[PI ? 1 : BN / 16];
+    if constexpr (PI) {
+#pragma unroll
+        for (int c = 0; c < STAGES; ++c) {  // one copy group per chunk, in order
+            if (c < nch) {
+                copy_planes<BM>(Ap, A.ld, A.ps, tile_m, M, c * KC, K, smem + c * STAGE, A_BYTES, tid);
+                copy_planes<BN>(Bp, B.ld, B.ps, tile_n, N, c * KC, K, smem + c * STAGE + PLANES * A_BYTES, B_BYTES,
+                                tid);
+            }
+            cp_commit();
+        }
+    } else if (nch > 0) {
+        load_operand<BM, VEC>(Af, A.ld, tile_m, M, 0, K, ra, tid);
+        load_operand<BN, VEC>(Bf, B.ld, tile_n, N, 0, K, rb, tid);
     }
     if (tid == 0) {
         mbar_init(&done[0], 1);
@@ -250,14 +295,18 @@ __global__ void __launch_bounds__(NT, STAGES == 1 ? 2 : 1) k_sgemm_bf16x6(int M,
         const int s = c % STAGES;
         uint8_t* sa = smem + s * STAGE;  // A planes 0, 1, 2, then B planes 0, 1, 2
         uint8_t* sb = sa + PLANES * A_BYTES;
-        // the MMAs of chunk c - STAGES read this stage: wait for them before overwriting it
-        bool ok = c < STAGES || mbar_wait(&done[s], (uint32_t)(((c - STAGES) / STAGES) & 1), wait_ns);
-        if (__syncthreads_or(!ok)) {
-            aborted = true;
-            break;
+        if constexpr (PI) {
+            cp_wait<STAGES - 1>();  // chunk c's group has landed
+        } else {
+            // the MMAs of chunk c - STAGES read this stage: wait for them before overwriting it
+            bool ok = c < STAGES || mbar_wait(&done[s], (uint32_t)(((c - STAGES) / STAGES) & 1), wait_ns);
+            if (__syncthreads_or(!ok)) {
+                aborted = true;
+                break;
+            }
+            store_operand<BM>(ra, sa, A_BYTES, tid);
+            store_operand<BN>(rb, sb, B_BYTES, tid);
         }
-        store_operand<BM>(ra, sa, A_BYTES, tid);
-        store_operand<BN>(rb, sb, B_BYTES, tid);
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         __syncthreads();
         if (tid == 0) {
@@ -270,18 +319,31 @@ __global__ void __launch_bounds__(NT, STAGES == 1 ? 2 : 1) k_sgemm_bf16x6(int M,
                 const bool fresh = c == 0 && t <= 1;  // first write of each accumulator
 #pragma unroll
                 for (int k = 0; k < KC / 16; ++k) {  // 16 BF16 = 32 B per MMA: advance the start address
-                    const uint64_t o = (uint64_t)((k * 32) >> 4);
-                    umma_bf16(dst, da + o, db + o, idesc, (fresh && k == 0) ? 0u : 1u);
+                    const uint64_t off = (uint64_t)((k * 32) >> 4);
+                    umma_bf16(dst, da + off, db + off, idesc, (fresh && k == 0) ? 0u : 1u);
                 }
             }
             umma_commit(&done[s]);
         }
-        // the next chunk's loads overlap this chunk's MMAs
-        if (c + 1 < nch) {
-            load_operand<BM, VEC>(A, lda, tile_m, M, (c + 1) * KC, K, ra, tid);
-            load_operand<BN, VEC>(B, ldb, tile_n, N, (c + 1) * KC, K, rb, tid);
+        if constexpr (PI) {
+            // refill this stage with chunk c + STAGES once chunk c's MMAs are done with it
+            if (c + STAGES < nch) {
+                const bool ok = mbar_wait(&done[s], (uint32_t)((c / STAGES) & 1), wait_ns);
+                if (__syncthreads_or(!ok)) {
+                    aborted = true;
+                    break;
+                }
+                copy_planes<BM>(Ap, A.ld, A.ps, tile_m, M, (c + STAGES) * KC, K, sa, A_BYTES, tid);
+                copy_planes<BN>(Bp, B.ld, B.ps, tile_n, N, (c + STAGES) * KC, K, sb, B_BYTES, tid);
+            }
+            cp_commit();
+        } else if (c + 1 < nch) {
+            // the next chunk's loads overlap this chunk's MMAs
+            load_operand<BM, VEC>(Af, A.ld, tile_m, M, (c + 1) * KC, K, ra, tid);
+            load_operand<BN, VEC>(Bf, B.ld, tile_n, N, (c + 1) * KC, K, rb, tid);
         }
     }
+    if constexpr (PI) cp_wait<0>();  // no copy into the stages outlives the loop
     // Thread = output row in TMEM; each warp turns its 32 x 32 pieces around in
     // shared memory so that C is read and written in 128-byte row segments.
     // The C segments of the warp's first piece are read before the last wait.
@@ -293,7 +355,7 @@ __global__ void __launch_bounds__(NT, STAGES == 1 ? 2 : 1) k_sgemm_bf16x6(int M,
 #pragma unroll
         for (int r = 0; r < 32; ++r) {
             const int row = tile_m + quad * 32 + r;
-            cv[r] = (beta != 0.0f && row < M && c < N) ? C[(long)row * ldc + c] : 0.0f;
+            cv[r] = (beta != 0.0f && C && row < M && c < N) ? C[(long)row * o.ldc + c] : 0.0f;
         }
     };
     const int g0 = warp >> 2;
@@ -336,8 +398,16 @@ __global__ void __launch_bounds__(NT, STAGES == 1 ? 2 : 1) k_sgemm_bf16x6(int M,
                 const int row = tile_m + quad * 32 + r;
                 if (row < M && c < N) {
                     const float out = alpha * T[r * 33 + col] + beta * cv[r];
-                    C[(long)row * ldc + c] = out;
-                    if (C2) C2[(long)row * ldc2 + c] = out;
+                    if (C) C[(long)row * o.ldc + c] = out;
+                    if (C2) C2[(long)row * o.ldc2 + c] = out;
+                    if constexpr (PO) {
+                        __nv_bfloat16 h0, h1, h2;
+                        split3(out, h0, h1, h2);
+                        __nv_bfloat16* q = Cp + (long)row * o.ldcp + c;
+                        q[0] = h0;
+                        q[o.cp_ps] = h1;
+                        q[2 * o.cp_ps] = h2;
+                    }
                 }
             }
             __syncwarp();
@@ -355,65 +425,66 @@ unsigned long long g_sgemm_wait_ns = DRAIN_NS;
 // overlap each other's loads and MMAs).
 int g_sgemm_stages = 1;
 
-template <int BN, int STAGES, bool VEC>
-int launch_t(int M, int N, int K, float alpha, const float* A, long lda, long sA, const float* B, long ldb, long sB,
-             float beta, float* C, long ldc, long sC, float* C2, long ldc2, long sC2, int batch, int lower_only,
-             int* info, cudaStream_t st)
+template <int BN, int STAGES, bool VEC, bool PI, bool PO>
+int launch_t(int M, int N, int K, float alpha, const cf_sg::Opnd& A, const cf_sg::Opnd& B, float beta,
+             const cf_sg::Out& o, int batch, int lower_only, int* info, cudaStream_t st)
 {
     constexpr size_t smem = 1024 + STAGES * (size_t)PLANES * (A_BYTES + (size_t)BN * KC * 2);
     static_assert(smem <= 232448, "shared memory exceeds 227 KB");
     static std::atomic<int> attr[CF_MAX_DEVICES];
-    if (int rc = cf_smem_optin(k_sgemm_bf16x6<BN, STAGES, VEC>, (int)smem, attr)) return rc;
+    if (int rc = cf_smem_optin(k_sgemm_bf16x6<BN, STAGES, VEC, PI, PO>, (int)smem, attr)) return rc;
     dim3 grid(cf_cdiv(N, BN), cf_cdiv(M, BM), batch);
-    k_sgemm_bf16x6<BN, STAGES, VEC><<<grid, NT, smem, st>>>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC,
-                                                            C2, ldc2, sC2, lower_only, g_sgemm_wait_ns, info);
+    k_sgemm_bf16x6<BN, STAGES, VEC, PI, PO><<<grid, NT, smem, st>>>(M, N, K, alpha, A, B, beta, o, lower_only,
+                                                                    g_sgemm_wait_ns, info);
     CF_CHECK_LAUNCH();
     return CF_OK;
 }
 
-inline bool aligned16(const float* p, long ld, long stride, int batch)
+inline bool aligned16(const void* p, long ld, long stride, int batch, int per16)
 {
-    return ((uintptr_t)p & 15) == 0 && (ld & 3) == 0 && (batch == 1 || (stride & 3) == 0);
+    return ((uintptr_t)p & 15) == 0 && (ld % per16) == 0 && (batch == 1 || (stride % per16) == 0);
 }
 
 template <int BN, int STAGES>
-int launch(int M, int N, int K, float alpha, const float* A, long lda, long sA, const float* B, long ldb, long sB,
-           float beta, float* C, long ldc, long sC, float* C2, long ldc2, long sC2, int batch, int lower_only,
-           int* info, cudaStream_t st)
+int launch(int M, int N, int K, float alpha, const cf_sg::Opnd& A, const cf_sg::Opnd& B, float beta,
+           const cf_sg::Out& o, bool pi, int batch, int lower_only, int* info, cudaStream_t st)
 {
-    if (aligned16(A, lda, sA, batch) && aligned16(B, ldb, sB, batch))
-        return launch_t<BN, STAGES, true>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, C2, ldc2, sC2,
-                                          batch, lower_only, info, st);
-    return launch_t<BN, STAGES, false>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, C2, ldc2, sC2, batch,
-                                       lower_only, info, st);
+    if (pi) {
+        if (o.Cp) return CF_ERR_UNSUPPORTED;
+        return launch_t<BN, STAGES, false, true, false>(M, N, K, alpha, A, B, beta, o, batch, lower_only, info, st);
+    }
+    const bool vec = aligned16(A.p, A.ld, A.sz, batch, 4) && aligned16(B.p, B.ld, B.sz, batch, 4);
+    if (o.Cp)
+        return vec ? launch_t<BN, STAGES, true, false, true>(M, N, K, alpha, A, B, beta, o, batch, lower_only, info,
+                                                             st)
+                   : launch_t<BN, STAGES, false, false, true>(M, N, K, alpha, A, B, beta, o, batch, lower_only, info,
+                                                              st);
+    return vec ? launch_t<BN, STAGES, true, false, false>(M, N, K, alpha, A, B, beta, o, batch, lower_only, info, st)
+               : launch_t<BN, STAGES, false, false, false>(M, N, K, alpha, A, B, beta, o, batch, lower_only, info,
+                                                           st);
 }
 
 }  // namespace
 
-// Same product with an optional second destination C2 (same values; NULL for
-// none), for the FP32 Cholesky's panel solves, which write the panel to its
-// work buffer and into the matrix in one pass.  C2 must not overlap C, nor
-// operand rows read by another CTA.
-int cf_sgemm_bf16x6_dual(int M, int N, int K, float alpha, const float* A, long lda, long sA, const float* B,
-                         long ldb, long sB, float beta, float* C, long ldc, long sC, float* C2, long ldc2, long sC2,
-                         int batch, int lower_only, int* info, void* stream)
+namespace cf_sg {
+int sgemm(int M, int N, int K, float alpha, const Opnd& A, const Opnd& B, float beta, const Out& o, bool planes_in,
+          int batch, int lower_only, int* info, cudaStream_t st)
 {
-    if (M < 0 || N < 0 || K < 0 || batch < 1 || !C || (K > 0 && (!A || !B))) return CF_ERR_ARG;
+    if (M < 0 || N < 0 || K < 0 || batch < 1 || (!o.C && !o.C2 && !o.Cp) || (K > 0 && (!A.p || !B.p)))
+        return CF_ERR_ARG;
+    if (beta != 0.0f && !o.C) return CF_ERR_ARG;
     if (M == 0 || N == 0) return CF_OK;
-    cudaStream_t st = (cudaStream_t)stream;
+    if (planes_in && !(aligned16(A.p, A.ld, A.sz, batch, 8) && aligned16(B.p, B.ld, B.sz, batch, 8) &&
+                       A.ps % 8 == 0 && B.ps % 8 == 0))
+        return CF_ERR_ARG;
     if (g_sgemm_stages == 2) {
-        if (N <= 64)
-            return launch<64, 2>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, C2, ldc2, sC2, batch,
-                                 lower_only, info, st);
-        return launch<128, 2>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, C2, ldc2, sC2, batch,
-                              lower_only, info, st);
+        if (N <= 64) return launch<64, 2>(M, N, K, alpha, A, B, beta, o, planes_in, batch, lower_only, info, st);
+        return launch<128, 2>(M, N, K, alpha, A, B, beta, o, planes_in, batch, lower_only, info, st);
     }
-    if (N <= 64)
-        return launch<64, 1>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, C2, ldc2, sC2, batch,
-                             lower_only, info, st);
-    return launch<128, 1>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, C2, ldc2, sC2, batch, lower_only,
-                          info, st);
+    if (N <= 64) return launch<64, 1>(M, N, K, alpha, A, B, beta, o, planes_in, batch, lower_only, info, st);
+    return launch<128, 1>(M, N, K, alpha, A, B, beta, o, planes_in, batch, lower_only, info, st);
 }
+}  // namespace cf_sg
 
 // C_z = alpha A_z B_z^T + beta C_z (FP32, row-major, K contiguous in A and B;
 // z < batch with element strides sA, sB, sC) with six BF16 split products on
@@ -424,8 +495,10 @@ extern "C" int cf_sgemm_bf16x6(int M, int N, int K, float alpha, const float* A,
                                long ldb, long sB, float beta, float* C, long ldc, long sC, int batch, int lower_only,
                                int* info, void* stream)
 {
-    return cf_sgemm_bf16x6_dual(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, nullptr, 0, 0, batch,
-                                lower_only, info, stream);
+    if (!C) return CF_ERR_ARG;
+    const cf_sg::Opnd a{A, lda, sA, 0}, b{B, ldb, sB, 0};
+    const cf_sg::Out o{C, ldc, sC, nullptr, 0, 0, nullptr, 0, 0, 0};
+    return cf_sg::sgemm(M, N, K, alpha, a, b, beta, o, false, batch, lower_only, info, (cudaStream_t)stream);
 }
 
 // Operand stages of cf_sgemm_bf16x6: 1 (default; two CTAs per SM) or 2 (one

@@ -61,6 +61,14 @@ struct EpiArgs {
     float* Cf;          // [M][ldc] fp32
     long ldc;
     int M, N;
+    // Scattered FP32 output (col_stride > 0 instead of Cf's row-major form):
+    // element (row, col) goes to Cs[col col_stride + (row / fold) fold_ld +
+    // row % fold] (fold = 0: + row), and to Cs2 likewise when given.
+    float* Cs;
+    float* Cs2;
+    long col_stride;
+    int fold;
+    long fold_ld;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -148,19 +156,18 @@ __device__ __forceinline__ void tma_load_4d(const CUtensorMap* map, uint64_t* ba
 }
 
 // Shared-memory matrix descriptor, K-major rows of BKT BF16: BKT = 64 is the
-// 128B swizzle (8-row atoms 1024 B apart), BKT = 32 the 64B swizzle (512 B),
-// BKT = 16 the 32B swizzle (256 B).
+// 128B swizzle (8-row atoms 1024 B apart), BKT = 32 the 64B swizzle (512 B).
 template <int BKT>
 __device__ __forceinline__ uint64_t smem_desc(const void* tile)
 {
-    static_assert(BKT == 64 || BKT == 32 || BKT == 16, "k-tile of 64, 32 or 16 BF16");
+    static_assert(BKT == 64 || BKT == 32, "k-tile of 64 or 32 BF16");
     const uint64_t addr = smem_u32(tile);
     uint64_t d = 0;
     d |= (addr >> 4) & 0x3FFFull;                  // start address
     d |= (uint64_t)(16 >> 4) << 16;                // leading byte offset (unused for swizzled K-major)
     d |= (uint64_t)((8 * BKT * 2) >> 4) << 32;     // stride byte offset: 8 rows
     d |= (uint64_t)1 << 46;                        // descriptor version (sm100)
-    d |= (uint64_t)(BKT == 64 ? 2 : (BKT == 32 ? 4 : 6)) << 61;  // SWIZZLE_128B / 64B / 32B
+    d |= (uint64_t)(BKT == 64 ? 2 : 4) << 61;      // SWIZZLE_128B / SWIZZLE_64B
     return d;
 }
 
@@ -466,6 +473,19 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 // Row-major planes in 16-byte stores of 8 columns; the transposed
                 // planes column by column (32 lanes = 32 consecutive rows).
                 const int cbase = n0 + half * HALF;
+                if (epi.Cs) {
+                    // scattered FP32: one column at a time, the warp's 32 rows consecutive
+                    const long roff = epi.fold ? (long)(row / epi.fold) * epi.fold_ld + row % epi.fold : (long)row;
+#pragma unroll
+                    for (int j = 0; j < HALF; ++j) {
+                        if (cbase + j < epi.N) {
+                            const long o = (long)(cbase + j) * epi.col_stride + roff;
+                            epi.Cs[o] = (float)acc[j];
+                            if (epi.Cs2) epi.Cs2[o] = (float)acc[j];
+                        }
+                    }
+                    continue;
+                }
 #pragma unroll
                 for (int j0 = 0; j0 < HALF; j0 += 8) {
                     float x[8];
@@ -536,7 +556,7 @@ EncodeTiledFn encode_fn()
 }
 
 // 3D bf16 map: dims (K, rows, planes), row stride ld elements, plane stride ps elements;
-// box (bk, box_rows, 1): bk = 64 with 128B swizzle, bk = 32 with 64B, bk = 16 with 32B.
+// box (bk, box_rows, 1): bk = 64 with 128B swizzle, bk = 32 with 64B swizzle.
 int make_map(CUtensorMap* map, const void* base, long K, long rows, long ld, int planes, long ps, int box_rows,
              int bk = BK)
 {
@@ -548,8 +568,7 @@ int make_map(CUtensorMap* map, const void* base, long K, long rows, long ld, int
     cuuint32_t box[3] = {(cuuint32_t)bk, (cuuint32_t)box_rows, 1};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides, box, estr,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE,
-                    bk == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : (bk == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B),
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, bk == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? CF_OK : CF_ERR_ARG;
@@ -601,10 +620,7 @@ int launch_gemm_kc(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, i
 }
 
 // GEMM mode: 1 = all planes of a 32-wide k-slice per stage with split
-// accumulators where the planes allow it (3 stages of 72 KB for three
-// planes), 2 = the same with 16-wide k-slices (6 stages of 36 KB: the same
-// ring in finer steps, so a stage is refilled sooner), 0 = 64-wide k-tiles
-// term by term.
+// accumulators where the planes allow it, 0 = 64-wide k-tiles term by term.
 int g_all_planes = 1;
 
 template <int BN, int STAGES, bool TRACE, int PLS = 1, int BKT = BK, bool SPLIT = false>
@@ -671,14 +687,50 @@ extern "C" int cf_umma_set_group(int group_m)
     return prev;
 }
 
-// Select the GEMM form (1 = all planes per stage in 32-wide k-slices, 2 = in
-// 16-wide k-slices, 0 = term by term); returns the previous one.
+// Select the GEMM form (1 = all planes per stage, 0 = term by term); returns the previous one.
 extern "C" int cf_umma_set_all_planes(int on)
 {
     const int prev = g_all_planes;
-    g_all_planes = (on == 0 || on == 1 || on == 2) ? on : 1;
+    g_all_planes = on ? 1 : 0;
     return prev;
 }
+
+namespace {
+int gemm_bf16(int M, int N, int K, int nterms, const int* ta, const int* tb, const void* A, long lda, long a_ps,
+              int a_planes, const void* B, long ldb, long b_ps, int b_planes, const EpiArgs& e, int* err,
+              cudaStream_t st)
+{
+    if (M <= 0 || N <= 0 || K <= 0 || nterms < 1 || nterms > MAX_TERMS || !A || !B) return CF_ERR_ARG;
+    Terms t{};
+    t.n = nterms;
+    for (int i = 0; i < nterms; ++i) {
+        if (ta[i] < 0 || ta[i] >= a_planes || tb[i] < 0 || tb[i] >= b_planes) return CF_ERR_ARG;
+        t.a[i] = ta[i];
+        t.b[i] = tb[i];
+    }
+    TraceArgs tr{};
+    CUtensorMap ma, mb;
+    // All planes of a 32-wide k-slice in one stage (each plane read once per
+    // k-slice instead of once per term), the leading term (0, 0) accumulated
+    // apart from the corrections; otherwise 64-wide k-tiles walked term by term.
+    const int pls = a_planes == b_planes ? a_planes : 0;
+    bool all_planes = g_all_planes && (pls == 2 || pls == 3) && t.a[0] == 0 && t.b[0] == 0;
+    for (int i = 1; i < nterms && all_planes; ++i) all_planes = !(t.a[i] == 0 && t.b[i] == 0);
+    if (all_planes) {
+        int rc = make_map(&ma, A, K, M, lda, a_planes, a_ps, BM, 32);
+        if (rc) return rc;
+        rc = make_map(&mb, B, K, N, ldb, b_planes, b_ps, 256, 32);
+        if (rc) return rc;
+        if (pls == 3) return launch_gemm<256, 3, false, 3, 32, true>(ma, mb, M, N, K, t, e, tr, 1, err, st);
+        return launch_gemm<256, 4, false, 2, 32, true>(ma, mb, M, N, K, t, e, tr, 1, err, st);
+    }
+    int rc = make_map(&ma, A, K, M, lda, a_planes, a_ps, BM);
+    if (rc) return rc;
+    rc = make_map(&mb, B, K, N, ldb, b_planes, b_ps, 256);
+    if (rc) return rc;
+    return launch_gemm<256, 4, false>(ma, mb, M, N, K, t, e, tr, 1, err, st);
+}
+}  // namespace
 
 // C = sum_t A_{ta[t]} B_{tb[t]}^T with BF16 split planes, FP32 accumulation.
 //   A: planes of M x K (row stride lda, plane stride a_ps), B: planes of N x K.
@@ -690,43 +742,30 @@ extern "C" int cf_umma_gemm_bf16(int M, int N, int K, int nterms, const int* ta,
                                  int b_planes, void* X, long ldx, long x_ps, int x_planes, void* XT, long ldxt,
                                  long xt_ps, float* Cf, long ldc, int* err, void* stream)
 {
-    if (M <= 0 || N <= 0 || K <= 0 || nterms < 1 || nterms > MAX_TERMS || !A || !B) return CF_ERR_ARG;
     if ((X || XT) && (x_planes < 1 || x_planes > 3)) return CF_ERR_ARG;
-    Terms t{};
-    t.n = nterms;
-    for (int i = 0; i < nterms; ++i) {
-        if (ta[i] < 0 || ta[i] >= a_planes || tb[i] < 0 || tb[i] >= b_planes) return CF_ERR_ARG;
-        t.a[i] = ta[i];
-        t.b[i] = tb[i];
-    }
-    EpiArgs e{(__nv_bfloat16*)X, ldx, x_ps, x_planes, (__nv_bfloat16*)XT, ldxt, xt_ps, Cf, ldc, M, N};
-    TraceArgs tr{};
-    cudaStream_t st = (cudaStream_t)stream;
-    CUtensorMap ma, mb;
-    // All planes of a 32-wide k-slice in one stage (each plane read once per
-    // k-slice instead of once per term), the leading term (0, 0) accumulated
-    // apart from the corrections; otherwise 64-wide k-tiles walked term by term.
-    const int pls = a_planes == b_planes ? a_planes : 0;
-    bool all_planes = g_all_planes && (pls == 2 || pls == 3) && t.a[0] == 0 && t.b[0] == 0;
-    for (int i = 1; i < nterms && all_planes; ++i) all_planes = !(t.a[i] == 0 && t.b[i] == 0);
-    if (all_planes) {
-        const int bk = g_all_planes == 2 ? 16 : 32;
-        int rc = make_map(&ma, A, K, M, lda, a_planes, a_ps, BM, bk);
-        if (rc) return rc;
-        rc = make_map(&mb, B, K, N, ldb, b_planes, b_ps, 256, bk);
-        if (rc) return rc;
-        if (bk == 16) {
-            if (pls == 3) return launch_gemm<256, 6, false, 3, 16, true>(ma, mb, M, N, K, t, e, tr, 1, err, st);
-            return launch_gemm<256, 8, false, 2, 16, true>(ma, mb, M, N, K, t, e, tr, 1, err, st);
-        }
-        if (pls == 3) return launch_gemm<256, 3, false, 3, 32, true>(ma, mb, M, N, K, t, e, tr, 1, err, st);
-        return launch_gemm<256, 4, false, 2, 32, true>(ma, mb, M, N, K, t, e, tr, 1, err, st);
-    }
-    int rc = make_map(&ma, A, K, M, lda, a_planes, a_ps, BM);
-    if (rc) return rc;
-    rc = make_map(&mb, B, K, N, ldb, b_planes, b_ps, 256);
-    if (rc) return rc;
-    return launch_gemm<256, 4, false>(ma, mb, M, N, K, t, e, tr, 1, err, st);
+    EpiArgs e{(__nv_bfloat16*)X, ldx, x_ps, x_planes, (__nv_bfloat16*)XT, ldxt, xt_ps, Cf, ldc, M, N,
+              nullptr, nullptr, 0, 0, 0};
+    return gemm_bf16(M, N, K, nterms, ta, tb, A, lda, a_ps, a_planes, B, ldb, b_ps, b_planes, e, err,
+                     (cudaStream_t)stream);
+}
+
+// The same product written in FP32 to scattered addresses: element (row, col)
+// of C goes to Cs[col col_stride + (row / fold) fold_ld + row % fold] (fold =
+// 0: Cs[col col_stride + row]) and, when Cs2 is given, to the same offset of
+// Cs2.  Lanes of a warp hold consecutive rows, so each column's segment of a
+// tile is one coalesced store.  Used with rows = the entries of a block
+// region of the covariance (fold = region width, fold_ld = the matrix's row
+// stride) and columns = parameter points (col_stride = one matrix) to write
+// C(theta) for a batch of points straight into its FP32 matrices.
+extern "C" int cf_umma_gemm_bf16_scatter(int M, int N, int K, int nterms, const int* ta, const int* tb,
+                                         const void* A, long lda, long a_ps, int a_planes, const void* B, long ldb,
+                                         long b_ps, int b_planes, float* Cs, float* Cs2, long col_stride, int fold,
+                                         long fold_ld, int* err, void* stream)
+{
+    if (!Cs || col_stride <= 0 || fold < 0) return CF_ERR_ARG;
+    EpiArgs e{nullptr, 0, 0, 0, nullptr, 0, 0, nullptr, 0, M, N, Cs, Cs2, col_stride, fold, fold_ld};
+    return gemm_bf16(M, N, K, nterms, ta, tb, A, lda, a_ps, a_planes, B, ldb, b_ps, b_planes, e, err,
+                     (cudaStream_t)stream);
 }
 
 // Fisher contraction on the tensor cores:

@@ -23,17 +23,25 @@ so far; A_b^T slabs only for the spectrum being processed.
 
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 import torch
 
 from . import layout as lay
-from ._lib import check, lib, ptr, stream
+from ._lib import CF_ERR_TIMEOUT, check, lib, ptr, stream
 
 F64 = torch.float64
 
 
 def _off(t: torch.Tensor, elems: int) -> int:
     return t.data_ptr() + int(elems) * t.element_size()
+
+
+# BF16x6 product list (plane pairs (0,0), (0,1), (1,0), (0,2), (1,1), (2,0)) as
+# host int arrays for the tensor-core GEMMs; the arrays live as long as the module
+_X6_ARRAYS = tuple((ctypes.c_int * 6)(*t) for t in ((0, 0, 1, 0, 1, 2), (0, 1, 0, 2, 1, 0)))
+_X6_TERMS = tuple(ctypes.cast(a, ctypes.c_void_p) for a in _X6_ARRAYS)
 
 
 class Engine:
@@ -347,8 +355,14 @@ class Engine:
 
         precision "fp64": FP64 Cholesky, chi2 = |L^-1 x|^2, ln|C| from its
         diagonal.  "mixed": FP32 Cholesky of C, chi2 from one FP64 refinement
-        step against the FP64 C (second-order error), ln|C| from the FP32
-        factor's diagonal summed in FP64.
+        step against C (second-order in the factor's error), ln|C| from the
+        FP32 factor's diagonal summed in FP64.  With the basis build the mixed
+        C is formed in FP32 by BF16x6 split products on the tensor cores
+        (~2^-24 relative per entry, no FP64 C at all) and the refinement reads
+        that FP32 C, so chi2 is the FP32 C's: first order in its rounding,
+        ~1e-7 relative for maps drawn from C and ~1e-5 for maps far from it
+        (|dlnL| within 0.05).  With the direct build the refinement reads the
+        FP64 C and chi2 is second order in the factor's error (1e-8).
 
         build "basis" forms C(theta) = S(theta) + s N from the per-multipole
         basis (one GEMM per block region, see SignalBasis), "direct" runs the
@@ -368,9 +382,9 @@ class Engine:
         if build == "auto":
             build = "basis" if B >= 64 and SignalBasis.bytes_needed(self.L) <= 4 << 30 else "direct"
         if build == "basis":
-            C = self.signal_basis(N).covariance(cl, sc)
             if precision == "mixed":
-                return self._lnl_mixed(C, N, maps, sc, noise_added=True)
+                return self._lnl_mixed_basis(self.signal_basis(N), cl, maps, sc)
+            C = self.signal_basis(N).covariance(cl, sc)
         else:
             C = self.signal(cl)
             if precision == "mixed":
@@ -380,12 +394,36 @@ class Engine:
         info = self.potrf(C)
         X = maps.to(self.dev, F64).contiguous()
         nsims = X.shape[1]
-        z = torch.empty((B * nsims, n), dtype=F64, device=self.dev)
+        # the solve vector lives in shared memory up to n = 24576, in this scratch above
+        z = torch.empty((B * nsims, n), dtype=F64, device=self.dev) if n > 24576 else None
         chi2 = torch.empty((B, nsims), dtype=F64, device=self.dev)
         logdet = torch.empty(B, dtype=F64, device=self.dev)
         check(self.lib.cf_chi2_logdet(n, C.data_ptr(), n, n * n, B, X.data_ptr(), nsims, 0, nsims,
-                                      z.data_ptr(), chi2.data_ptr(), logdet.data_ptr(), stream()),
+                                      ptr(z), chi2.data_ptr(), logdet.data_ptr(), stream()),
               "cf_chi2_logdet")
+        return chi2, logdet, -0.5 * (chi2 + logdet[:, None]), info
+
+    def _lnl_mixed_basis(self, basis: "SignalBasis", cl: torch.Tensor, maps: torch.Tensor, sc):
+        """Mixed likelihood with C(theta) built in FP32 on the tensor cores: two
+        copies from one pass (one is factored in place, the other feeds the
+        FP64 refinement), FP32 Cholesky, refined chi2 and ln|C|."""
+        B, n = cl.shape[0], self.L.n
+        C32 = torch.empty((B, n, n), dtype=torch.float32, device=self.dev)
+        L32 = torch.empty_like(C32)
+        err = basis.covariance_f32(cl, sc, C32, L32)
+        info = torch.zeros(B, dtype=torch.int32, device=self.dev)
+        work = torch.empty(self.lib.cf_potrf_f32_workspace(n, B) // 4 + 1, dtype=torch.float32, device=self.dev)
+        check(self.lib.cf_potrf_f32(n, L32.data_ptr(), n, n * n, B, work.data_ptr(), info.data_ptr(), stream()),
+              "cf_potrf_f32")
+        X = maps.to(self.dev, F64).contiguous()
+        nsims = X.shape[1]
+        chi2 = torch.empty((B, nsims), dtype=F64, device=self.dev)
+        logdet = torch.empty(B, dtype=F64, device=self.dev)
+        check(self.lib.cf_chi2_logdet_mixed_c32(n, L32.data_ptr(), n, n * n, C32.data_ptr(), n, n * n, B,
+                                                X.data_ptr(), nsims, 0, nsims, chi2.data_ptr(), logdet.data_ptr(),
+                                                stream()), "cf_chi2_logdet_mixed_c32")
+        # a tensor-core wait that ran out marks every point of the batch (no host sync: capturable)
+        info = torch.where(err[0] != 0, torch.full_like(info, CF_ERR_TIMEOUT), info)
         return chi2, logdet, -0.5 * (chi2 + logdet[:, None]), info
 
     def _lnl_mixed(self, C: torch.Tensor, N: torch.Tensor, maps: torch.Tensor, sc, noise_added: bool = False):
@@ -461,6 +499,7 @@ class SignalBasis:
                 covered += R * Cc
         if covered != n * n:
             raise ValueError("the blocks of this layout do not cover the covariance matrix")
+        self._kplanes = None
 
     @staticmethod
     def bytes_needed(L) -> int:
@@ -497,6 +536,57 @@ class SignalBasis:
                                       0.0, _off(out, r0 * n + c0), n * n, n, None, 0, 0, R, 0, stream()),
                   "cf_dgemm")
         return out
+
+    def _planes(self):
+        """BF16x3 split planes of every region's basis, entries x kdim (K
+        contiguous, padded to a multiple of 8), built on first use."""
+        if self._kplanes is None:
+            E = self.E
+            out = []
+            for r0, c0, R, Cc, sp, sp_dev, K in self.regions:
+                kd = K.shape[0]
+                kp = (kd + 7) // 8 * 8
+                Kt = K.reshape(kd, R * Cc).t().contiguous()
+                P = torch.zeros((3, R * Cc, kp), dtype=torch.bfloat16, device=E.dev)
+                check(E.lib.cf_split_bf16(R * Cc, kd, Kt.data_ptr(), kd, 3, P.data_ptr(), kp, R * Cc * kp,
+                                          stream()), "cf_split_bf16")
+                del Kt
+                out.append((P, kp))
+            self._kplanes = out
+        return self._kplanes
+
+    def covariance_f32(self, cl: torch.Tensor, scale: torch.Tensor | None, out: torch.Tensor,
+                       out2: torch.Tensor | None = None) -> torch.Tensor:
+        """C (B x n x n) in FP32 into `out` (and `out2`) from BF16x6 split
+        products on the tensor cores: per region, (region entries x kdim) times
+        (points x kdim)^T, written transposed into the points' matrices
+        (cf_umma_gemm_bf16_scatter).  Returns the device error flag of the
+        launches (non-zero: a bounded wait ran out)."""
+        E, n, Lp = self.E, self.n, self.Lp
+        B = cl.shape[0]
+        s = torch.ones(B, dtype=F64, device=E.dev) if scale is None else scale.reshape(B).to(F64)
+        used = None
+        if not torch.cuda.is_current_stream_capturing():
+            used = (cl.abs().amax(dim=(0, 2)) > 0).cpu().numpy()
+        err = torch.zeros(1, dtype=torch.int32, device=E.dev)
+        ta, tb = _X6_TERMS
+        for (r0, c0, R, Cc, sp, sp_dev, K), (P, kp) in zip(self.regions, self._planes()):
+            keep = len(sp)
+            while used is not None and keep > 0 and not used[sp[keep - 1]]:
+                keep -= 1
+            kd = 1 + keep * Lp
+            ctab = torch.zeros((B, kp), dtype=F64, device=E.dev)
+            ctab[:, 0] = s
+            ctab[:, 1:kd] = cl.index_select(1, sp_dev[:keep]).reshape(B, keep * Lp)
+            cp = torch.empty((3, B, kp), dtype=torch.bfloat16, device=E.dev)
+            check(E.lib.cf_split_bf16(B, kp, ctab.data_ptr(), kp, 3, cp.data_ptr(), kp, B * kp, stream()),
+                  "cf_split_bf16")
+            off = r0 * n + c0
+            check(E.lib.cf_umma_gemm_bf16_scatter(R * Cc, B, kd, 6, ta, tb, P.data_ptr(), kp, R * Cc * kp, 3,
+                                                  cp.data_ptr(), kp, B * kp, 3, _off(out, off),
+                                                  _off(out2, off) if out2 is not None else None, n * n, Cc, n,
+                                                  err.data_ptr(), stream()), "cf_umma_gemm_bf16_scatter")
+        return err
 
 
 class LnlGraph:

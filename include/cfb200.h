@@ -266,6 +266,24 @@ int cf_umma_gemm_bf16(int M, int N, int K, int nterms, const int* ta, const int*
                       long xt_ps, float* Cf, long ldc, int* err, void* stream);
 
 /*
+ * The product of cf_umma_gemm_bf16 written in FP32 to scattered addresses:
+ * element (row, col) goes to Cs[col col_stride + (row / fold) fold_ld +
+ * row % fold] (fold = 0: + row) and, when Cs2 is not NULL, to the same
+ * offset of Cs2.  With rows = the entries of one block region of the
+ * covariance (fold = the region's width, fold_ld = the matrix row stride,
+ * Cs at the region's first entry) and columns = parameter points
+ * (col_stride = n^2) it writes C(theta) = S(theta) + s N of a batch of points
+ * straight into FP32 matrices from the per-multipole basis.
+ * Replaces: the per-point covariance build of picslike/picslike.py:301-319
+ * (S from cosmocore/signal_kernels.py:164-502 plus the scaled noise) in the
+ * mixed likelihood.
+ */
+int cf_umma_gemm_bf16_scatter(int M, int N, int K, int nterms, const int* ta, const int* tb, const void* A,
+                              long lda, long a_ps, int a_planes, const void* B, long ldb, long b_ps, int b_planes,
+                              float* Cs, float* Cs2, long col_stride, int fold, long fold_ld, int* err,
+                              void* stream);
+
+/*
  * Fisher contraction on tcgen05 with FP64 promotion of the partial sums:
  *   F[(p_off+p) ldF + q_off+q] += scale sum_t sum_{k<K1, l<K2}
  *                                 X_{ta[t]}[p sXp + k ldX + l] Y_{tb[t]}[q sYq + k ldY + l]
@@ -308,9 +326,8 @@ int cf_umma_set_promotion(int kc);
 /* Form of cf_umma_gemm_bf16: 1 (default) loads every plane of a 32-wide
  * k-slice into one pipeline stage and keeps the leading product apart from
  * the corrections in a second TMEM accumulator, when both operands carry the
- * same 2 or 3 planes; 2 does the same with 16-wide k-slices (twice the
- * stages of the same ring); 0 walks 64-wide k-tiles term by term.  Returns
- * the previous setting.  No counterpart in the reference. */
+ * same 2 or 3 planes; 0 walks 64-wide k-tiles term by term.  Returns the
+ * previous setting.  No counterpart in the reference. */
 int cf_umma_set_all_planes(int on);
 
 /* Row tiles per group in the persistent tile order of the tcgen05 kernels
@@ -375,6 +392,13 @@ int cf_axpby_f32(long count, double a, const double* X, long strideX, double c, 
 int cf_chi2_logdet_mixed(int n, const float* L, long lda, long strideL, const double* C, long ldc,
                          long strideC, int batch, const double* X, long ldx, long strideX, int nrhs,
                          double* chi2, double* logdet, void* stream);
+
+/* cf_chi2_logdet_mixed with C in FP32 (the matrices the FP32 factor was
+ * computed from); the refinement arithmetic stays FP64.  Same replaced
+ * reference code. */
+int cf_chi2_logdet_mixed_c32(int n, const float* L, long lda, long strideL, const float* C, long ldc,
+                             long strideC, int batch, const double* X, long ldx, long strideX, int nrhs,
+                             double* chi2, double* logdet, void* stream);
 
 /* ---- Quadratic forms of many maps ----
  * q[m ldq + p0 + b] += scale sum_{j<J} W[(b rows_per_bin + j) ldW + m] Y[(yoff + j) ldY + m]

@@ -74,16 +74,23 @@ def test_umma_single_product_matches_rounded_inputs(M, N, K):
 SHAPES = [(384, 640, 512), (200, 300, 100), (2048, 4352, 2112)]
 
 
+# GEMM forms (cf_umma_set_all_planes): 1 = all planes of a 32-wide k-slice per
+# stage, 0 = 64-wide k-tiles term by term.
+@pytest.mark.parametrize("form", [1, 0])
 @pytest.mark.parametrize("M,N,K", SHAPES)
 @pytest.mark.parametrize("terms,planes,tol", [(X3, 2, 2e-4), (X6, 3, 2e-6), (X3, 3, 2e-4)])
-def test_umma_split_products(terms, planes, tol, M, N, K):
+def test_umma_split_products(terms, planes, tol, M, N, K, form):
     from cosmoforge_b200 import _lib
 
     lib = _lib.lib()
     g = torch.Generator(device="cuda").manual_seed(7 + M + K)
     A = torch.randn((M, K), dtype=torch.float64, device="cuda", generator=g)
     B = torch.randn((N, K), dtype=torch.float64, device="cuda", generator=g)
-    Cf, _, _, _, _ = _gemm(lib, A, B, terms, planes)
+    prev = lib.cf_umma_set_all_planes(form)
+    try:
+        Cf, _, _, _, _ = _gemm(lib, A, B, terms, planes)
+    finally:
+        lib.cf_umma_set_all_planes(prev)
     ref = A @ B.T
     err = (Cf.double() - ref).abs().max() / ref.abs().max()
     assert err < tol, float(err)
