@@ -345,15 +345,25 @@ def secondary(args, dev):
         G = engine.LnlGraph(E, N, X, 1024, precision=prec)
         graph_ms[prec], _ = _cuda_ms(torch, lambda: G(cl, s), 3)
         del G
+    # the opt-in tensor-core build of C (FP32 C, refinement against it)
+    ms_tc, r_tc = _cuda_ms(torch, lambda: E.lnl(cl, N, X, noise_scale=s, precision="mixed", build="basis_tc"), 3)
     d = (res["mixed"][1][2] - res["fp64"][1][2]).abs()
+    d_tc = (r_tc[2] - res["fp64"][1][2]).abs()
     lnl = {"workload": "config3_tqu_nside8_lnl", "n_pixels": L.n, "points_per_batch": 1024,
            "fp64_evals_per_s": 1024 / res["fp64"][0] * 1e3, "mixed_evals_per_s": 1024 / res["mixed"][0] * 1e3,
            "fp64_graph_evals_per_s": 1024 / graph_ms["fp64"] * 1e3,
            "mixed_graph_evals_per_s": 1024 / graph_ms["mixed"] * 1e3,
            "mixed_over_fp64": res["fp64"][0] / res["mixed"][0],
            "mixed_max_abs_dlnL": float(d.max()),
-           "build": "C(theta) from the per-multipole basis (one FP64 GEMM per block region)",
-           "mixed_form": "FP32 Cholesky with BF16x6 tensor-core products, FP64-refined chi2"}
+           "mixed_tc_build_evals_per_s": 1024 / ms_tc * 1e3,
+           "mixed_tc_build_over_fp64": res["fp64"][0] / ms_tc,
+           "mixed_tc_build_max_abs_dlnL": float(d_tc.max()),
+           "build": "lower triangle of C(theta) from the per-multipole basis (one FP64 GEMM per block region; "
+                    "mixed: the FP32 copy from the same epilogue); tc build: C in FP32 from BF16x6 tensor-core "
+                    "products",
+           "mixed_form": "FP32 Cholesky (diagonal blocks per CTA, panel solves and narrow updates on a one-tile "
+                         "tcgen05 kernel, trailing updates on the persistent tcgen05 kernel, BF16x6 products), "
+                         "FP64-refined chi2 against the FP64 C"}
     if int(os.environ.get("WORLD_SIZE", "1")) == 1 and not args.no_cpu_baseline:
         from oracle import oracle as orc
 
@@ -747,7 +757,7 @@ def main():
 # --------------------------------------------------------------------------
 KERNEL_DOC = """Single-kernel timing cases (``python bench.py kernel CASE SHAPE``).
 
-    python bench.py kernel umma_gemm M,N,K [--planes 3] [--reps 5] [--kc 16] [--form 1|0]
+    python bench.py kernel umma_gemm M,N,K [--planes 3] [--reps 5] [--kc 16] [--form 1|2|0]
     python bench.py kernel umma_trace P1,P2,K1,K2 [--planes 3]
     python bench.py kernel dgemm M,N,K
     python bench.py kernel spd_inverse N
@@ -961,8 +971,9 @@ def kernel_main(argv=None):
     ap.add_argument("--kc", type=int, default=16, help="promotion interval of the tensor-core kernels")
     ap.add_argument("--splits", type=int, default=0)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed", help="map_solves and lnl")
-    ap.add_argument("--form", type=int, choices=[0, 1], default=1,
-                    help="tensor-core GEMM form: 1 = all planes per 32-wide k-slice, 0 = term by term")
+    ap.add_argument("--form", type=int, choices=[0, 1, 2], default=1,
+                    help="tensor-core GEMM form: 1 = all planes per 32-wide k-slice, 2 = the same on CTA pairs, "
+                         "0 = term by term")
     a = ap.parse_args(argv)
     dims = [int(x) for x in a.shape.split(",")]
     lib = _lib.lib()

@@ -38,6 +38,8 @@ SIGNATURES = {
                                    _d, _p, _p, _l, _p]),
     "cf_dgemm": (_i, [_i, _i, _i, _i, _i, _d, _p, _l, _l, _p, _l, _l, _d, _p, _l, _l, _p, _l, _l,
                       _i, _i, _p]),
+    "cf_dgemm_f32copy": (_i, [_i, _i, _i, _i, _i, _d, _p, _l, _l, _p, _l, _l, _d, _p, _l, _l, _p, _l, _l, _i, _i,
+                              _p]),
     "cf_potrf_workspace": (_sz, [_i, _i]),
     "cf_potrf": (_i, [_i, _p, _l, _l, _i, _p, _p, _p]),
     "cf_trtri_lower": (_i, [_i, _p, _l, _l, _p, _l, _l, _i, _p, _p]),

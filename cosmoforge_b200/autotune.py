@@ -3,7 +3,8 @@ patch batches' size buckets and the batched likelihood's launch shape.
 
 For each spectrum it times the candidate forms of the split-product GEMM
 (``cf_umma_gemm_bf16``: all planes of a 32-wide k-slice per stage with
-split accumulators, or 64-wide k-tiles term by term), promotion
+split accumulators, on one CTA or a CTA pair per tile, or 64-wide k-tiles term
+by term), promotion
 intervals and the row-tile group of the persistent tile order on the
 spectrum's own operands, checks every candidate's accuracy where it matters
 for the Fisher matrix, and keeps the fastest one within tolerance:
@@ -39,7 +40,7 @@ import torch
 from ._lib import check, stream
 from .engine_mixed import MixedPlan, _build_planes, default_gemm_forms
 
-CANDIDATES = ((1, 16), (1, 8), (0, 16), (0, 32))
+CANDIDATES = ((1, 16), (2, 16), (1, 8), (0, 16), (0, 32))
 GROUPS = (8, 16, 32)
 _MEM = {}
 

@@ -82,7 +82,8 @@ template <bool AT, bool BT>
 __global__ void __launch_bounds__(NT) k_dgemm(int M, int N, int K, double alpha, const double* A,
                                               long lda, long sA, const double* B, long ldb, long sB,
                                               double beta, double* C, long ldc, long sC, double* CT,
-                                              long ldct, long sCT, int lower_only)
+                                              long ldct, long sCT, float* C32, long ldc32, long sC32,
+                                              int lower_only)
 {
     extern __shared__ double smem[];
     // B stored [n][k] when BT (operand given N x K), else [k][n]
@@ -94,11 +95,15 @@ __global__ void __launch_bounds__(NT) k_dgemm(int M, int N, int K, double alpha,
 
     const int tile_m = blockIdx.y * BM, tile_n = blockIdx.x * BN;
     if ((lower_only & 1) && tile_n > tile_m + BM - 1) return;
+    // bit 3: batch entry z is row z of a symmetric block whose columns past
+    // z are not needed (tiles starting right of it are skipped)
+    if ((lower_only & 8) && tile_n > (int)blockIdx.z) return;
     const long bz = blockIdx.z;
     A += bz * sA;
     B += bz * sB;
     C += bz * sC;
     if (CT) CT += bz * sCT;
+    if (C32) C32 += bz * sC32;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = (warp >> 2) * 64, wn = (warp & 3) * 32;
@@ -177,6 +182,7 @@ __global__ void __launch_bounds__(NT) k_dgemm(int M, int N, int K, double alpha,
                 const double v = acc[mi][ni][h];
                 C[(long)r * ldc + c] = v;
                 if (CT) CT[(long)c * ldct + r] = v;
+                if (C32) C32[(long)r * ldc32 + c] = (float)v;
             }
         }
     }
@@ -185,7 +191,7 @@ __global__ void __launch_bounds__(NT) k_dgemm(int M, int N, int K, double alpha,
 template <bool AT, bool BT>
 int launch(int M, int N, int K, double alpha, const double* A, long lda, long sA, const double* B,
            long ldb, long sB, double beta, double* C, long ldc, long sC, double* CT, long ldct,
-           long sCT, int batch, int lower_only, cudaStream_t st)
+           long sCT, float* C32, long ldc32, long sC32, int batch, int lower_only, cudaStream_t st)
 {
     constexpr int SA = TileShape<AT>::elems, SB = TileShape<!BT>::elems;
     const size_t smem = (size_t)STAGES * (SA + SB) * sizeof(double);
@@ -193,11 +199,33 @@ int launch(int M, int N, int K, double alpha, const double* A, long lda, long sA
     if (int rc = cf_smem_optin(k_dgemm<AT, BT>, (int)smem, attr)) return rc;
     dim3 grid(cf_cdiv(N, BN), cf_cdiv(M, BM), batch);
     k_dgemm<AT, BT><<<grid, NT, smem, st>>>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC,
-                                            CT, ldct, sCT, lower_only);
+                                            CT, ldct, sCT, C32, ldc32, sC32, lower_only);
     CF_CHECK_LAUNCH();
     return CF_OK;
 }
 
+}  // namespace
+
+namespace {
+int dgemm(int transa, int transb, int M, int N, int K, double alpha, const double* A, long lda, long strideA,
+          const double* B, long ldb, long strideB, double beta, double* C, long ldc, long strideC, double* CT,
+          long ldct, long strideCT, float* C32, long ldc32, long strideC32, int batch, int lower_only,
+          cudaStream_t st)
+{
+    if (M < 0 || N < 0 || K < 0 || batch < 1 || !C) return CF_ERR_ARG;
+    if (M == 0 || N == 0) return CF_OK;
+    if (!transa && !transb)
+        return launch<false, false>(M, N, K, alpha, A, lda, strideA, B, ldb, strideB, beta, C, ldc, strideC, CT,
+                                    ldct, strideCT, C32, ldc32, strideC32, batch, lower_only, st);
+    if (!transa && transb)
+        return launch<false, true>(M, N, K, alpha, A, lda, strideA, B, ldb, strideB, beta, C, ldc, strideC, CT,
+                                   ldct, strideCT, C32, ldc32, strideC32, batch, lower_only, st);
+    if (transa && !transb)
+        return launch<true, false>(M, N, K, alpha, A, lda, strideA, B, ldb, strideB, beta, C, ldc, strideC, CT,
+                                   ldct, strideCT, C32, ldc32, strideC32, batch, lower_only, st);
+    return launch<true, true>(M, N, K, alpha, A, lda, strideA, B, ldb, strideB, beta, C, ldc, strideC, CT, ldct,
+                              strideCT, C32, ldc32, strideC32, batch, lower_only, st);
+}
 }  // namespace
 
 // transa / transb: 0 = operand given in its own orientation (A: M x K,
@@ -207,18 +235,17 @@ extern "C" int cf_dgemm(int transa, int transb, int M, int N, int K, double alph
                         double* C, long ldc, long strideC, double* CT, long ldct, long strideCT,
                         int batch, int lower_only, void* stream)
 {
-    if (M < 0 || N < 0 || K < 0 || batch < 1 || !C) return CF_ERR_ARG;
-    if (M == 0 || N == 0) return CF_OK;
-    cudaStream_t st = (cudaStream_t)stream;
-    if (!transa && !transb)
-        return launch<false, false>(M, N, K, alpha, A, lda, strideA, B, ldb, strideB, beta, C, ldc,
-                                    strideC, CT, ldct, strideCT, batch, lower_only, st);
-    if (!transa && transb)
-        return launch<false, true>(M, N, K, alpha, A, lda, strideA, B, ldb, strideB, beta, C, ldc,
-                                   strideC, CT, ldct, strideCT, batch, lower_only, st);
-    if (transa && !transb)
-        return launch<true, false>(M, N, K, alpha, A, lda, strideA, B, ldb, strideB, beta, C, ldc,
-                                   strideC, CT, ldct, strideCT, batch, lower_only, st);
-    return launch<true, true>(M, N, K, alpha, A, lda, strideA, B, ldb, strideB, beta, C, ldc, strideC,
-                              CT, ldct, strideCT, batch, lower_only, st);
+    return dgemm(transa, transb, M, N, K, alpha, A, lda, strideA, B, ldb, strideB, beta, C, ldc, strideC, CT, ldct,
+                 strideCT, nullptr, 0, 0, batch, lower_only, (cudaStream_t)stream);
+}
+
+// cf_dgemm with a rounded FP32 copy of the result (C32, row stride ldc32,
+// batch stride strideC32) written from the same epilogue instead of CT.
+extern "C" int cf_dgemm_f32copy(int transa, int transb, int M, int N, int K, double alpha, const double* A,
+                                long lda, long strideA, const double* B, long ldb, long strideB, double beta,
+                                double* C, long ldc, long strideC, float* C32, long ldc32, long strideC32,
+                                int batch, int lower_only, void* stream)
+{
+    return dgemm(transa, transb, M, N, K, alpha, A, lda, strideA, B, ldb, strideB, beta, C, ldc, strideC, nullptr,
+                 0, 0, C32, ldc32, strideC32, batch, lower_only, (cudaStream_t)stream);
 }

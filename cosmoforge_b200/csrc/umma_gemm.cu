@@ -171,11 +171,11 @@ __device__ __forceinline__ uint64_t smem_desc(const void* tile)
     return d;
 }
 
-template <int BN>
+template <int BN, int MM = BM>
 __device__ __forceinline__ uint32_t instr_desc()
 {
-    // D = F32, A = B = BF16, both K-major, M = 128, N = BN.
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+    // D = F32, A = B = BF16, both K-major, M = MM (128, or 256 for a CTA pair), N = BN.
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(MM >> 4) << 24);
 }
 
 __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
@@ -194,6 +194,56 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar)
                  : "memory");
 }
 
+// --- CTA pairs (cta_group::2): one 256 x BN tile per pair of SMs ---
+__device__ __forceinline__ uint32_t cluster_rank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+// Address of the same shared-memory location in CTA `rank` of the cluster.
+__device__ __forceinline__ uint32_t at_rank(const void* p, uint32_t rank)
+{
+    uint32_t out;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(out) : "r"(smem_u32(p)), "r"(rank));
+    return out;
+}
+__device__ __forceinline__ void cluster_sync()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void umma_bf16_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                               uint32_t accumulate)
+{
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+        ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+// Arrive on the barrier at this offset in both CTAs of the pair once the MMAs issued so far are done.
+__device__ __forceinline__ void umma_commit_pair(uint64_t* bar)
+{
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;\n" ::"r"(
+            smem_u32(bar)),
+        "h"((uint16_t)3)
+        : "memory");
+}
+// A TMA load into this CTA's shared memory whose bytes are counted on the
+// pair leader's barrier (mbar: a shared::cluster address); no multicast.
+__device__ __forceinline__ void tma_load_3d_pair(const CUtensorMap* map, uint32_t mbar, void* dst, int c0, int c1,
+                                                 int c2)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];\n"
+        ::"r"(smem_u32(dst)), "l"((uint64_t)map), "r"(mbar), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t mbar)
+{
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(mbar) : "memory");
+}
+
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
 {
     asm volatile(
@@ -208,7 +258,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 
-template <int BN, int STAGES, bool TRACE, int KC, int PLS, int BKT, bool SPLIT>
+template <int BN, int STAGES, bool TRACE, int KC, int PLS, int BKT, bool SPLIT, int CG = 1>
 __global__ void __launch_bounds__(NTHREADS, 1)
     k_umma_gemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int K,
                 int n_split, Terms terms, EpiArgs epi, TraceArgs tr, int group_m, unsigned long long wait_ns,
@@ -231,9 +281,17 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     // same chunk instead of alternating, so the small corrections are not added
     // into the large leading sum inside the tensor core; the MMA thread waits
     // for the epilogue to read both before it starts the next chunk.
+    // CG == 2: a CTA pair (cluster of two) computes a 256 x BN tile with
+    // tcgen05.mma.cta_group::2 issued by the leader (rank 0); each CTA loads
+    // its own 128 rows of A and half of the BN rows of B, the loads of both
+    // are counted on the leader's barriers, MMA completions are multicast to
+    // both CTAs' barriers and each CTA's epilogue drains its own TMEM half
+    // (rows 128 rank ..) and reports to the leader.
+    static_assert(CG == 1 || (CG == 2 && !TRACE && PLS > 1), "CTA pairs: all-planes GEMM form only");
     using AccT = typename std::conditional<TRACE, double, float>::type;
     constexpr int HALF = BN / 2;
-    constexpr uint32_t A_BYTES = BM * BKT * 2, B_BYTES = BN * BKT * 2;
+    constexpr int BNL = BN / CG;  // rows of B held by this CTA
+    constexpr uint32_t A_BYTES = BM * BKT * 2, B_BYTES = BNL * BKT * 2;
     // stages per promotion chunk: KC k-tiles of 64
     constexpr int CH = PLS > 1 ? KC * (64 / BKT) : KC;
     static_assert(!SPLIT || PLS > 1, "split accumulators need all planes per stage");
@@ -252,7 +310,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int n_mt = (epi.M + BM - 1) / BM, n_nt = (epi.N + BN - 1) / BN;
+    const uint32_t rank = CG == 2 ? cluster_rank() : 0u;
+    const bool leader = rank == 0;
+    const long t_first = CG == 2 ? (long)(blockIdx.x >> 1) : (long)blockIdx.x;
+    const long t_step = CG == 2 ? (long)(gridDim.x >> 1) : (long)gridDim.x;
+    const int n_mt = (epi.M + BM * CG - 1) / (BM * CG), n_nt = (epi.N + BN - 1) / BN;
     const long n_tiles = (long)n_mt * n_nt * n_split;
     const int nl = TRACE ? (tr.K2 + BKT - 1) / BKT : 1;
     const long kt_total = TRACE ? (long)tr.K1 * nl : (long)((K + BKT - 1) / BKT);
@@ -269,7 +331,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         const long within = t_in - (long)g * gm_full * n_nt;
         const int mt = g * gm_full + (int)(within % gm);
         const int nt = (int)(within / gm);
-        m0 = mt * BM;
+        m0 = mt * BM * CG + (int)rank * BM;  // this CTA's rows
         n0 = nt * BN;
         t_lo = kt_total * z / n_split;
         kt = (int)(kt_total * (z + 1) / n_split - t_lo);
@@ -282,19 +344,29 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         }
         mbar_init(&accf[0], 1);
         mbar_init(&accf[1], 1);
-        mbar_init(&acce[0], EPI_WARPS);
-        mbar_init(&acce[1], EPI_WARPS);
+        mbar_init(&acce[0], EPI_WARPS * CG);  // a pair's leader hears both CTAs' epilogues
+        mbar_init(&acce[1], EPI_WARPS * CG);
         mbar_init(dbar, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     if (warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
-                     "r"(TMEM_COLS));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+        if constexpr (CG == 2) {
+            asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                             smem_u32(tmem_slot)),
+                         "r"(TMEM_COLS));
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;\n");
+        } else {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                             smem_u32(tmem_slot)),
+                         "r"(TMEM_COLS));
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+        }
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
+    // a pair's barriers (initialised above) are signalled by the other CTA from here on
+    if constexpr (CG == 2) cluster_sync();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     const uint32_t tmem = *tmem_slot;
 
@@ -302,7 +374,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         if (lane == 0) {
             long g = 0;
             bool stop = false;
-            for (long tile = blockIdx.x; tile < n_tiles && !stop; tile += gridDim.x) {
+            for (long tile = t_first; tile < n_tiles && !stop; tile += t_step) {
                 int m0, n0, kt;
                 long t_lo;
                 coords(tile, m0, n0, t_lo, kt);
@@ -325,7 +397,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         t = rem / wlen;
                         ktile = t_lo + (long)w * KC + rem % wlen;
                     }
-                    mbar_expect_tx(&full[s], A_STAGE + B_STAGE);
+                    // a pair's leader expects both CTAs' bytes on its barrier
+                    if (leader) mbar_expect_tx(&full[s], CG * (A_STAGE + B_STAGE));
 #pragma unroll
                     for (int pl = 0; pl < PLS; ++pl) {
                         const int pa = PLS > 1 ? pl : terms.a[t], pb = PLS > 1 ? pl : terms.b[t];
@@ -337,22 +410,30 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                             tma_load_4d(&mapB, &full[s], db, l0, k, n0, pb);
                         } else {
                             const int kk = (int)ktile * BKT;
-                            tma_load_3d(&mapA, &full[s], da, kk, m0, pa);
-                            tma_load_3d(&mapB, &full[s], db, kk, n0, pb);
+                            if constexpr (CG == 2) {
+                                const uint32_t fb = at_rank(&full[s], 0);
+                                tma_load_3d_pair(&mapA, fb, da, kk, m0, pa);
+                                tma_load_3d_pair(&mapB, fb, db, kk, n0 + (int)rank * BNL, pb);
+                            } else {
+                                tma_load_3d(&mapA, &full[s], da, kk, m0, pa);
+                                tma_load_3d(&mapB, &full[s], db, kk, n0, pb);
+                            }
                         }
                     }
                 }
             }
-            // drain: every issued copy lands before the CTA may exit
-            for (long q = (g > STAGES ? g - STAGES : 0); q < g; ++q)
-                mbar_drain(&full[q % STAGES], (uint32_t)((q / STAGES) & 1));
+            // drain: every issued copy lands before the CTA may exit (a pair's leader
+            // sees both CTAs' copies complete; the other waits at the final cluster barrier)
+            if (leader)
+                for (long q = (g > STAGES ? g - STAGES : 0); q < g; ++q)
+                    mbar_drain(&full[q % STAGES], (uint32_t)((q / STAGES) & 1));
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            const uint32_t idesc = instr_desc<BN>();
+            const uint32_t idesc = instr_desc<BN, BM * CG>();
             bool aborted = false;
             long g = 0, gc = 0;
-            for (long tile = blockIdx.x; tile < n_tiles && !aborted; tile += gridDim.x) {
+            for (long tile = t_first; tile < n_tiles && !aborted && (CG == 1 || leader); tile += t_step) {
                 int m0, n0, kt;
                 long t_lo;
                 coords(tile, m0, n0, t_lo, kt);
@@ -398,19 +479,33 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         const uint32_t dst = tmem + (uint32_t)((SPLIT ? (t > 0) : buf) * BN);
                         const bool fresh = first && (SPLIT ? t <= 1 : t == 0);
 #pragma unroll
-                        for (int k = 0; k < BKT / 16; ++k)  // 16 BF16 = 32 B per MMA; advance the start address
-                            umma_bf16(dst, ad + (uint64_t)((k * 32) >> 4), bd + (uint64_t)((k * 32) >> 4), idesc,
-                                      (fresh && k == 0) ? 0u : 1u);
+                        for (int k = 0; k < BKT / 16; ++k) {  // 16 BF16 = 32 B per MMA; advance the start address
+                            if constexpr (CG == 2)
+                                umma_bf16_pair(dst, ad + (uint64_t)((k * 32) >> 4), bd + (uint64_t)((k * 32) >> 4),
+                                               idesc, (fresh && k == 0) ? 0u : 1u);
+                            else
+                                umma_bf16(dst, ad + (uint64_t)((k * 32) >> 4), bd + (uint64_t)((k * 32) >> 4), idesc,
+                                          (fresh && k == 0) ? 0u : 1u);
+                        }
                     }
-                    umma_commit(&empty[s]);
+                    if constexpr (CG == 2)
+                        umma_commit_pair(&empty[s]);
+                    else
+                        umma_commit(&empty[s]);
                     if (pos == clen - 1 || it == iters - 1) {
-                        umma_commit(&accf[SPLIT ? 0 : buf]);
+                        if constexpr (CG == 2)
+                            umma_commit_pair(&accf[SPLIT ? 0 : buf]);
+                        else
+                            umma_commit(&accf[SPLIT ? 0 : buf]);
                         ++gc;
                     }
                 }
             }
             if (aborted) {  // MMAs already issued finish before TMEM is freed
-                umma_commit(dbar);
+                if constexpr (CG == 2)
+                    umma_commit_pair(dbar);
+                else
+                    umma_commit(dbar);
                 mbar_drain(dbar, 0);
             }
         }
@@ -421,7 +516,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         const uint32_t lane_addr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(half * HALF);
         long gc = 0;
         bool ok = true;
-        for (long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
+        for (long tile = t_first; tile < n_tiles && ok; tile += t_step) {
             int m0, n0, kt;
             long t_lo;
             coords(tile, m0, n0, t_lo, kt);
@@ -452,8 +547,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 }
                 asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
                 __syncwarp();
-                if (lane == 0)
-                    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(&acce[buf])) : "memory");
+                if (lane == 0) {
+                    if (CG == 2 && !leader)
+                        mbar_arrive_remote(at_rank(&acce[buf], 0));
+                    else
+                        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(&acce[buf])) : "memory");
+                }
             }
             const int row = m0 + quad * 32 + lane;
             if (!ok || *abort_flag || iters == 0 || row >= epi.M) continue;
@@ -530,7 +629,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
-    if (warp == 1) {
+    if constexpr (CG == 2) {
+        // neither CTA leaves (or frees its TMEM) while the pair's MMAs or copies may touch it
+        cluster_sync();
+        if (warp == 1)
+            asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TMEM_COLS));
+    } else if (warp == 1) {
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TMEM_COLS));
     }
     if (threadIdx.x == 0 && *abort_flag && err) atomicExch(err, 1);
@@ -599,43 +703,73 @@ int g_group_m = 16;
 // Bound of the kernels' waits on pipeline barriers (drains of issued work keep WAIT_NS).
 unsigned long long g_wait_ns = WAIT_NS;
 
-template <int BN, int STAGES, bool TRACE, int KC, int PLS = 1, int BKT = BK, bool SPLIT = false>
+template <int BN, int STAGES, bool TRACE, int KC, int PLS = 1, int BKT = BK, bool SPLIT = false, int CG = 1>
 int launch_gemm_kc(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, int K, const Terms& t,
                    const EpiArgs& e, const TraceArgs& tr, int splits, int* err, cudaStream_t st)
 {
-    const size_t smem = 1024 + (size_t)STAGES * PLS * (BM * BKT * 2 + BN * BKT * 2) + 256;
-    static_assert(1024 + (size_t)STAGES * PLS * (BM * BKT * 2 + BN * BKT * 2) + 256 <= 232448,
-                  "shared memory ring exceeds 227 KB");
+    constexpr size_t RING = (size_t)STAGES * PLS * (BM * BKT * 2 + (BN / CG) * BKT * 2);
+    const size_t smem = 1024 + RING + 256;
+    static_assert(1024 + RING + 256 <= 232448, "shared memory ring exceeds 227 KB");
+    auto kern = k_umma_gemm<BN, STAGES, TRACE, KC, PLS, BKT, SPLIT, CG>;
     static std::atomic<int> attr[CF_MAX_DEVICES];
-    if (int rc = cf_smem_optin(k_umma_gemm<BN, STAGES, TRACE, KC, PLS, BKT, SPLIT>, (int)smem, attr)) return rc;
+    if (int rc = cf_smem_optin(kern, (int)smem, attr)) return rc;
     int dev = 0, sms = 0;
     CF_CHECK(cudaGetDevice(&dev));
     CF_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const long tiles = (long)cf_cdiv(M, BM) * cf_cdiv(N, BN) * splits;
+    const long tiles = (long)cf_cdiv(M, BM * CG) * cf_cdiv(N, BN) * splits;
+    if constexpr (CG == 2) {
+        // clusters of two CTAs on neighbouring SMs, one output tile per pair at a time
+        const int np = (int)(tiles < sms / 2 ? tiles : sms / 2);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(2 * np);
+        cfg.blockDim = dim3(NTHREADS);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = 2;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        CF_CHECK(cudaLaunchKernelEx(&cfg, kern, ma, mb, K, splits, t, e, tr, g_group_m, g_wait_ns, err));
+        return CF_OK;
+    }
     const int grid = (int)(tiles < sms ? tiles : sms);
-    k_umma_gemm<BN, STAGES, TRACE, KC, PLS, BKT, SPLIT><<<grid, NTHREADS, smem, st>>>(ma, mb, K, splits, t, e, tr,
-                                                                                     g_group_m, g_wait_ns, err);
+    kern<<<grid, NTHREADS, smem, st>>>(ma, mb, K, splits, t, e, tr, g_group_m, g_wait_ns, err);
     CF_CHECK_LAUNCH();
     return CF_OK;
 }
 
 // GEMM mode: 1 = all planes of a 32-wide k-slice per stage with split
-// accumulators where the planes allow it, 0 = 64-wide k-tiles term by term.
+// accumulators where the planes allow it, 2 = the same for three planes on
+// CTA pairs (256-row tiles, 4 stages of 48 KB per CTA), 0 = 64-wide k-tiles
+// term by term.
 int g_all_planes = 1;
 
-template <int BN, int STAGES, bool TRACE, int PLS = 1, int BKT = BK, bool SPLIT = false>
+template <int BN, int STAGES, bool TRACE, int PLS = 1, int BKT = BK, bool SPLIT = false, int CG = 1>
 int launch_gemm(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, int K, const Terms& t,
                 const EpiArgs& e, const TraceArgs& tr, int splits, int* err, cudaStream_t st)
 {
     switch (g_promote_kc) {
-        case 1: return launch_gemm_kc<BN, STAGES, TRACE, 1, PLS, BKT, SPLIT>(ma, mb, M, N, K, t, e, tr, splits, err, st);
-        case 2: return launch_gemm_kc<BN, STAGES, TRACE, 2, PLS, BKT, SPLIT>(ma, mb, M, N, K, t, e, tr, splits, err, st);
-        case 8: return launch_gemm_kc<BN, STAGES, TRACE, 8, PLS, BKT, SPLIT>(ma, mb, M, N, K, t, e, tr, splits, err, st);
+        case 1:
+            return launch_gemm_kc<BN, STAGES, TRACE, 1, PLS, BKT, SPLIT, CG>(ma, mb, M, N, K, t, e, tr, splits,
+                                                                                   err, st);
+        case 2:
+            return launch_gemm_kc<BN, STAGES, TRACE, 2, PLS, BKT, SPLIT, CG>(ma, mb, M, N, K, t, e, tr, splits,
+                                                                                   err, st);
+        case 8:
+            return launch_gemm_kc<BN, STAGES, TRACE, 8, PLS, BKT, SPLIT, CG>(ma, mb, M, N, K, t, e, tr, splits,
+                                                                                   err, st);
         case 16:
-            return launch_gemm_kc<BN, STAGES, TRACE, 16, PLS, BKT, SPLIT>(ma, mb, M, N, K, t, e, tr, splits, err, st);
+            return launch_gemm_kc<BN, STAGES, TRACE, 16, PLS, BKT, SPLIT, CG>(ma, mb, M, N, K, t, e, tr,
+                                                                                    splits, err, st);
         case 32:
-            return launch_gemm_kc<BN, STAGES, TRACE, 32, PLS, BKT, SPLIT>(ma, mb, M, N, K, t, e, tr, splits, err, st);
-        default: return launch_gemm_kc<BN, STAGES, TRACE, 4, PLS, BKT, SPLIT>(ma, mb, M, N, K, t, e, tr, splits, err, st);
+            return launch_gemm_kc<BN, STAGES, TRACE, 32, PLS, BKT, SPLIT, CG>(ma, mb, M, N, K, t, e, tr,
+                                                                                    splits, err, st);
+        default:
+            return launch_gemm_kc<BN, STAGES, TRACE, 4, PLS, BKT, SPLIT, CG>(ma, mb, M, N, K, t, e, tr, splits,
+                                                                                   err, st);
     }
 }
 
@@ -687,11 +821,12 @@ extern "C" int cf_umma_set_group(int group_m)
     return prev;
 }
 
-// Select the GEMM form (1 = all planes per stage, 0 = term by term); returns the previous one.
+// Select the GEMM form (1 = all planes per stage, 2 = all planes on CTA
+// pairs, 0 = term by term); returns the previous one.
 extern "C" int cf_umma_set_all_planes(int on)
 {
     const int prev = g_all_planes;
-    g_all_planes = on ? 1 : 0;
+    g_all_planes = (on == 0 || on == 1 || on == 2) ? on : 1;
     return prev;
 }
 
@@ -717,10 +852,13 @@ int gemm_bf16(int M, int N, int K, int nterms, const int* ta, const int* tb, con
     bool all_planes = g_all_planes && (pls == 2 || pls == 3) && t.a[0] == 0 && t.b[0] == 0;
     for (int i = 1; i < nterms && all_planes; ++i) all_planes = !(t.a[i] == 0 && t.b[i] == 0);
     if (all_planes) {
+        // form 2: three planes on CTA pairs (each CTA holds half of B's 256 rows)
+        const bool pairs = g_all_planes == 2 && pls == 3;
         int rc = make_map(&ma, A, K, M, lda, a_planes, a_ps, BM, 32);
         if (rc) return rc;
-        rc = make_map(&mb, B, K, N, ldb, b_planes, b_ps, 256, 32);
+        rc = make_map(&mb, B, K, N, ldb, b_planes, b_ps, pairs ? 128 : 256, 32);
         if (rc) return rc;
+        if (pairs) return launch_gemm<256, 4, false, 3, 32, true, 2>(ma, mb, M, N, K, t, e, tr, 1, err, st);
         if (pls == 3) return launch_gemm<256, 3, false, 3, 32, true>(ma, mb, M, N, K, t, e, tr, 1, err, st);
         return launch_gemm<256, 4, false, 2, 32, true>(ma, mb, M, N, K, t, e, tr, 1, err, st);
     }

@@ -356,18 +356,18 @@ class Engine:
         precision "fp64": FP64 Cholesky, chi2 = |L^-1 x|^2, ln|C| from its
         diagonal.  "mixed": FP32 Cholesky of C, chi2 from one FP64 refinement
         step against C (second-order in the factor's error), ln|C| from the
-        FP32 factor's diagonal summed in FP64.  With the basis build the mixed
-        C is formed in FP32 by BF16x6 split products on the tensor cores
-        (~2^-24 relative per entry, no FP64 C at all) and the refinement reads
-        that FP32 C, so chi2 is the FP32 C's: first order in its rounding,
-        ~1e-7 relative for maps drawn from C and ~1e-5 for maps far from it
-        (|dlnL| within 0.05).  With the direct build the refinement reads the
-        FP64 C and chi2 is second order in the factor's error (1e-8).
+        FP32 factor's diagonal summed in FP64.
 
-        build "basis" forms C(theta) = S(theta) + s N from the per-multipole
-        basis (one GEMM per block region, see SignalBasis), "direct" runs the
-        pair kernel per point, "auto" takes the basis for batches of 64 or more
-        points when it fits in 4 GB.
+        build "basis" forms the lower triangle of C(theta) = S(theta) + s N
+        from the per-multipole basis (one FP64 GEMM per block region, see
+        SignalBasis; for "mixed" the same epilogue writes the FP32 copy to
+        factor), "direct" runs the pair kernel per point, "auto" takes the
+        basis for batches of 64 or more points when it fits in 4 GB.
+        "basis_tc" (mixed only) forms C in FP32 with BF16x6 split products on
+        the tensor cores and refines against that FP32 C: the fastest form,
+        but chi2 is then the FP32 C's (first order in its rounding: ~1e-7
+        relative for maps drawn from C, up to ~1e-5 for maps far from it)
+        instead of second order in the factor's error (1e-8).
         """
         if precision not in ("fp64", "mixed"):
             raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
@@ -381,10 +381,19 @@ class Engine:
             sc = torch.as_tensor(noise_scale, dtype=F64, device=self.dev).reshape(B).contiguous()
         if build == "auto":
             build = "basis" if B >= 64 and SignalBasis.bytes_needed(self.L) <= 4 << 30 else "direct"
+        if build not in ("basis", "direct", "basis_tc"):
+            raise ValueError(f"build must be 'auto', 'basis', 'direct' or 'basis_tc', got {build!r}")
+        if build == "basis_tc":
+            if precision != "mixed":
+                raise ValueError("build 'basis_tc' forms C in FP32: it serves precision 'mixed' only")
+            return self._lnl_mixed_basis_tc(self.signal_basis(N), cl, maps, sc)
         if build == "basis":
+            # lower triangles only: the factors and the chi2 kernels read nothing else
             if precision == "mixed":
-                return self._lnl_mixed_basis(self.signal_basis(N), cl, maps, sc)
-            C = self.signal_basis(N).covariance(cl, sc)
+                C32 = torch.empty((B, n, n), dtype=torch.float32, device=self.dev)
+                C = self.signal_basis(N).covariance(cl, sc, lower=True, out32=C32)
+                return self._lnl_mixed(C, N, maps, sc, C32=C32)
+            C = self.signal_basis(N).covariance(cl, sc, lower=True)
         else:
             C = self.signal(cl)
             if precision == "mixed":
@@ -403,10 +412,10 @@ class Engine:
               "cf_chi2_logdet")
         return chi2, logdet, -0.5 * (chi2 + logdet[:, None]), info
 
-    def _lnl_mixed_basis(self, basis: "SignalBasis", cl: torch.Tensor, maps: torch.Tensor, sc):
+    def _lnl_mixed_basis_tc(self, basis: "SignalBasis", cl: torch.Tensor, maps: torch.Tensor, sc):
         """Mixed likelihood with C(theta) built in FP32 on the tensor cores: two
         copies from one pass (one is factored in place, the other feeds the
-        FP64 refinement), FP32 Cholesky, refined chi2 and ln|C|."""
+        FP64 refinement arithmetic), FP32 Cholesky, refined chi2 and ln|C|."""
         B, n = cl.shape[0], self.L.n
         C32 = torch.empty((B, n, n), dtype=torch.float32, device=self.dev)
         L32 = torch.empty_like(C32)
@@ -426,13 +435,12 @@ class Engine:
         info = torch.where(err[0] != 0, torch.full_like(info, CF_ERR_TIMEOUT), info)
         return chi2, logdet, -0.5 * (chi2 + logdet[:, None]), info
 
-    def _lnl_mixed(self, C: torch.Tensor, N: torch.Tensor, maps: torch.Tensor, sc, noise_added: bool = False):
+    def _lnl_mixed(self, C: torch.Tensor, N: torch.Tensor, maps: torch.Tensor, sc, C32: torch.Tensor | None = None):
+        """C holds S (C32 None: the noise is added here, with the FP32 copy) or
+        S + s N with its FP32 copy already in C32."""
         B, n = C.shape[0], self.L.n
-        C32 = torch.empty((B, n, n), dtype=torch.float32, device=self.dev)
-        if noise_added:  # C already holds S + s N: only its FP32 copy is made
-            check(self.lib.cf_axpby_f32(n * n, 1.0, C.data_ptr(), n * n, 0.0, None, N.data_ptr(), 0,
-                                        None, n * n, C32.data_ptr(), n * n, B, stream()), "cf_axpby_f32")
-        else:
+        if C32 is None:
+            C32 = torch.empty((B, n, n), dtype=torch.float32, device=self.dev)
             check(self.lib.cf_axpby_f32(n * n, 1.0, C.data_ptr(), n * n, 1.0, ptr(sc), N.data_ptr(), 0,
                                         C.data_ptr(), n * n, C32.data_ptr(), n * n, B, stream()), "cf_axpby_f32")
         info = torch.zeros(B, dtype=torch.int32, device=self.dev)
@@ -511,8 +519,15 @@ class SignalBasis:
             tot += k * fa.nrows * fb.nrows * (1 if blk.fa == blk.fb else 2)
         return 8 * tot
 
-    def covariance(self, cl: torch.Tensor, scale: torch.Tensor | None = None, out=None) -> torch.Tensor:
-        """C (B x n x n, FP64) for beam-smoothed tables cl (B, nspectra, L+1)."""
+    def covariance(self, cl: torch.Tensor, scale: torch.Tensor | None = None, out=None, lower: bool = False,
+                   out32: torch.Tensor | None = None) -> torch.Tensor:
+        """C (B x n x n, FP64) for beam-smoothed tables cl (B, nspectra, L+1).
+
+        lower: only the lower triangle is formed (the mirror span of each
+        off-diagonal block is left out, the diagonal blocks skip the tiles
+        right of their rows; entries above the diagonal are left unset or
+        partly filled).  out32: an FP32 copy written by the same GEMM
+        epilogue."""
         E, n, Lp = self.E, self.n, self.Lp
         B = cl.shape[0]
         if out is None:
@@ -525,6 +540,8 @@ class SignalBasis:
         if not torch.cuda.is_current_stream_capturing():
             used = (cl.abs().amax(dim=(0, 2)) > 0).cpu().numpy()
         for r0, c0, R, Cc, sp, sp_dev, K in self.regions:
+            if lower and r0 < c0:
+                continue  # the mirror span of an off-diagonal block lies above the diagonal
             keep = len(sp)
             while used is not None and keep > 0 and not used[sp[keep - 1]]:
                 keep -= 1
@@ -532,9 +549,16 @@ class SignalBasis:
             # spectra picked with a device index (no host-to-device copy: capturable)
             ctab = torch.cat([s[:, None], cl.index_select(1, sp_dev[:keep]).reshape(B, keep * Lp)],
                              dim=1).contiguous()
-            check(self.E.lib.cf_dgemm(0, 0, B, Cc, kd, 1.0, ctab.data_ptr(), kd, 0, K.data_ptr(), R * Cc, Cc,
-                                      0.0, _off(out, r0 * n + c0), n * n, n, None, 0, 0, R, 0, stream()),
-                  "cf_dgemm")
+            # batch entry = region row; bit 3 skips the tiles right of the row on a diagonal block
+            lo = 8 if (lower and r0 == c0) else 0
+            off = r0 * n + c0
+            if out32 is None:
+                check(self.E.lib.cf_dgemm(0, 0, B, Cc, kd, 1.0, ctab.data_ptr(), kd, 0, K.data_ptr(), R * Cc, Cc,
+                                          0.0, _off(out, off), n * n, n, None, 0, 0, R, lo, stream()), "cf_dgemm")
+            else:
+                check(self.E.lib.cf_dgemm_f32copy(0, 0, B, Cc, kd, 1.0, ctab.data_ptr(), kd, 0, K.data_ptr(), R * Cc,
+                                                  Cc, 0.0, _off(out, off), n * n, n, _off(out32, off), n * n, n, R,
+                                                  lo, stream()), "cf_dgemm_f32copy")
         return out
 
     def _planes(self):

@@ -147,15 +147,17 @@ def default_gemm_forms(L) -> dict:
 
     The all-planes form (every plane of a k-slice per pipeline stage, the
     leading product in its own TMEM accumulator, the five corrections sharing
-    a second one) is the faster one.  On blocks that involve a spin-0 field
-    its errors correlate with the transposed entries of A_b at the lowest
-    multipoles (measured on the TQU nside-16 problem: |dF_bb|/F_bb 1.2e-5 for
-    TT l=2 against 4e-6 term by term), so those spectra run term by term.
+    a second one) is the faster one, and faster again on CTA pairs (form 2:
+    256-row tiles, each CTA holding half of B; the same arithmetic per output
+    entry).  On blocks that involve a spin-0 field its errors correlate with
+    the transposed entries of A_b at the lowest multipoles (measured on the
+    TQU nside-16 problem: |dF_bb|/F_bb 1.2e-5 for TT l=2 against 4e-6 term by
+    term), so those spectra run term by term.
     """
     forms = {}
     for s, sp in enumerate(L.spectra):
         spin0 = any(L.fields[f].spin == 0 for f in (sp.fi, sp.fj))
-        forms[s] = (0, 16) if spin0 else (1, 16)
+        forms[s] = (0, 16) if spin0 else (2, 16)
     return forms
 
 

@@ -90,12 +90,28 @@ int cf_build_block(int kind, int mode, int na, const double* va, int nb, const d
  * starts each tile's K sum at its first row (op(A) upper triangular, e.g.
  * op(A) = Y^T with Y lower); bit 2 ends it after its last row (op(A) lower
  * triangular).  Bits 1 and 2 assume M == K (a square triangular op(A)).
+ * Bit 3 treats batch entry z as row z of a symmetric block and skips the
+ * output tiles that start right of column z (the lower triangle of a block
+ * built row by row; entries right of z inside a computed tile are written too).
  * Replaces: cosmocore/basics/linalg.py:18-32 (matrix_mult, np.matmul).
  */
 int cf_dgemm(int transa, int transb, int M, int N, int K, double alpha, const double* A, long lda,
              long strideA, const double* B, long ldb, long strideB, double beta, double* C, long ldc,
              long strideC, double* CT, long ldct, long strideCT, int batch, int lower_only,
              void* stream);
+
+/*
+ * cf_dgemm with a rounded FP32 copy of the result (C32: row stride ldc32,
+ * batch stride strideC32) written by the same epilogue in place of CT, so an
+ * FP64 matrix and its FP32 copy come out of one pass.  Used to build the
+ * mixed likelihood's C(theta) (FP64 for the refinement, FP32 to factor).
+ * Replaces: the per-point covariance build of picslike/picslike.py:301-319
+ * with its FP32 cast, in the mixed likelihood.
+ */
+int cf_dgemm_f32copy(int transa, int transb, int M, int N, int K, double alpha, const double* A, long lda,
+                     long strideA, const double* B, long ldb, long strideB, double beta, double* C, long ldc,
+                     long strideC, float* C32, long ldc32, long strideC32, int batch, int lower_only,
+                     void* stream);
 
 /* Bytes of workspace cf_potrf needs for `batch` problems of order n. */
 size_t cf_potrf_workspace(int n, int batch);
@@ -326,8 +342,10 @@ int cf_umma_set_promotion(int kc);
 /* Form of cf_umma_gemm_bf16: 1 (default) loads every plane of a 32-wide
  * k-slice into one pipeline stage and keeps the leading product apart from
  * the corrections in a second TMEM accumulator, when both operands carry the
- * same 2 or 3 planes; 0 walks 64-wide k-tiles term by term.  Returns the
- * previous setting.  No counterpart in the reference. */
+ * same 2 or 3 planes; 2 does the same for three planes on CTA pairs
+ * (clusters of two CTAs on neighbouring SMs, tcgen05.mma.cta_group::2 on
+ * 256-row tiles, each CTA holding half of B); 0 walks 64-wide k-tiles term by
+ * term.  Returns the previous setting.  No counterpart in the reference. */
 int cf_umma_set_all_planes(int on);
 
 /* Row tiles per group in the persistent tile order of the tcgen05 kernels

@@ -31,7 +31,7 @@ def test_tuned_forms_meet_fisher_tolerance(name, tmp_path, monkeypatch):
     Cinv = E.spd_inverse(E.signal(L.smoothed_cl_table(cls_of(d))) + N)
     forms, report = autotune.tune_fisher(E, Cinv, use_cache=False)
     assert set(forms) == set(range(L.nspectra))
-    assert all(ap in (0, 1) and kc in (8, 16, 32) and gm in autotune.GROUPS for ap, kc, gm in forms.values())
+    assert all(ap in (0, 1, 2) and kc in (8, 16, 32) and gm in autotune.GROUPS for ap, kc, gm in forms.values())
     assert set(report) == {s.label for s in L.spectra}
     F64 = E.fisher_qml(Cinv)[0].cpu().numpy()
     Fm = engine_mixed.fisher(E, Cinv, forms=forms).cpu().numpy()

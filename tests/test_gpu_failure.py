@@ -45,24 +45,31 @@ def _gemm_case(lib, M, N, K):
     return run, Cf, err, ref
 
 
-def test_timed_out_wait_reports_timeout_and_context_survives():
+@pytest.mark.parametrize("form", [1, 2])
+def test_timed_out_wait_reports_timeout_and_context_survives(form):
+    """form 1: one CTA per tile; form 2: CTA pairs (the leader's MMAs write both
+    CTAs' TMEM; both drain and meet at the final cluster barrier)."""
     from cosmoforge_b200 import _lib
 
     lib = _lib.lib()
     st = torch.cuda.current_stream().cuda_stream
     run, Cf, err, ref = _gemm_case(lib, 384, 512, 1024)
-    prev = lib.cf_umma_set_wait_limit(0)
+    prev_form = lib.cf_umma_set_all_planes(form)
     try:
+        prev = lib.cf_umma_set_wait_limit(0)
+        try:
+            run()
+            assert lib.cf_umma_status(err.data_ptr(), st) == _lib.CF_ERR_TIMEOUT
+            with pytest.raises(_lib.DeviceError, match="timeout"):
+                _lib.check(lib.cf_umma_status(err.data_ptr(), st), "tensor-core kernel")
+        finally:
+            lib.cf_umma_set_wait_limit(-1)
+        assert prev == 2_000_000_000
+        err.zero_()
         run()
-        assert lib.cf_umma_status(err.data_ptr(), st) == _lib.CF_ERR_TIMEOUT
-        with pytest.raises(_lib.DeviceError, match="timeout"):
-            _lib.check(lib.cf_umma_status(err.data_ptr(), st), "tensor-core kernel")
+        assert lib.cf_umma_status(err.data_ptr(), st) == _lib.CF_OK
     finally:
-        lib.cf_umma_set_wait_limit(-1)
-    assert prev == 2_000_000_000
-    err.zero_()
-    run()
-    assert lib.cf_umma_status(err.data_ptr(), st) == _lib.CF_OK
+        lib.cf_umma_set_all_planes(prev_form)
     got = Cf.double()
     assert float((got - ref).abs().max() / ref.abs().max()) < 1e-5
 
@@ -165,3 +172,35 @@ def test_likelihood_reports_a_non_finite_point():
         info = info.cpu().numpy()
         assert info[2] > 0 and np.all(info[[0, 1, 3]] == 0), (prec, info)
         assert bool(torch.isfinite(lnl[[0, 1, 3]]).all())
+
+
+def test_potrf_f32_tensor_core_timeout():
+    """A bounded wait of the FP32 factor's tensor-core GEMMs that runs out
+    marks the problem with CF_ERR_TIMEOUT (-3) in info (the kernel drains its
+    MMAs and frees its TMEM first), and the next call on the same context
+    factors exactly."""
+    from cosmoforge_b200 import _lib
+
+    lib = _lib.lib()
+    n, batch = 300, 4
+    A64 = torch.stack([torch.from_numpy(_spd(n, 20 + b)) for b in range(batch)]).cuda()
+    st = torch.cuda.current_stream().cuda_stream
+
+    def run():
+        A = A64.float().contiguous()
+        work = torch.empty(lib.cf_potrf_f32_workspace(n, batch) // 4 + 1, dtype=torch.float32, device="cuda")
+        info = torch.zeros(batch, dtype=torch.int32, device="cuda")
+        assert lib.cf_potrf_f32(n, A.data_ptr(), n, n * n, batch, work.data_ptr(), info.data_ptr(), st) == 0
+        torch.cuda.synchronize()
+        return A, info
+
+    lib.cf_sgemm_bf16x6_set_wait_limit(0)
+    try:
+        _, info = run()
+    finally:
+        lib.cf_sgemm_bf16x6_set_wait_limit(-1)
+    assert (info.cpu().numpy() == _lib.CF_ERR_TIMEOUT).all(), info
+    A, info = run()
+    assert int(info.abs().max()) == 0
+    L64 = torch.linalg.cholesky(A64)
+    assert float((torch.tril(A.double()) - L64).abs().max() / L64.abs().max()) <= 1e-5

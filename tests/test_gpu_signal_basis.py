@@ -4,11 +4,11 @@ The basis path forms each block region of C as one GEMM of the points'
 beam-smoothed tables against basis matrices the pair kernel built once
 (``cosmocore/signal_kernels.py:164-502`` per basis entry), so it differs from
 the direct per-point build only in the order of the multipole sum.  Checks:
-C against the direct build at 1e-13 (relative to the largest entry), the FP32
-tensor-core build of the mixed path at 1e-6, the likelihood through the basis
-against the reference's outputs at 1e-10, and the basis and direct
-likelihoods on 256 Sobol points (FP64 at 1e-10 relative, mixed at 5e-3 in
-lnL).
+C against the direct build at 1e-13 (relative to the largest entry), the
+lower-triangle build with its FP32 copy against the full one (bit for bit),
+the FP32 tensor-core build at 1e-6, the likelihood through the basis against
+the reference's outputs at 1e-10, and the basis and direct likelihoods on 256
+Sobol points (FP64 at 1e-10, mixed at 1e-6 relative).
 """
 
 import numpy as np
@@ -67,6 +67,24 @@ def test_basis_covariance_f32_on_tensor_cores(config3):
     assert e <= 1e-6, e
 
 
+def test_basis_covariance_lower_and_fp32_copy(config3):
+    """The likelihood's build: lower triangle only (mirror spans left out,
+    tiles right of each row of a diagonal block skipped) with the FP32 copy
+    from the same epilogue.  Every lower entry equals the full build's bit for
+    bit, and the copy is its FP32 rounding."""
+    E, L, N, th, cl = config3
+    s = torch.from_numpy(th[:, 4].copy()).cuda()
+    basis = E.signal_basis(N)
+    full = basis.covariance(cl, s)
+    B, n = cl.shape[0], L.n
+    C = torch.full((B, n, n), float("nan"), dtype=torch.float64, device="cuda")
+    C32 = torch.full((B, n, n), float("nan"), dtype=torch.float32, device="cuda")
+    basis.covariance(cl, s, out=C, lower=True, out32=C32)
+    low = torch.tril(torch.ones((n, n), dtype=torch.bool, device="cuda"))
+    assert torch.equal(C[:, low], full[:, low])
+    assert torch.equal(C32[:, low], full[:, low].float())
+
+
 def test_basis_likelihood_matches_reference():
     from cosmoforge_b200 import engine, workloads
     from cosmoforge_b200.layout import build_layout
@@ -94,10 +112,5 @@ def test_basis_and_direct_likelihoods_agree(config3, precision):
     _, _, lb, ib = E.lnl(cl, N, X, noise_scale=th[:, 4], precision=precision, build="basis")
     _, _, ld, idd = E.lnl(cl, N, X, noise_scale=th[:, 4], precision=precision, build="direct")
     assert int(ib.abs().max()) == 0 and int(idd.abs().max()) == 0
-    if precision == "fp64":
-        assert float(((lb - ld).abs() / ld.abs()).max()) <= 1e-10
-    else:
-        # the basis build forms the mixed C in FP32 on the tensor cores, the
-        # direct build in FP64: the two refined likelihoods agree to well
-        # below the mixed path's 0.05 bar on |dlnL|
-        assert float((lb - ld).abs().max()) <= 5e-3
+    tol = 1e-10 if precision == "fp64" else 1e-6
+    assert float(((lb - ld).abs() / ld.abs()).max()) <= tol

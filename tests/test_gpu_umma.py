@@ -75,8 +75,9 @@ SHAPES = [(384, 640, 512), (200, 300, 100), (2048, 4352, 2112)]
 
 
 # GEMM forms (cf_umma_set_all_planes): 1 = all planes of a 32-wide k-slice per
-# stage, 0 = 64-wide k-tiles term by term.
-@pytest.mark.parametrize("form", [1, 0])
+# stage, 2 = the same on CTA pairs (three planes; two planes fall back to 1),
+# 0 = 64-wide k-tiles term by term.
+@pytest.mark.parametrize("form", [1, 2, 0])
 @pytest.mark.parametrize("M,N,K", SHAPES)
 @pytest.mark.parametrize("terms,planes,tol", [(X3, 2, 2e-4), (X6, 3, 2e-6), (X3, 3, 2e-4)])
 def test_umma_split_products(terms, planes, tol, M, N, K, form):
