@@ -361,8 +361,8 @@ def secondary(args, dev):
            "build": "lower triangle of C(theta) from the per-multipole basis (one FP64 GEMM per block region; "
                     "mixed: the FP32 copy from the same epilogue); tc build: C in FP32 from BF16x6 tensor-core "
                     "products",
-           "mixed_form": "FP32 Cholesky (diagonal blocks per CTA, panel solves and narrow updates on a one-tile "
-                         "tcgen05 kernel, trailing updates on the persistent tcgen05 kernel, BF16x6 products), "
+           "mixed_form": "FP32 Cholesky (diagonal blocks per CTA; panel solves, in-pass and trailing updates as "
+                         "BF16x6 products on the one-tile tcgen05 kernel, the work panel as split planes), "
                          "FP64-refined chi2 against the FP64 C"}
     if int(os.environ.get("WORLD_SIZE", "1")) == 1 and not args.no_cpu_baseline:
         from oracle import oracle as orc

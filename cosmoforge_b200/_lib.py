@@ -75,6 +75,7 @@ SIGNATURES = {
     "cf_sgemm_bf16x6_set_wait_limit": (C.c_longlong, [C.c_longlong]),
     "cf_sgemm_bf16x6_set_stages": (_i, [_i]),
     "cf_potrf_f32_set_tensor": (_i, [_i]),
+    "cf_potrf_f32_set_group": (_i, [_i]),
     "cf_axpby_f32": (_i, [_l, _d, _p, _l, _d, _p, _p, _l, _p, _l, _p, _l, _i, _p]),
     "cf_chi2_logdet_mixed": (_i, [_i, _p, _l, _l, _p, _l, _l, _i, _p, _l, _l, _i, _p, _p, _p]),
     "cf_chi2_logdet_mixed_c32": (_i, [_i, _p, _l, _l, _p, _l, _l, _i, _p, _l, _l, _i, _p, _p, _p]),

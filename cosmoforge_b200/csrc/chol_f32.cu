@@ -26,6 +26,11 @@ constexpr int NB = cf_diag::NB;
 
 using cf_diag::k_potrf_diag_inv;
 
+// Panels of 64 columns factored per pass before one trailing update (K = 64
+// per panel): 2 or 4.
+constexpr int MAX_GROUP = 4;
+int g_potrf_f32_group = 2;
+
 // Product kernel of the FP32 factor's panel solves and trailing updates:
 // 1 = BF16x6 split products on the tensor cores (tc_sgemm.cu, default),
 // 0 = the FP32 SIMT kernel below.
@@ -153,7 +158,7 @@ struct Panel {
     float* f;
     long ws;
     int n;
-    static constexpr int LD = 2 * NB;
+    static constexpr int LD = MAX_GROUP * NB;  // columns: the panels of one pass
     __nv_bfloat16* planes() const { return reinterpret_cast<__nv_bfloat16*>(f); }
     long plane_stride() const { return (long)n * LD; }
 };
@@ -308,8 +313,8 @@ __global__ void __launch_bounds__(CNT) k_logdet_f32(int n, const float* L, long 
 }
 
 // floats per problem: two diagonal-block inverses and the work panel (FP32, or
-// three BF16 planes of it: 3 n 2 NB BF16 = 3 n NB floats)
-inline size_t potrf_f32_ws(int n) { return (size_t)2 * NB * NB + (size_t)3 * n * NB; }
+// three BF16 planes of it: 3 n LD BF16 = 3 n LD / 2 floats)
+inline size_t potrf_f32_ws(int n) { return (size_t)2 * NB * NB + (size_t)3 * n * Panel::LD / 2; }
 
 }  // namespace
 
@@ -322,12 +327,21 @@ extern "C" int cf_potrf_f32_set_tensor(int on)
     return prev;
 }
 
+// Panels per pass of cf_potrf_f32 (2 or 4: one trailing update per 128 or 256
+// columns).  Returns the previous setting.
+extern "C" int cf_potrf_f32_set_group(int panels)
+{
+    const int prev = g_potrf_f32_group;
+    if (panels == 2 || panels == 4) g_potrf_f32_group = panels;
+    return prev;
+}
+
 extern "C" size_t cf_potrf_f32_workspace(int n, int batch) { return potrf_f32_ws(n) * sizeof(float) * (size_t)batch; }
 
 // Blocked FP32 Cholesky in place (lower factor), batched: per 64-wide panel the
 // diagonal block is factored and inverted by one CTA and L21 = A21 L11^-T is a
-// GEMM; panels go in pairs so the trailing update A22 -= L21 L21^T runs once
-// per 128 columns.  The GEMMs are BF16x6 split products on the tensor cores
+// GEMM; panels go in passes of four (cf_potrf_f32_set_group) so the trailing
+// update A22 -= L21 L21^T runs once per 256 columns.  The GEMMs are BF16x6 split products on the tensor cores
 // unless cf_potrf_f32_set_tensor(0) selects the SIMT kernel: each panel solve
 // writes its panel into the matrix (FP32) and into the work panel as three
 // BF16 split planes, which the updates then copy straight into shared memory.
@@ -342,33 +356,42 @@ extern "C" int cf_potrf_f32(int n, float* A, long lda, long strideA, int batch, 
     float* D2 = D1 + (long)NB * NB;  // [batch][NB][NB]
     const Panel W{D2 + (long)NB * NB, ws, n};
     constexpr size_t DSM = cf_diag::smem_bytes<float>();
-    // Panels in pairs with a look-ahead (see cf_potrf): one K = 128 trailing
-    // update per 128 columns.
-    for (int k0 = 0; k0 < n; k0 += 2 * NB) {
-        const int kb1 = n - k0 < NB ? n - k0 : NB;
-        k_potrf_diag_inv<float><<<batch, cf_diag::NTHREADS, DSM, st>>>(A, lda, strideA, k0, kb1, D1, ws, info);
-        CF_CHECK_LAUNCH();
-        const int rest1 = n - k0 - kb1;
-        if (rest1 <= 0) break;
-        float* a21_1 = A + (long)(k0 + kb1) * lda + k0;
-        // panel 1 into W rows 0.., columns 0..kb1
-        int rc = panel_solve(rest1, kb1, a21_1, lda, strideA, D1, W, 0, 0, batch, info, st);
-        if (rc) return rc;
-        const int kb2 = rest1 < NB ? rest1 : NB;
-        // panel 2's columns, every row below panel 1
-        rc = panel_update(rest1, kb2, kb1, W, 0, 0, a21_1 + kb1, lda, strideA, batch, 0, info, st);
-        if (rc) return rc;
-        const int k1 = k0 + kb1;
-        k_potrf_diag_inv<float><<<batch, cf_diag::NTHREADS, DSM, st>>>(A, lda, strideA, k1, kb2, D2, ws, info);
-        CF_CHECK_LAUNCH();
-        const int rest2 = rest1 - kb2;
-        if (rest2 <= 0) break;
-        float* a21_2 = A + (long)(k1 + kb2) * lda + k1;
-        // panel 2 into W rows kb2.., columns kb1..kb1+kb2
-        rc = panel_solve(rest2, kb2, a21_2, lda, strideA, D2, W, kb2, kb1, batch, info, st);
-        if (rc) return rc;
-        // trailing update with both panels, lower tiles
-        rc = panel_update(rest2, rest2, kb1 + kb2, W, kb2, kb2, a21_2 + kb2, lda, strideA, batch, 1, info, st);
+    const int G = g_potrf_f32_group;
+    // Passes of G panels.  W row r holds matrix row k0 + NB + r (the rows
+    // below the pass's first diagonal block); panel j's columns are W columns
+    // j NB ..  Panel j is first brought up to date with the pass's earlier
+    // panels (K = j NB), then factored and solved; one trailing update of
+    // K = G NB follows the pass, so the trailing matrix is read and written
+    // once per G NB columns.
+    for (int k0 = 0; k0 < n; k0 += G * NB) {
+        int kdone = 0;
+        bool last = false;
+        for (int jp = 0; jp < G; ++jp) {
+            const int kj = k0 + jp * NB;
+            const int kbj = n - kj < NB ? n - kj : NB;
+            if (jp > 0) {
+                int rc = panel_update(n - kj, kbj, kdone, W, (jp - 1) * NB, (jp - 1) * NB,
+                                      A + (long)kj * lda + kj, lda, strideA, batch, 0, info, st);
+                if (rc) return rc;
+            }
+            float* D = (jp & 1) ? D2 : D1;
+            k_potrf_diag_inv<float><<<batch, cf_diag::NTHREADS, DSM, st>>>(A, lda, strideA, kj, kbj, D, ws, info);
+            CF_CHECK_LAUNCH();
+            const int rest = n - kj - kbj;
+            if (rest <= 0) {
+                last = true;
+                break;
+            }
+            int rc = panel_solve(rest, kbj, A + (long)(kj + kbj) * lda + kj, lda, strideA, D, W, jp * NB, jp * NB,
+                                 batch, info, st);
+            if (rc) return rc;
+            kdone += kbj;
+        }
+        if (last) break;
+        // trailing update with the pass's panels, lower tiles
+        const int t0 = k0 + G * NB;
+        int rc = panel_update(n - t0, n - t0, kdone, W, (G - 1) * NB, (G - 1) * NB, A + (long)t0 * (lda + 1), lda,
+                              strideA, batch, 1, info, st);
         if (rc) return rc;
     }
     return CF_OK;

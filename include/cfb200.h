@@ -390,6 +390,11 @@ int cf_sgemm_bf16x6_set_stages(int stages);
  * No counterpart in the reference. */
 int cf_potrf_f32_set_tensor(int on);
 
+/* Panels of 64 columns per pass of cf_potrf_f32 (2 or 4; default 4): the
+ * trailing update runs once per pass with K = 64 x panels.  Returns the
+ * previous setting.  No counterpart in the reference. */
+int cf_potrf_f32_set_group(int panels);
+
 /* Blocked lower Cholesky in FP32, in place (batch), 64-wide panels with FP32
  * GEMM updates; info as for cf_potrf.  The factor of the mixed likelihood:
  * replaces cosmocore/basics/linalg.py:362-406 (cholesky_factor) at FP32. */

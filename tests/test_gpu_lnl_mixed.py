@@ -30,8 +30,11 @@ def _spd_batch(n, batch, seed):
     return R @ R.transpose(1, 2) / n + torch.eye(n, dtype=torch.float64, device="cuda")
 
 
+@pytest.mark.parametrize("group", [4, 2])
 @pytest.mark.parametrize("n,batch", [(200, 3), (333, 2), (1000, 3), (1312, 2)])
-def test_potrf_f32_matches_fp64_factor(n, batch):
+def test_potrf_f32_matches_fp64_factor(n, batch, group):
+    """Passes of 4 (default) or 2 panels: ragged last passes (n not a multiple
+    of 256 or 128), narrow in-pass updates of K = 64 .. 192."""
     from cosmoforge_b200 import _lib
 
     lib = _lib.lib()
@@ -39,8 +42,12 @@ def test_potrf_f32_matches_fp64_factor(n, batch):
     A = C.float().contiguous()
     info = torch.zeros(batch, dtype=torch.int32, device="cuda")
     work = torch.empty(lib.cf_potrf_f32_workspace(n, batch) // 4 + 1, dtype=torch.float32, device="cuda")
-    assert lib.cf_potrf_f32(n, A.data_ptr(), n, n * n, batch, work.data_ptr(), info.data_ptr(),
-                            torch.cuda.current_stream().cuda_stream) == 0
+    prev = lib.cf_potrf_f32_set_group(group)
+    try:
+        assert lib.cf_potrf_f32(n, A.data_ptr(), n, n * n, batch, work.data_ptr(), info.data_ptr(),
+                                torch.cuda.current_stream().cuda_stream) == 0
+    finally:
+        lib.cf_potrf_f32_set_group(prev)
     assert int(info.abs().max()) == 0
     L64 = torch.linalg.cholesky(C)
     L32 = torch.tril(A.double())
