@@ -64,7 +64,7 @@ def map_solves(E: eng.Engine, Cinv: torch.Tensor, X: torch.Tensor, precision: st
         raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
     plan = MixedPlan(E, scheme)
     Pl = plan.planes
-    Yt = E.gemm(X, Cinv, transa=True)  # (C^-1 X)^T = X^T C^-1
+    Yt = Y.t().contiguous()  # X^T C^-1 = (C^-1 X)^T: C^-1 is symmetric, so a transpose, not a second GEMM
     Ytp = {}
     for fi, f in enumerate(L.fields):
         ldk = _r8(f.nrows)

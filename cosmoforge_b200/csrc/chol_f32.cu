@@ -29,7 +29,7 @@ using cf_diag::k_potrf_diag_inv;
 // Panels of 64 columns factored per pass before one trailing update (K = 64
 // per panel): 2 or 4.
 constexpr int MAX_GROUP = 4;
-int g_potrf_f32_group = 2;
+int g_potrf_f32_group = 4;
 
 // Product kernel of the FP32 factor's panel solves and trailing updates:
 // 1 = BF16x6 split products on the tensor cores (tc_sgemm.cu, default),
