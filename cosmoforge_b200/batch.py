@@ -72,6 +72,20 @@ def map_solves(E: eng.Engine, Cinv: torch.Tensor, X: torch.Tensor, precision: st
         check(E.lib.cf_split_bf16(m, f.nrows, _ptr(Yt, f.offset), n, Pl, buf.data_ptr(), ldk, m * ldk, st),
               "cf_split_bf16")
         Ytp[fi] = buf
+    # all planes per stage on CTA pairs (the split-product GEMM's fastest form here)
+    prev_form = E.lib.cf_umma_set_all_planes(2)
+    try:
+        _map_solve_spectra(E, L, plan, Ytp, Y, q, m, nb, P, st)
+    finally:
+        E.lib.cf_umma_set_all_planes(prev_form)
+    check(E.lib.cf_umma_status(plan.err.data_ptr(), stream()), "tensor-core kernel")
+    return q
+
+
+def _map_solve_spectra(E, L, plan, Ytp, Y, q, m, nb, P, st):
+    """q_b += 1/2 y^T dC_b y for every bin: per spectrum and column segment, the
+    split-product GEMM W = dC_b-planes . Y^T-planes and the q reduction."""
+    Pl = plan.planes
     for s in range(L.nspectra):
         blk, ops = _build_planes(plan, s)
         for seg, (B, K, kseg) in ops.items():
@@ -87,8 +101,6 @@ def map_solves(E: eng.Engine, Cinv: torch.Tensor, X: torch.Tensor, precision: st
                                             q.data_ptr(), P, s * nb, st), "cf_qform_reduce_f32")
             del W
         del ops
-    check(E.lib.cf_umma_status(plan.err.data_ptr(), stream()), "tensor-core kernel")
-    return q
 
 
 class _PatchGroup:

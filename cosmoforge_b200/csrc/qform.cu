@@ -4,8 +4,9 @@
 // blocks, Y = C^-1 X holds the maps in its columns),
 //   q[m, p0 + b] += scale sum_{j < J} W[b * rows_per_bin + j, m] Y[yoff + j, m],
 // i.e. q_b(m) = 1/2 y_m^T dC_b y_m of qube/spectra.py:1124-1186 for every map
-// m at once.  One thread per (bin, map, chunk of rows): both reads coalesce
-// across maps; the rows of a bin are split over enough CTAs to fill the GPU
+// m at once.  One thread per (bin, map, chunk of rows), eight rows (sixteen
+// loads) in flight per step: both reads coalesce across maps; the rows of a
+// bin are split over enough CTAs to fill the GPU
 // (W is read once from HBM, the Y rows of a chunk stay in L2 across bins), and
 // the partial sums meet in q by FP64 atomics.
 #include "cf_common.cuh"
@@ -23,14 +24,22 @@ __global__ void k_qform(int nb, int J, long rows_per_bin, const WT* W, long ldW,
     if (m >= nmaps || b >= nb || j0 >= j1) return;
     const WT* w = W + (long)b * rows_per_bin * ldW + m;
     const double* y = Y + yoff * ldY + m;
-    double a0 = 0.0, a1 = 0.0;
+    // eight rows per step, all sixteen loads issued before the products
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
     int j = j0;
-    for (; j + 1 < j1; j += 2) {
-        a0 += (double)w[(long)j * ldW] * y[(long)j * ldY];
-        a1 += (double)w[(long)(j + 1) * ldW] * y[(long)(j + 1) * ldY];
+    for (; j + 7 < j1; j += 8) {
+        WT wv[8];
+        double yv[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            wv[u] = w[(long)(j + u) * ldW];
+            yv[u] = y[(long)(j + u) * ldY];
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) acc[u & 3] += (double)wv[u] * yv[u];
     }
-    if (j < j1) a0 += (double)w[(long)j * ldW] * y[(long)j * ldY];
-    atomicAdd(q + (long)m * ldq + p0 + b, scale * (a0 + a1));
+    for (; j < j1; ++j) acc[0] += (double)w[(long)j * ldW] * y[(long)j * ldY];
+    atomicAdd(q + (long)m * ldq + p0 + b, scale * ((acc[0] + acc[1]) + (acc[2] + acc[3])));
 }
 
 template <typename WT>
