@@ -52,6 +52,8 @@ SIGNATURES = {
     "cf_qml_reduce_f64": (_i, [_i, _i, _i, _p, _l, _l, _p, _l, _l, _l, _p, _l, _i, _l, _l, _d, _p,
                                _p, _l, _p]),
     "cf_chi2_logdet": (_i, [_i, _p, _l, _l, _i, _p, _l, _l, _i, _p, _p, _p, _p]),
+    "cf_chi2_logdet_dinv": (_i, [_i, _p, _l, _l, _p, _l, _i, _p, _l, _l, _i, _p, _p, _p]),
+    "cf_potrf_dinv_stride": (_sz, [_i]),
     "cf_axpby": (_i, [_l, _d, _p, _l, _d, _p, _p, _l, _p, _l, _i, _p]),
     "cf_transpose": (_i, [_i, _i, _p, _l, _p, _l, _p]),
     "cf_umma_trace_bf16": (_i, [_i, _i, _i, _i, _i, _p, _p, _p, _l, _l, _l, _i, _p, _l, _l, _l, _i, _d,
@@ -79,6 +81,9 @@ SIGNATURES = {
     "cf_axpby_f32": (_i, [_l, _d, _p, _l, _d, _p, _p, _l, _p, _l, _p, _l, _i, _p]),
     "cf_chi2_logdet_mixed": (_i, [_i, _p, _l, _l, _p, _l, _l, _i, _p, _l, _l, _i, _p, _p, _p]),
     "cf_chi2_logdet_mixed_c32": (_i, [_i, _p, _l, _l, _p, _l, _l, _i, _p, _l, _l, _i, _p, _p, _p]),
+    "cf_chi2_logdet_mixed_dinv": (_i, [_i, _p, _l, _l, _p, _l, _p, _l, _l, _i, _p, _l, _l, _i, _p, _p, _p]),
+    "cf_chi2_logdet_mixed_c32_dinv": (_i, [_i, _p, _l, _l, _p, _l, _p, _l, _l, _i, _p, _l, _l, _i, _p, _p, _p]),
+    "cf_potrf_f32_dinv_stride": (_sz, [_i]),
     "cf_mlp_dense_fwd": (_i, [_i, _i, _i, _p, _l, _p, _p, _i, _p, _p, _l, _p]),
     "cf_mlp_dense_bwd_data": (_i, [_i, _i, _i, _p, _p, _p, _p, _p]),
     "cf_mlp_dense_bwd_weight": (_i, [_i, _i, _i, _p, _p, _l, _p, _p, _p]),

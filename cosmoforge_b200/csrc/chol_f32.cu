@@ -296,6 +296,77 @@ __global__ void __launch_bounds__(CNT, 2) k_chi2_refined(int n, const float* L, 
     }
 }
 
+// k_chi2_refined with the FP32 factor's diagonal-block inverses D: 64-row
+// blocks, each diagonal solve a block-times-vector product (forward with D,
+// backward with D^T), the rows below / columns left of the block and the
+// quadratic-form strip as in k_chi2_refined.
+template <bool VL, bool VC, typename TC>
+__global__ void __launch_bounds__(CNT, 2) k_chi2_refined_dinv(int n, const float* L, long lda, long sL,
+                                                              const float* D, long sD, const TC* C, long ldc,
+                                                              long sC, const double* X, long ldx, long sX, int nrhs,
+                                                              double* chi2)
+{
+    extern __shared__ double sh[];
+    double* w = sh;
+    double* v = sh + n;
+    double* tb = sh + 2 * n;  // 64 doubles: a block's solution before it replaces the right-hand side
+    const int b = blockIdx.x / nrhs, m = blockIdx.x % nrhs;
+    L += (long)b * sL;
+    D += (long)b * sD;
+    C += (long)b * sC;
+    X += (long)b * sX;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    __shared__ double red[CNT / 32];
+    for (int i = tid; i < n; i += CNT) w[i] = X[(long)i * ldx + m];
+    __syncthreads();
+    const int nb64 = (n + 63) / 64;
+    for (int blk = 0; blk < nb64; ++blk) {
+        const int b0 = blk * 64, kb = n - b0 < 64 ? n - b0 : 64;
+        cf_tri::block_matvec<float, false>(D + (long)blk * 64 * 64, kb, w + b0, tb, tid);
+        __syncthreads();
+        if (tid < kb) w[b0 + tid] = tb[tid];
+        __syncthreads();
+        for (int r = b0 + kb + tid; r < n; r += CNT) w[r] -= cf_tri::seg_dot64<VL>(L + (long)r * lda + b0, w + b0, kb);
+        __syncthreads();
+    }
+    double s = 0.0;
+    for (int i = tid; i < n; i += CNT) {
+        v[i] = w[i];
+        s += 2.0 * w[i] * w[i];
+    }
+    __syncthreads();
+    double qf = 0.0;  // this thread's share of v^T C v
+    for (int blk = nb64 - 1; blk >= 0; --blk) {
+        const int b0 = blk * 64, kb = n - b0 < 64 ? n - b0 : 64;
+        cf_tri::block_matvec<float, true>(D + (long)blk * 64 * 64, kb, v + b0, tb, tid);
+        __syncthreads();
+        if (tid < kb) v[b0 + tid] = tb[tid];
+        __syncthreads();
+        for (int q = tid; q < n; q += CNT) {
+            if (q < b0) {
+                v[q] -= cf_tri::col_dot64(L, lda, b0, q, v + b0, kb);
+            } else if (q >= b0 + kb) {
+                qf += 2.0 * v[q] * cf_tri::seg_dot64<VC>(C + (long)q * ldc + b0, v + b0, kb);
+            } else {
+                const TC* cr = C + (long)q * ldc;
+                double t = (double)cr[q] * v[q];
+                for (int c = b0; c < q; ++c) t += 2.0 * (double)cr[c] * v[c];
+                qf += v[q] * t;
+            }
+        }
+        __syncthreads();
+    }
+    s -= qf;
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) red[warp] = s;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int q = 0; q < CNT / 32; ++q) t += red[q];
+        chi2[blockIdx.x] = t;
+    }
+}
+
 __global__ void __launch_bounds__(CNT) k_logdet_f32(int n, const float* L, long lda, long sL, double* logdet)
 {
     L += (long)blockIdx.x * sL;
@@ -312,9 +383,11 @@ __global__ void __launch_bounds__(CNT) k_logdet_f32(int n, const float* L, long 
     }
 }
 
-// floats per problem: two diagonal-block inverses and the work panel (FP32, or
-// three BF16 planes of it: 3 n LD BF16 = 3 n LD / 2 floats)
-inline size_t potrf_f32_ws(int n) { return (size_t)2 * NB * NB + (size_t)3 * n * Panel::LD / 2; }
+// floats per problem: every diagonal-block inverse (kept for the chi2 solves)
+// and the work panel (FP32, or three BF16 planes of it: 3 n LD / 2 floats)
+inline int nblk(int n) { return (n + NB - 1) / NB; }
+inline size_t potrf_f32_dinv(int n) { return (size_t)nblk(n) * NB * NB; }
+inline size_t potrf_f32_ws(int n) { return potrf_f32_dinv(n) + (size_t)3 * n * Panel::LD / 2; }
 
 }  // namespace
 
@@ -336,6 +409,10 @@ extern "C" int cf_potrf_f32_set_group(int panels)
     return prev;
 }
 
+// Floats between consecutive problems' diagonal-block inverses in the
+// cf_potrf_f32 workspace (block j of problem z at work + z stride + j 64^2).
+extern "C" size_t cf_potrf_f32_dinv_stride(int n) { return potrf_f32_ws(n); }
+
 extern "C" size_t cf_potrf_f32_workspace(int n, int batch) { return potrf_f32_ws(n) * sizeof(float) * (size_t)batch; }
 
 // Blocked FP32 Cholesky in place (lower factor), batched: per 64-wide panel the
@@ -352,9 +429,8 @@ extern "C" int cf_potrf_f32(int n, float* A, long lda, long strideA, int batch, 
     if (n <= 0 || batch < 1 || !A || !work || lda < n) return CF_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     const long ws = (long)potrf_f32_ws(n);
-    float* D1 = (float*)work;        // [batch][NB][NB]
-    float* D2 = D1 + (long)NB * NB;  // [batch][NB][NB]
-    const Panel W{D2 + (long)NB * NB, ws, n};
+    float* Dall = (float*)work;  // [batch][blocks][NB][NB]: block j's inverse at j NB^2
+    const Panel W{Dall + potrf_f32_dinv(n), ws, n};
     constexpr size_t DSM = cf_diag::smem_bytes<float>();
     const int G = g_potrf_f32_group;
     // Passes of G panels.  W row r holds matrix row k0 + NB + r (the rows
@@ -374,7 +450,7 @@ extern "C" int cf_potrf_f32(int n, float* A, long lda, long strideA, int batch, 
                                       A + (long)kj * lda + kj, lda, strideA, batch, 0, info, st);
                 if (rc) return rc;
             }
-            float* D = (jp & 1) ? D2 : D1;
+            float* D = Dall + (long)(kj / NB) * NB * NB;
             k_potrf_diag_inv<float><<<batch, cf_diag::NTHREADS, DSM, st>>>(A, lda, strideA, kj, kbj, D, ws, info);
             CF_CHECK_LAUNCH();
             const int rest = n - kj - kbj;
@@ -417,22 +493,33 @@ extern "C" int cf_axpby_f32(long count, double a, const double* X, long strideX,
 namespace {
 template <typename TC>
 int chi2_mixed(int n, const float* L, long lda, long strideL, const TC* C, long ldc, long strideC, int batch,
-               const double* X, long ldx, long strideX, int nrhs, double* chi2, double* logdet, cudaStream_t st)
+               const double* X, long ldx, long strideX, int nrhs, double* chi2, double* logdet, cudaStream_t st,
+               const float* Dinv = nullptr, long strideD = 0)
 {
     if (n <= 0 || batch < 1 || nrhs < 0 || !L) return CF_ERR_ARG;
-    if (n > 12288) return CF_ERR_UNSUPPORTED;
+    if (n > 12288 - 32) return CF_ERR_UNSUPPORTED;
     if (nrhs > 0) {
         if (!X || !C || !chi2) return CF_ERR_ARG;
-        const size_t smem = 2 * (size_t)n * sizeof(double);
+        const size_t smem = (2 * (size_t)n + 64) * sizeof(double);
         constexpr long VW = 16 / sizeof(TC);  // elements per 16-byte vector
         const bool vl = ((uintptr_t)L & 15) == 0 && (lda & 3) == 0 && (batch == 1 || (strideL & 3) == 0);
         const bool vc = ((uintptr_t)C & 15) == 0 && (ldc % VW) == 0 && (batch == 1 || (strideC % VW) == 0);
-        auto kern = vl ? (vc ? k_chi2_refined<true, true, TC> : k_chi2_refined<true, false, TC>)
-                       : (vc ? k_chi2_refined<false, true, TC> : k_chi2_refined<false, false, TC>);
-        static std::atomic<int> attr[4][CF_MAX_DEVICES];
-        int rc = cf_smem_optin(kern, 2 * 12288 * (int)sizeof(double), attr[2 * vl + vc]);
-        if (rc) return rc;
-        kern<<<batch * nrhs, CNT, smem, st>>>(n, L, lda, strideL, C, ldc, strideC, X, ldx, strideX, nrhs, chi2);
+        if (Dinv) {
+            auto kern = vl ? (vc ? k_chi2_refined_dinv<true, true, TC> : k_chi2_refined_dinv<true, false, TC>)
+                           : (vc ? k_chi2_refined_dinv<false, true, TC> : k_chi2_refined_dinv<false, false, TC>);
+            static std::atomic<int> attr[4][CF_MAX_DEVICES];
+            int rc = cf_smem_optin(kern, 2 * 12288 * (int)sizeof(double), attr[2 * vl + vc]);
+            if (rc) return rc;
+            kern<<<batch * nrhs, CNT, smem, st>>>(n, L, lda, strideL, Dinv, strideD, C, ldc, strideC, X, ldx,
+                                                  strideX, nrhs, chi2);
+        } else {
+            auto kern = vl ? (vc ? k_chi2_refined<true, true, TC> : k_chi2_refined<true, false, TC>)
+                           : (vc ? k_chi2_refined<false, true, TC> : k_chi2_refined<false, false, TC>);
+            static std::atomic<int> attr[4][CF_MAX_DEVICES];
+            int rc = cf_smem_optin(kern, 2 * 12288 * (int)sizeof(double), attr[2 * vl + vc]);
+            if (rc) return rc;
+            kern<<<batch * nrhs, CNT, smem, st>>>(n, L, lda, strideL, C, ldc, strideC, X, ldx, strideX, nrhs, chi2);
+        }
         CF_CHECK_LAUNCH();
     }
     if (logdet) {
@@ -463,4 +550,28 @@ extern "C" int cf_chi2_logdet_mixed_c32(int n, const float* L, long lda, long st
 {
     return chi2_mixed<float>(n, L, lda, strideL, C, ldc, strideC, batch, X, ldx, strideX, nrhs, chi2, logdet,
                              (cudaStream_t)stream);
+}
+
+// cf_chi2_logdet_mixed / cf_chi2_logdet_mixed_c32 with the FP32 factor's
+// diagonal-block inverses as cf_potrf_f32 leaves them in its workspace (Dinv =
+// the workspace, strideD = cf_potrf_f32_dinv_stride(n) floats between
+// problems): 64-row blocks, each diagonal solve a block-times-vector product.
+extern "C" int cf_chi2_logdet_mixed_dinv(int n, const float* L, long lda, long strideL, const float* Dinv,
+                                         long strideD, const double* C, long ldc, long strideC, int batch,
+                                         const double* X, long ldx, long strideX, int nrhs, double* chi2,
+                                         double* logdet, void* stream)
+{
+    if (!Dinv) return CF_ERR_ARG;
+    return chi2_mixed<double>(n, L, lda, strideL, C, ldc, strideC, batch, X, ldx, strideX, nrhs, chi2, logdet,
+                              (cudaStream_t)stream, Dinv, strideD);
+}
+
+extern "C" int cf_chi2_logdet_mixed_c32_dinv(int n, const float* L, long lda, long strideL, const float* Dinv,
+                                             long strideD, const float* C, long ldc, long strideC, int batch,
+                                             const double* X, long ldx, long strideX, int nrhs, double* chi2,
+                                             double* logdet, void* stream)
+{
+    if (!Dinv) return CF_ERR_ARG;
+    return chi2_mixed<float>(n, L, lda, strideL, C, ldc, strideC, batch, X, ldx, strideX, nrhs, chi2, logdet,
+                             (cudaStream_t)stream, Dinv, strideD);
 }

@@ -125,6 +125,10 @@ int lookahead_init(Lookahead& la)
 
 extern "C" size_t cf_potrf_workspace(int n, int batch) { return potrf_ws_total(n, batch) * sizeof(double); }
 
+// Doubles between consecutive problems' diagonal-block inverses in the potrf
+// workspace (block j of a problem at work + z stride + j 64^2).
+extern "C" size_t cf_potrf_dinv_stride(int n) { return potrf_ws(n); }
+
 namespace {
 // One 128-column step of the factorisation up to the trailing update: factor
 // the two diagonal blocks (keeping their inverses), solve both panels into W

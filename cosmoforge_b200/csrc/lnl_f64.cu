@@ -51,6 +51,48 @@ __global__ void __launch_bounds__(NT, 2) k_chi2(int n, const double* L, long lda
     }
 }
 
+// The same chi2 with the factor's 64 x 64 diagonal-block inverses D (block j
+// at D + j 64^2, row-major with row stride kb_j): 64-row blocks, each
+// diagonal solve one block-times-vector product (no dependent chain), then
+// the rows below take the block's 64-wide segment (z in shared memory).
+template <bool VEC>
+__global__ void __launch_bounds__(NT, 2) k_chi2_dinv(int n, const double* L, long lda, long sL, const double* D,
+                                                     long sD, const double* X, long ldx, long sX, int nrhs,
+                                                     double* chi2)
+{
+    extern __shared__ double zsh[];
+    double* z = zsh;
+    double* zb = zsh + n;
+    const int b = blockIdx.x / nrhs, m = blockIdx.x % nrhs;
+    L += (long)b * sL;
+    D += (long)b * sD;
+    X += (long)b * sX;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = tid; i < n; i += NT) z[i] = X[(long)i * ldx + m];
+    __syncthreads();
+    for (int b0 = 0, blk = 0; b0 < n; b0 += 64, ++blk) {
+        const int kb = n - b0 < 64 ? n - b0 : 64;
+        cf_tri::block_matvec<double, false>(D + (long)blk * 64 * 64, kb, z + b0, zb, tid);
+        __syncthreads();
+        if (tid < kb) z[b0 + tid] = zb[tid];
+        __syncthreads();
+        for (int r = b0 + kb + tid; r < n; r += NT)
+            z[r] -= cf_tri::seg_dot64<VEC>(L + (long)r * lda + b0, z + b0, kb);
+        __syncthreads();
+    }
+    double s = 0.0;
+    for (int i = tid; i < n; i += NT) s += z[i] * z[i];
+    __shared__ double red[NT / 32];
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) red[warp] = s;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int w = 0; w < NT / 32; ++w) t += red[w];
+        chi2[blockIdx.x] = t;
+    }
+}
+
 __global__ void __launch_bounds__(NT) k_logdet(int n, const double* L, long lda, long sL, double* logdet)
 {
     L += (long)blockIdx.x * sL;
@@ -86,6 +128,35 @@ extern "C" int cf_chi2_logdet(int n, const double* L, long lda, long strideL, in
         static std::atomic<int> attr[2][CF_MAX_DEVICES];
         if (int rc = cf_smem_optin(kern, SMEM_MAX_N * (int)sizeof(double), attr[vec])) return rc;
         kern<<<batch * nrhs, NT, smem, st>>>(n, L, lda, strideL, X, ldx, strideX, nrhs, sh ? nullptr : z_work, chi2);
+        CF_CHECK_LAUNCH();
+    }
+    if (logdet) {
+        k_logdet<<<batch, NT, 0, st>>>(n, L, lda, strideL, logdet);
+        CF_CHECK_LAUNCH();
+    }
+    return CF_OK;
+}
+
+// cf_chi2_logdet with the factor's diagonal-block inverses as cf_potrf leaves
+// them in its workspace (Dinv = the workspace, strideD = cf_potrf_dinv_stride(n)
+// doubles between problems): 64-row blocks solved by block-times-vector
+// products instead of dependent substitution chains.  n <= 24576 (the solve
+// vector in shared memory).
+extern "C" int cf_chi2_logdet_dinv(int n, const double* L, long lda, long strideL, const double* Dinv, long strideD,
+                                   int batch, const double* X, long ldx, long strideX, int nrhs, double* chi2,
+                                   double* logdet, void* stream)
+{
+    if (n <= 0 || batch < 1 || nrhs < 0 || !L) return CF_ERR_ARG;
+    if (n > SMEM_MAX_N - 64) return CF_ERR_UNSUPPORTED;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (nrhs > 0) {
+        if (!X || !chi2 || !Dinv) return CF_ERR_ARG;
+        const bool vec = ((uintptr_t)L & 15) == 0 && (lda & 1) == 0 && (batch == 1 || (strideL & 1) == 0);
+        const int smem = (n + 64) * (int)sizeof(double);
+        auto kern = vec ? k_chi2_dinv<true> : k_chi2_dinv<false>;
+        static std::atomic<int> attr[2][CF_MAX_DEVICES];
+        if (int rc = cf_smem_optin(kern, SMEM_MAX_N * (int)sizeof(double), attr[vec])) return rc;
+        kern<<<batch * nrhs, NT, smem, st>>>(n, L, lda, strideL, Dinv, strideD, X, ldx, strideX, nrhs, chi2);
         CF_CHECK_LAUNCH();
     }
     if (logdet) {

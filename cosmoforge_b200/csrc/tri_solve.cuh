@@ -4,7 +4,10 @@
 // A solve runs over 32-row blocks: warp 0 solves the 32 x 32 diagonal block
 // in registers (lane = row for L z = x, lane = column for L^T v = w, one
 // shuffle per step, reciprocal pivots), then every thread of the CTA applies
-// one 32-wide segment of L to the rest of the vector.  The vector lives in
+// one 32-wide segment of L to the rest of the vector.  With the inverses of
+// the factor's 64 x 64 diagonal blocks at hand (both Cholesky kernels keep
+// them) a solve runs over 64-row blocks instead, each diagonal solve one
+// parallel block-times-vector product (block_matvec).  The vector lives in
 // shared memory; the segments are read with vector loads (a thread's 32
 // elements of one row are contiguous), all of them in flight at once.
 #pragma once
@@ -109,6 +112,40 @@ __device__ __forceinline__ double col_dot(const T* L, long lda, int b0, int i, c
         for (int k = 0; k < kb; ++k) acc += (double)c[(long)k * lda] * vb[k];
     }
     return acc;
+}
+
+// out[r] = sum_c D[r kb + c] v[c] (TRANS: D[c kb + r]) for r < kb <= 64: a
+// 64 x 64 block (row-major, row stride kb) times a vector, 256 threads, four
+// per output row (16 columns each, combined by shuffles).
+template <typename T, bool TRANS>
+__device__ __forceinline__ void block_matvec(const T* D, int kb, const double* v, double* out, int tid)
+{
+    const int r = tid >> 2, p = tid & 3;
+    double acc = 0.0;
+    if (r < kb) {
+#pragma unroll 4
+        for (int c = p * 16; c < p * 16 + 16; ++c)
+            if (c < kb) acc += (double)(TRANS ? D[(long)c * kb + r] : D[(long)r * kb + c]) * v[c];
+    }
+    acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+    if (r < kb && p == 0) out[r] = acc;
+}
+
+// Row segment of up to 64 elements (two halves of 32).
+template <bool VEC, typename T>
+__device__ __forceinline__ double seg_dot64(const T* row, const double* zb, int kb)
+{
+    if (kb <= 32) return seg_dot<VEC>(row, zb, kb);
+    return seg_dot<VEC>(row, zb, 32) + seg_dot<VEC>(row + 32, zb + 32, kb - 32);
+}
+
+// Column of a block row of up to 64 rows (two halves of 32).
+template <typename T>
+__device__ __forceinline__ double col_dot64(const T* L, long lda, int b0, int i, const double* vb, int kb)
+{
+    if (kb <= 32) return col_dot(L, lda, b0, i, vb, kb);
+    return col_dot(L, lda, b0, i, vb, 32) + col_dot(L, lda, b0 + 32, i, vb + 32, kb - 32);
 }
 
 }  // namespace cf_tri

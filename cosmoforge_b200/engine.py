@@ -331,14 +331,16 @@ class Engine:
         return F, bias, q
 
     # ------------------------------------------------------------------
-    def potrf(self, A: torch.Tensor) -> torch.Tensor:
+    def potrf(self, A: torch.Tensor, keep_work: bool = False):
+        """In-place lower Cholesky factor(s); info (and the workspace with the
+        diagonal-block inverses when keep_work)."""
         n = A.shape[-1]
         B = A.shape[0] if A.dim() == 3 else 1
         info = torch.zeros(B, dtype=torch.int32, device=A.device)
         work = torch.empty(self.lib.cf_potrf_workspace(n, B) // 8 + 1, dtype=F64, device=A.device)
         check(self.lib.cf_potrf(n, A.data_ptr(), n, n * n, B, work.data_ptr(), info.data_ptr(), stream()),
               "cf_potrf")
-        return info
+        return (info, work) if keep_work else info
 
     def signal_basis(self, N: torch.Tensor) -> "SignalBasis":
         """The per-multipole basis of C(theta) for this layout and noise (cached on N)."""
@@ -400,16 +402,21 @@ class Engine:
                 return self._lnl_mixed(C, N, maps, sc)
             check(self.lib.cf_axpby(n * n, 1.0, C.data_ptr(), n * n, 1.0, ptr(sc), N.data_ptr(), 0,
                                     C.data_ptr(), n * n, B, stream()), "cf_axpby")
-        info = self.potrf(C)
+        info, work = self.potrf(C, keep_work=True)
         X = maps.to(self.dev, F64).contiguous()
         nsims = X.shape[1]
-        # the solve vector lives in shared memory up to n = 24576, in this scratch above
-        z = torch.empty((B * nsims, n), dtype=F64, device=self.dev) if n > 24576 else None
         chi2 = torch.empty((B, nsims), dtype=F64, device=self.dev)
         logdet = torch.empty(B, dtype=F64, device=self.dev)
-        check(self.lib.cf_chi2_logdet(n, C.data_ptr(), n, n * n, B, X.data_ptr(), nsims, 0, nsims,
-                                      ptr(z), chi2.data_ptr(), logdet.data_ptr(), stream()),
-              "cf_chi2_logdet")
+        if n <= 24576 - 64:
+            # 64-row blocks solved with the factor's diagonal-block inverses
+            check(self.lib.cf_chi2_logdet_dinv(n, C.data_ptr(), n, n * n, work.data_ptr(),
+                                               self.lib.cf_potrf_dinv_stride(n), B, X.data_ptr(), nsims, 0, nsims,
+                                               chi2.data_ptr(), logdet.data_ptr(), stream()), "cf_chi2_logdet_dinv")
+        else:
+            z = torch.empty((B * nsims, n), dtype=F64, device=self.dev)
+            check(self.lib.cf_chi2_logdet(n, C.data_ptr(), n, n * n, B, X.data_ptr(), nsims, 0, nsims,
+                                          z.data_ptr(), chi2.data_ptr(), logdet.data_ptr(), stream()),
+                  "cf_chi2_logdet")
         return chi2, logdet, -0.5 * (chi2 + logdet[:, None]), info
 
     def _lnl_mixed_basis_tc(self, basis: "SignalBasis", cl: torch.Tensor, maps: torch.Tensor, sc):
@@ -428,9 +435,10 @@ class Engine:
         nsims = X.shape[1]
         chi2 = torch.empty((B, nsims), dtype=F64, device=self.dev)
         logdet = torch.empty(B, dtype=F64, device=self.dev)
-        check(self.lib.cf_chi2_logdet_mixed_c32(n, L32.data_ptr(), n, n * n, C32.data_ptr(), n, n * n, B,
-                                                X.data_ptr(), nsims, 0, nsims, chi2.data_ptr(), logdet.data_ptr(),
-                                                stream()), "cf_chi2_logdet_mixed_c32")
+        check(self.lib.cf_chi2_logdet_mixed_c32_dinv(n, L32.data_ptr(), n, n * n, work.data_ptr(),
+                                                     self.lib.cf_potrf_f32_dinv_stride(n), C32.data_ptr(), n, n * n,
+                                                     B, X.data_ptr(), nsims, 0, nsims, chi2.data_ptr(),
+                                                     logdet.data_ptr(), stream()), "cf_chi2_logdet_mixed_c32_dinv")
         # a tensor-core wait that ran out marks every point of the batch (no host sync: capturable)
         info = torch.where(err[0] != 0, torch.full_like(info, CF_ERR_TIMEOUT), info)
         return chi2, logdet, -0.5 * (chi2 + logdet[:, None]), info
@@ -451,9 +459,10 @@ class Engine:
         nsims = X.shape[1]
         chi2 = torch.empty((B, nsims), dtype=F64, device=self.dev)
         logdet = torch.empty(B, dtype=F64, device=self.dev)
-        check(self.lib.cf_chi2_logdet_mixed(n, C32.data_ptr(), n, n * n, C.data_ptr(), n, n * n, B,
-                                            X.data_ptr(), nsims, 0, nsims, chi2.data_ptr(), logdet.data_ptr(),
-                                            stream()), "cf_chi2_logdet_mixed")
+        check(self.lib.cf_chi2_logdet_mixed_dinv(n, C32.data_ptr(), n, n * n, work.data_ptr(),
+                                                 self.lib.cf_potrf_f32_dinv_stride(n), C.data_ptr(), n, n * n, B,
+                                                 X.data_ptr(), nsims, 0, nsims, chi2.data_ptr(), logdet.data_ptr(),
+                                                 stream()), "cf_chi2_logdet_mixed_dinv")
         return chi2, logdet, -0.5 * (chi2 + logdet[:, None]), info
 
 

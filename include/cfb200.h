@@ -116,6 +116,11 @@ int cf_dgemm_f32copy(int transa, int transb, int M, int N, int K, double alpha, 
 /* Bytes of workspace cf_potrf needs for `batch` problems of order n. */
 size_t cf_potrf_workspace(int n, int batch);
 
+/* Doubles between consecutive problems' diagonal-block inverses in the
+ * cf_potrf workspace (block j of problem z at work + z stride + j 64^2, row
+ * major with row stride kb_j).  No counterpart in the reference. */
+size_t cf_potrf_dinv_stride(int n);
+
 /*
  * Blocked lower Cholesky factorisation in place (batch of n x n matrices):
  * 64-wide panels, diagonal block factored and inverted by one CTA, panel and
@@ -207,6 +212,15 @@ int cf_qml_reduce_f64(int P, int R, int Ccols, const double* D, long ldD, long s
  */
 int cf_chi2_logdet(int n, const double* L, long lda, long strideL, int batch, const double* X, long ldx,
                    long strideX, int nrhs, double* z_work, double* chi2, double* logdet, void* stream);
+
+/* cf_chi2_logdet with the factor's 64 x 64 diagonal-block inverses that
+ * cf_potrf leaves in its workspace (Dinv = the workspace, strideD =
+ * cf_potrf_dinv_stride(n) doubles between problems): the solve runs over
+ * 64-row blocks, each diagonal solve one block-times-vector product instead
+ * of a dependent substitution.  n <= 24512.  Same replaced reference code. */
+int cf_chi2_logdet_dinv(int n, const double* L, long lda, long strideL, const double* Dinv, long strideD,
+                        int batch, const double* X, long ldx, long strideX, int nrhs, double* chi2,
+                        double* logdet, void* stream);
 
 /* Z_b = a X_b + c_b W_b (c_b = cvec[b] if cvec else c; strideW = 0 shares W).
  * Used for C = S + s N (picslike/picslike.py:301-319, qube/fisher.py:311-344). */
@@ -422,6 +436,23 @@ int cf_chi2_logdet_mixed(int n, const float* L, long lda, long strideL, const do
 int cf_chi2_logdet_mixed_c32(int n, const float* L, long lda, long strideL, const float* C, long ldc,
                              long strideC, int batch, const double* X, long ldx, long strideX, int nrhs,
                              double* chi2, double* logdet, void* stream);
+
+/* The two mixed chi2 forms with the FP32 factor's diagonal-block inverses as
+ * cf_potrf_f32 leaves them in its workspace (strideD =
+ * cf_potrf_f32_dinv_stride(n) floats between problems): 64-row blocks, each
+ * diagonal solve a block-times-vector product.  Same replaced reference code. */
+int cf_chi2_logdet_mixed_dinv(int n, const float* L, long lda, long strideL, const float* Dinv, long strideD,
+                              const double* C, long ldc, long strideC, int batch, const double* X, long ldx,
+                              long strideX, int nrhs, double* chi2, double* logdet, void* stream);
+int cf_chi2_logdet_mixed_c32_dinv(int n, const float* L, long lda, long strideL, const float* Dinv,
+                                  long strideD, const float* C, long ldc, long strideC, int batch,
+                                  const double* X, long ldx, long strideX, int nrhs, double* chi2,
+                                  double* logdet, void* stream);
+
+/* Floats between consecutive problems' diagonal-block inverses in the
+ * cf_potrf_f32 workspace (it keeps every one).  No counterpart in the
+ * reference. */
+size_t cf_potrf_f32_dinv_stride(int n);
 
 /* ---- Quadratic forms of many maps ----
  * q[m ldq + p0 + b] += scale sum_{j<J} W[(b rows_per_bin + j) ldW + m] Y[(yoff + j) ldY + m]

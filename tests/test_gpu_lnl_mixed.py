@@ -282,3 +282,44 @@ def test_potrf_f32_tensor_cores_vs_simt(n, batch):
     finally:
         lib.cf_potrf_f32_set_tensor(prev)
     assert errs[1] <= max(4 * errs[0], 2e-6), errs
+
+
+@pytest.mark.parametrize("n,batch", [(200, 3), (333, 2), (1312, 4)])
+def test_chi2_with_block_inverses_matches_substitution(n, batch):
+    """The chi2 kernels that solve 64-row blocks with the factors' kept
+    diagonal-block inverses against the 32-row substitution kernels: FP64 to
+    1e-12 relative, the FP64-refined mixed chi2 to 1e-10."""
+    from cosmoforge_b200 import _lib
+
+    lib = _lib.lib()
+    st = torch.cuda.current_stream().cuda_stream
+    C = _spd_batch(n, batch, 7 + n)
+    g = torch.Generator(device="cuda").manual_seed(n)
+    X = torch.randn((n, 2), dtype=torch.float64, device="cuda", generator=g) * 3.0
+    # FP64
+    L = C.clone()
+    info = torch.zeros(batch, dtype=torch.int32, device="cuda")
+    work = torch.empty(lib.cf_potrf_workspace(n, batch) // 8 + 1, dtype=torch.float64, device="cuda")
+    assert lib.cf_potrf(n, L.data_ptr(), n, n * n, batch, work.data_ptr(), info.data_ptr(), st) == 0
+    c_sub = torch.empty((batch, 2), dtype=torch.float64, device="cuda")
+    c_inv = torch.empty_like(c_sub)
+    ld1 = torch.empty(batch, dtype=torch.float64, device="cuda")
+    ld2 = torch.empty_like(ld1)
+    assert lib.cf_chi2_logdet(n, L.data_ptr(), n, n * n, batch, X.data_ptr(), 2, 0, 2, None, c_sub.data_ptr(),
+                              ld1.data_ptr(), st) == 0
+    assert lib.cf_chi2_logdet_dinv(n, L.data_ptr(), n, n * n, work.data_ptr(), lib.cf_potrf_dinv_stride(n), batch,
+                                   X.data_ptr(), 2, 0, 2, c_inv.data_ptr(), ld2.data_ptr(), st) == 0
+    assert float(((c_inv - c_sub).abs() / c_sub).max()) <= 1e-12
+    assert torch.equal(ld1, ld2)
+    # mixed
+    L32 = C.float().contiguous()
+    work32 = torch.empty(lib.cf_potrf_f32_workspace(n, batch) // 4 + 1, dtype=torch.float32, device="cuda")
+    assert lib.cf_potrf_f32(n, L32.data_ptr(), n, n * n, batch, work32.data_ptr(), info.data_ptr(), st) == 0
+    assert lib.cf_chi2_logdet_mixed(n, L32.data_ptr(), n, n * n, C.data_ptr(), n, n * n, batch, X.data_ptr(), 2, 0,
+                                    2, c_sub.data_ptr(), ld1.data_ptr(), st) == 0
+    assert lib.cf_chi2_logdet_mixed_dinv(n, L32.data_ptr(), n, n * n, work32.data_ptr(),
+                                         lib.cf_potrf_f32_dinv_stride(n), C.data_ptr(), n, n * n, batch,
+                                         X.data_ptr(), 2, 0, 2, c_inv.data_ptr(), ld2.data_ptr(), st) == 0
+    torch.cuda.synchronize()
+    assert int(info.abs().max()) == 0
+    assert float(((c_inv - c_sub).abs() / c_sub).max()) <= 1e-10
