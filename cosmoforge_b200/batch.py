@@ -34,6 +34,10 @@ def _ptr(t, off=0):
     return t.data_ptr() + off * t.element_size()
 
 
+def _ptr16(t: torch.Tensor, elems: int) -> int:
+    return t.data_ptr() + int(elems) * t.element_size()
+
+
 def map_solves(E: eng.Engine, Cinv: torch.Tensor, X: torch.Tensor, precision: str = "fp64",
                scheme: str = "bf16x6") -> torch.Tensor:
     """Raw q (nmaps x P) for the maps in the columns of X (n x nmaps), no bias removed."""
@@ -41,10 +45,10 @@ def map_solves(E: eng.Engine, Cinv: torch.Tensor, X: torch.Tensor, precision: st
     n, nb, P = L.n, L.nbins, L.n_params
     X = X.to(E.dev, F64).contiguous()
     m = X.shape[1]
-    Y = E.gemm(Cinv, X)
     q = torch.zeros((m, P), dtype=F64, device=E.dev)
     st = stream()
     if precision == "fp64":
+        Y = E.gemm(Cinv, X)
         for s in range(L.nspectra):
             blk, D = E._deriv_blocks(s)
             fa, fb = L.fields[blk.fa], L.fields[blk.fb]
@@ -63,19 +67,28 @@ def map_solves(E: eng.Engine, Cinv: torch.Tensor, X: torch.Tensor, precision: st
     if precision != "mixed":
         raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
     plan = MixedPlan(E, scheme)
-    Pl = plan.planes
-    Yt = Y.t().contiguous()  # X^T C^-1 = (C^-1 X)^T: C^-1 is symmetric, so a transpose, not a second GEMM
-    Ytp = {}
-    for fi, f in enumerate(L.fields):
-        ldk = _r8(f.nrows)
-        buf = torch.zeros((Pl, m, ldk), dtype=torch.bfloat16, device=E.dev)
-        check(E.lib.cf_split_bf16(m, f.nrows, _ptr(Yt, f.offset), n, Pl, buf.data_ptr(), ldk, m * ldk, st),
-              "cf_split_bf16")
-        Ytp[fi] = buf
+    Pl, npd = plan.planes, plan.n_pad
+    # Y = C^-1 X as a split-product GEMM too (fields padded to multiples of 8):
+    # its epilogue writes Y in FP32 (for the reductions) and the split planes of
+    # Y^T that the per-spectrum GEMMs read, so no FP64 GEMM, transpose or split
+    Cp = plan.split_cinv(Cinv)
+    Xt = plan.pad_rows(X).t().contiguous()  # m x npd
+    Xtp = torch.zeros((Pl, m, npd), dtype=torch.bfloat16, device=E.dev)
+    check(E.lib.cf_split_bf16(m, npd, Xt.data_ptr(), npd, Pl, Xtp.data_ptr(), npd, m * npd, st), "cf_split_bf16")
+    del Xt
+    YTp = torch.zeros((Pl, m, npd), dtype=torch.bfloat16, device=E.dev)
+    Y32 = torch.empty((npd, m), dtype=torch.float32, device=E.dev)
     # all planes per stage on CTA pairs (the split-product GEMM's fastest form here)
     prev_form = E.lib.cf_umma_set_all_planes(2)
     try:
-        _map_solve_spectra(E, L, plan, Ytp, Y, q, m, nb, P, st)
+        check(E.lib.cf_umma_gemm_bf16(npd, m, npd, plan.nterms, plan.ta, plan.tb, Cp.data_ptr(), npd, npd * npd, Pl,
+                                      Xtp.data_ptr(), npd, m * npd, Pl, None, 0, 0, Pl, YTp.data_ptr(), npd, m * npd,
+                                      Y32.data_ptr(), m, plan.err.data_ptr(), st), "cf_umma_gemm_bf16")
+        del Cp, Xtp
+        Ypad = Y32.double()
+        del Y32
+        Ytp = {fi: (_ptr16(YTp, plan.po[fi]), npd, m * npd) for fi in range(len(L.fields))}
+        _map_solve_spectra(E, L, plan, Ytp, Ypad, q, m, nb, P, st)
     finally:
         E.lib.cf_umma_set_all_planes(prev_form)
     check(E.lib.cf_umma_status(plan.err.data_ptr(), stream()), "tensor-core kernel")
@@ -84,7 +97,9 @@ def map_solves(E: eng.Engine, Cinv: torch.Tensor, X: torch.Tensor, precision: st
 
 def _map_solve_spectra(E, L, plan, Ytp, Y, q, m, nb, P, st):
     """q_b += 1/2 y^T dC_b y for every bin: per spectrum and column segment, the
-    split-product GEMM W = dC_b-planes . Y^T-planes and the q reduction."""
+    split-product GEMM W = dC_b-planes . Y^T-planes and the q reduction (Y in
+    the plan's padded field layout; Ytp[field] = (pointer, row stride, plane
+    stride) of that field's columns of the Y^T planes)."""
     Pl = plan.planes
     for s in range(L.nspectra):
         blk, ops = _build_planes(plan, s)
@@ -92,13 +107,14 @@ def _map_solve_spectra(E, L, plan, Ytp, Y, q, m, nb, P, st):
             M, ld = B.shape[1], B.shape[2]
             rpb = M // nb
             W = torch.empty((M, m), dtype=torch.float32, device=E.dev)
-            Yk = Ytp[kseg]
+            yk, ldk, psk = Ytp[kseg]
             check(E.lib.cf_umma_gemm_bf16(M, m, K, plan.nterms, plan.ta, plan.tb, B.data_ptr(), ld, M * ld, Pl,
-                                          Yk.data_ptr(), Yk.shape[2], m * Yk.shape[2], Pl, None, 0, 0, 0, None, 0,
+                                          yk, ldk, psk, Pl, None, 0, 0, 0, None, 0,
                                           0, W.data_ptr(), m, plan.err.data_ptr(), st), "cf_umma_gemm_bf16")
             f = L.fields[seg]
-            check(E.lib.cf_qform_reduce_f32(nb, f.nrows, rpb, W.data_ptr(), m, Y.data_ptr(), m, f.offset, m, 0.5,
-                                            q.data_ptr(), P, s * nb, st), "cf_qform_reduce_f32")
+            # Y rows in the padded field layout of the plan
+            check(E.lib.cf_qform_reduce_f32(nb, f.nrows, rpb, W.data_ptr(), m, Y.data_ptr(), m, plan.po[seg], m,
+                                            0.5, q.data_ptr(), P, s * nb, st), "cf_qform_reduce_f32")
             del W
         del ops
 

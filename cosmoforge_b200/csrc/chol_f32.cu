@@ -301,7 +301,7 @@ __global__ void __launch_bounds__(CNT, 2) k_chi2_refined(int n, const float* L, 
 // backward with D^T), the rows below / columns left of the block and the
 // quadratic-form strip as in k_chi2_refined.
 template <bool VL, bool VC, typename TC>
-__global__ void __launch_bounds__(CNT, 2) k_chi2_refined_dinv(int n, const float* L, long lda, long sL,
+__global__ void __launch_bounds__(CNT, 4) k_chi2_refined_dinv(int n, const float* L, long lda, long sL,
                                                               const float* D, long sD, const TC* C, long ldc,
                                                               long sC, const double* X, long ldx, long sX, int nrhs,
                                                               double* chi2)

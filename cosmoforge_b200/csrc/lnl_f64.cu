@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(NT, 2) k_chi2(int n, const double* L, long lda
 // diagonal solve one block-times-vector product (no dependent chain), then
 // the rows below take the block's 64-wide segment (z in shared memory).
 template <bool VEC>
-__global__ void __launch_bounds__(NT, 2) k_chi2_dinv(int n, const double* L, long lda, long sL, const double* D,
+__global__ void __launch_bounds__(NT, 4) k_chi2_dinv(int n, const double* L, long lda, long sL, const double* D,
                                                      long sD, const double* X, long ldx, long sX, int nrhs,
                                                      double* chi2)
 {
