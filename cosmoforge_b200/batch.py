@@ -4,9 +4,11 @@
   y = C^-1 x_m, for thousands of maps given one C^-1 (qube/spectra.py:
   1124-1186 with nsims large).  Per spectrum one GEMM W = D^T Y against the
   stacked derivative blocks of all its bins, then a per-(bin, map) reduction
-  (``cf_qform_reduce_*``).  ``precision="mixed"`` runs the GEMM as the BF16
-  split-product tensor-core kernel on derivative planes emitted by the pair
-  builder.
+  (``cf_qform_reduce_*``).  ``precision="mixed"`` runs every product on the
+  BF16 split-product tensor-core kernel (CTA-pair form): Y = C^-1 X first,
+  whose epilogue writes Y in FP32 for the reductions and the split planes of
+  Y^T for the per-spectrum GEMMs, then W against the derivative planes
+  emitted by the pair builder (q within 1e-5 of max |q| of the FP64 path).
 * :class:`PatchBatch` - many independent spin-0 QML problems of uneven size
   (sky patches) solved together: the problems are grouped by size into
   buckets, every problem of a bucket is padded to the bucket's order with an
