@@ -17,7 +17,8 @@ for the Fisher matrix, and keeps the fastest one within tolerance:
   the same trace of an FP64 product;
 * speed: CUDA-event time of the spectrum's GEMMs (second of two runs);
 * choice: the fastest candidate whose error is below ``tol`` or within
-  ``slack`` of the most accurate candidate's (the split-product floor).
+  ``slack`` of the most accurate candidate's (the split-product floor); a
+  CTA-pair candidate within 2 % of the fastest wins the tie.
 
 ``tune_patches`` picks the number of size buckets of ``batch.PatchBatch``
 (the fastest graph replay); ``tune_lnl`` the points per captured likelihood
@@ -177,6 +178,11 @@ def tune_fisher(E, Cinv: torch.Tensor, scheme: str = "bf16x6", tol: float = 6e-6
             floor = min(r[1] for r in results)
             ok = [r for r in results if r[1] <= max(tol, slack * floor)]
             best = min(ok)
+            # a near tie (within 2 %) goes to the CTA-pair form: same arithmetic,
+            # a third fewer bytes from L2 per MMA (and less power under the cap)
+            pair = [r for r in ok if r[2] == 2 and r[0] <= 1.02 * best[0]]
+            if pair:
+                best = min(pair)
             # the row-tile group only orders the tiles (same arithmetic per tile): timed, not re-checked
             groups = {16: best[0]}
             for gm in GROUPS:
