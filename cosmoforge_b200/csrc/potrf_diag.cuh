@@ -3,9 +3,10 @@
 // matrix, for FP64 and FP32.
 //
 // The block is factored right-looking in 16-column panels:
-//   (a) warp 0 factors the panel's 16 x 16 diagonal tile in registers (lane i
-//       holds row i; pivots are broadcast by shuffles, one reciprocal square
-//       root per column, l_kk = d rsqrt(d));
+//   (a) warp 0 factors the panel's 16 x 16 diagonal tile, left-looking (lane i
+//       holds row i in registers; column k's entries are independent dot
+//       products with row k read from shared memory; one shuffle and one
+//       reciprocal square root per pivot, l_kk = d rsqrt(d));
 //   (b) every row below the tile is solved against it by one thread
 //       (x_k = a_k / l_kk, then a_j -= x_k l_jk for the later columns j);
 //   (c) the trailing lower triangle takes the rank-16 update, 3 x 3 entries
@@ -96,35 +97,43 @@ __global__ void __launch_bounds__(NTHREADS) k_potrf_diag_inv(T* A, long lda, lon
     for (int p = 0; p < kb; p += PW) {
         const int pw = kb - p < PW ? kb - p : PW;
         p_last = p;
-        // (a) the pw x pw diagonal tile, warp 0, lane i = row p + i
+        // (a) the pw x pw diagonal tile, warp 0, lane i = row p + i, left-looking
+        // (Crout): at column k every lane forms its entry as an independent dot
+        // product of its own row of L with row k of L (broadcast reads of the
+        // tile in shared memory), so a pivot costs one shuffle and one
+        // reciprocal square root on the critical path
         if (warp == 0) {
             T r[PW];
 #pragma unroll
             for (int j = 0; j < PW; ++j) r[j] = (lane < pw && j <= lane) ? S[(p + lane) * LDS + p + j] : T(0);
+            T* Sp = S + p * LDS + p;
 #pragma unroll
             for (int k = 0; k < PW; ++k) {
                 if (k < pw) {
-                    T d = __shfl_sync(FULL, r[k], k);
+                    T acc0 = r[k], acc1 = T(0);
+#pragma unroll
+                    for (int m = 0; m < k; ++m) {
+                        const T lkm = Sp[k * LDS + m];
+                        if (m & 1)
+                            acc1 -= r[m] * lkm;
+                        else
+                            acc0 -= r[m] * lkm;
+                    }
+                    const T sv = acc0 + acc1;
+                    T d = __shfl_sync(FULL, sv, k);
                     if (!(d > T(0))) {  // also catches NaN
                         if (lane == 0 && bad == 0) bad = k0 + p + k + 1;
                         d = T(1);
                     }
                     const T rl = rsqrt(d);
-                    const T lkk = d * rl;
-                    if (lane == k) r[k] = lkk;
-                    else if (lane > k) r[k] *= rl;
+                    if (lane == k)
+                        r[k] = d * rl;
+                    else if (lane > k)
+                        r[k] = sv * rl;
                     if (lane == 0) rdg[p + k] = rl;
-#pragma unroll
-                    for (int j = k + 1; j < PW; ++j) {
-                        const T ljk = __shfl_sync(FULL, r[k], j);
-                        if (j < pw && lane >= j) r[j] -= r[k] * ljk;
-                    }
+                    if (lane >= k && lane < pw) Sp[lane * LDS + k] = r[k];
+                    __syncwarp();
                 }
-            }
-            if (lane < pw) {
-#pragma unroll
-                for (int j = 0; j < PW; ++j)
-                    if (j <= lane) S[(p + lane) * LDS + p + j] = r[j];
             }
         }
         __syncthreads();
