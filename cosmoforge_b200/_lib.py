@@ -66,6 +66,7 @@ SIGNATURES = {
     "cf_umma_trace_bf16_mapped": (_i, [_i, _i, _i, _i, _i, _p, _p, _p, _l, _l, _l, _i, _p, _l, _l, _l, _i,
                                        _d, _p, _l, _p, _p, _i, _i, _p, _p]),
     "cf_outer_planes": (_i, [_i, _i, _p, _p, _l, _i, _p, _l, _l, _l, _p]),
+    "cf_outer_planes_rect": (_i, [_i, _i, _i, _p, _p, _l, _i, _p, _l, _l, _l, _p]),
     "cf_split_bf16": (_i, [_i, _i, _p, _l, _i, _p, _l, _l, _p]),
     "cf_umma_gemm_bf16": (_i, [_i, _i, _i, _i, _p, _p, _p, _l, _l, _i, _p, _l, _l, _i, _p, _l, _l, _i,
                                _p, _l, _l, _p, _l, _p, _p]),

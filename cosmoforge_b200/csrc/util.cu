@@ -99,13 +99,13 @@ extern "C" int cf_split_bf16(int R, int C, const double* X, long ldx, int planes
 
 namespace {
 
-// out[p][q][i][j] = p-th BF16 split plane of x_q[i] * y_q[j]  (i, j < n)
-__global__ void k_outer_planes(int n, int nvec, const double* x, const double* y, long ldv, int planes,
+// out[p][q][i][j] = p-th BF16 split plane of x_q[i] * y_q[j]  (i < m, j < n)
+__global__ void k_outer_planes(int m, int n, int nvec, const double* x, const double* y, long ldv, int planes,
                                __nv_bfloat16* out, long ld, long q_stride, long plane_stride)
 {
-    const long total = (long)nvec * n * n;
+    const long per = (long)m * n, total = (long)nvec * per;
     for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
-        const long q = e / ((long)n * n), rem = e % ((long)n * n);
+        const long q = e / per, rem = e % per;
         const long i = rem / n, j = rem % n;
         double v = x[i * ldv + q] * y[j * ldv + q];
         for (int p = 0; p < planes; ++p) {
@@ -118,18 +118,25 @@ __global__ void k_outer_planes(int n, int nvec, const double* x, const double* y
 
 }  // namespace
 
-// BF16 split planes of the outer products x_q y_q^T, q < nvec (x, y: n x nvec
-// column-major-by-vector with row stride ldv), into out[p][q] (n x n, row
-// stride ld, q_stride / plane_stride elements apart).
-extern "C" int cf_outer_planes(int n, int nvec, const double* x, const double* y, long ldv, int planes, void* out,
-                               long ld, long q_stride, long plane_stride, void* stream)
+// BF16 split planes of the outer products x_q y_q^T, q < nvec (x: m x nvec,
+// y: n x nvec, both with row stride ldv), into out[p][q] (m x n, row stride
+// ld, q_stride / plane_stride elements apart).
+extern "C" int cf_outer_planes_rect(int m, int n, int nvec, const double* x, const double* y, long ldv, int planes,
+                                    void* out, long ld, long q_stride, long plane_stride, void* stream)
 {
-    if (n <= 0 || nvec <= 0 || !x || !y || !out || planes < 1 || planes > 3) return CF_ERR_ARG;
-    long blocks = ((long)nvec * n * n + 255) / 256;
+    if (m <= 0 || n <= 0 || nvec <= 0 || !x || !y || !out || planes < 1 || planes > 3) return CF_ERR_ARG;
+    long blocks = ((long)nvec * m * n + 255) / 256;
     if (blocks > 148 * 16) blocks = 148 * 16;
-    k_outer_planes<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(n, nvec, x, y, ldv, planes,
+    k_outer_planes<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(m, n, nvec, x, y, ldv, planes,
                                                                        (__nv_bfloat16*)out, ld, q_stride,
                                                                        plane_stride);
     CF_CHECK_LAUNCH();
     return CF_OK;
+}
+
+// The square case (m = n).
+extern "C" int cf_outer_planes(int n, int nvec, const double* x, const double* y, long ldv, int planes, void* out,
+                               long ld, long q_stride, long plane_stride, void* stream)
+{
+    return cf_outer_planes_rect(n, n, nvec, x, y, ldv, planes, out, ld, q_stride, plane_stride, stream);
 }

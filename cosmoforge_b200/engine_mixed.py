@@ -9,16 +9,17 @@ cores:
   emitted by the pair builder directly as BF16 planes (FP64 recurrences,
   split at the store);
 * A_b = C^-1 dC_b runs as the split-product GEMM ``cf_umma_gemm_bf16``
-  (FP32 accumulation in TMEM) whose epilogue writes A_b, and A_b^T, as BF16
-  planes again;
+  (FP32 accumulation in TMEM) whose epilogue writes A_b, and A_b^T, as two
+  BF16 planes (16 significant bits);
 * the traces F_pq = 1/2 sum_{k,l} A_p[k,l] A_q[l,k] run as the tensor-core
-  contraction ``cf_umma_trace_bf16`` over the flattened (k, l) plane, partial
-  sums added into an FP64 F.
+  contraction ``cf_umma_trace_bf16`` over the flattened (k, l) plane with the
+  products (0,0), (0,1), (1,0), (1,1) of those planes, partial sums added
+  into an FP64 F.
 
 Schemes: ``bf16x3`` = planes {(0,0), (0,1), (1,0)} (~16 bits per product),
 ``bf16x6`` adds {(0,2), (1,1), (2,0)} (~24 bits).  The noise bias and the
-quadratic forms are contractions of the same resident A_b slabs against
-G = N C^-1 and x (C^-1 x)^T (``_qml_core``).
+quadratic forms come out of the same traces: C^-1 N and (C^-1 x) x^T are
+appended to the A_b slabs as extra parameters (``_extra_slabs``).
 
 Field segments are placed at 8-element-aligned offsets of a padded index
 space (zero rows / columns in the gaps) so every TMA box starts 16-byte
@@ -40,6 +41,16 @@ SCHEMES = {
     "bf16x3": (2, (0, 0, 1), (0, 1, 0)),
     "bf16x6": (3, (0, 0, 1, 0, 1, 2), (0, 1, 0, 2, 1, 0)),
 }
+# How A_b is stored and traced: (planes, ta, tb).  The traces sum ~n^2 products
+# per entry of F, so the rounding of A_b to two planes (16 significant bits,
+# unbiased) averages out; (1,1) is kept because on the diagonal it is the
+# square of the second planes, a bias if left out (measured on the TQU
+# nside-16 problem: |dF_bb|/F_bb 4.1e-6 with two planes and four terms,
+# 3.8e-6 with three planes and six).
+TRACE = {
+    "bf16x3": (2, (0, 0, 1), (0, 1, 0)),
+    "bf16x6": (2, (0, 0, 1, 1), (0, 1, 0, 1)),
+}
 
 
 def _r8(x: int) -> int:
@@ -57,6 +68,9 @@ class MixedPlan:
         self.nterms = len(ta)
         self._ta = (ctypes.c_int * len(ta))(*ta)
         self._tb = (ctypes.c_int * len(tb))(*tb)
+        # planes of the stored A_b slabs, and the product terms of their traces
+        self.out_planes, qa, qb = TRACE[scheme]
+        self.trace = (self.out_planes, len(qa), (ctypes.c_int * len(qa))(*qa), (ctypes.c_int * len(qb))(*qb))
         L = E.L
         self.po = []  # padded offset of each field segment
         off = 0
@@ -167,7 +181,8 @@ def fisher(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6", forms: dict | 
 
 
 def _fisher_core(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6", N=None, maps=None, forms=None):
-    """F (P x P, FP64) with the A_b GEMMs and traces on the tensor cores.
+    """F (P x P, FP64), and the noise bias and quadratic forms when N / maps are
+    given, with the A_b GEMMs and the traces on the tensor cores.
 
     A_b is kept for every parameter in one buffer per column segment (field):
     ``X[f]`` holds, for every spectrum whose derivative touches columns of
@@ -175,15 +190,24 @@ def _fisher_core(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6", N=None, 
     ``XT[f]`` their transposes.  After all spectra, each ordered segment pair
     (s, t) is one tensor-core contraction of all parameters touching s against
     all parameters touching t, scattered into F through parameter-index maps.
+
+    The noise bias and the quadratic forms are the same contraction against
+    other matrices (qube/spectra.py:1124-1186):
+    b_p = 1/2 Tr(A_p C^-1 N) and q_p = 1/2 y^T dC_p y = 1/2 Tr(A_p y x^T),
+    y = C^-1 x.  So C^-1 N and each y x^T are appended to every segment's slabs
+    as extra parameters, and the one pass of traces that forms F also forms
+    F[p, extra] = b_p and q_p, reading every A_b slab once for all three.
     """
     plan = MixedPlan(E, scheme)
     L = E.L
     nb, P = L.nbins, L.n_params
     npd = plan.n_pad
-    Pl = plan.planes
+    Pl, Po = plan.planes, plan.out_planes
     ev = E._probe_begin("split_cinv")
     Cp = plan.split_cinv(Cinv)
     E._probe_end("split_cinv", ev, 0)
+    nsims = 0 if maps is None else maps.shape[1]
+    nx = (1 if N is not None else 0) + nsims  # extra parameters: C^-1 N, then y_q x_q^T
     segrows = {i: f.nrows for i, f in enumerate(L.fields)}
     segpad = {i: _r8(f.nrows) for i, f in enumerate(L.fields)}
     cols_of = {}
@@ -191,16 +215,17 @@ def _fisher_core(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6", N=None, 
         blk = L.blocks[E.block_of_spec[s]]
         cols_of[s] = [blk.fa] if blk.fa == blk.fb else [blk.fa, blk.fb]
     seg_specs = {f: [s for s in range(L.nspectra) if f in cols_of[s]] for f in range(len(L.fields))}
-    X, XT, pmap, ldseg = {}, {}, {}, {}
+    X, XT, pmap, ldseg, xcol = {}, {}, {}, {}, {}
     for f, specs in seg_specs.items():
-        if not specs:
+        if not specs and not nx:
             continue
-        ncols = len(specs) * nb * segpad[f]
+        xcol[f] = len(specs) * nb * segpad[f]  # first column of the extra parameters
+        ncols = xcol[f] + nx * segpad[f]
         ldseg[f] = _r8(ncols)
-        X[f] = torch.empty((Pl, npd, ldseg[f]), dtype=BF16, device=E.dev)
-        XT[f] = torch.empty((Pl, ncols, npd), dtype=BF16, device=E.dev)
-        pmap[f] = torch.tensor([s * nb + b for s in specs for b in range(nb)], dtype=torch.int32,
-                               device=E.dev)
+        X[f] = torch.empty((Po, npd, ldseg[f]), dtype=BF16, device=E.dev)
+        XT[f] = torch.empty((Po, ncols, npd), dtype=BF16, device=E.dev)
+        pmap[f] = torch.tensor([s * nb + b for s in specs for b in range(nb)] + [P + q for q in range(nx)],
+                               dtype=torch.int32, device=E.dev)
     if forms is None:
         from .autotune import forms_for
 
@@ -226,7 +251,7 @@ def _fisher_core(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6", N=None, 
             check(E.lib.cf_umma_gemm_bf16(
                 npd, ncol, K, plan.nterms, plan.ta, plan.tb, _off(Cp, plan.po[kseg]), npd, npd * npd, Pl,
                 B.data_ptr(), B.shape[2], B.shape[1] * B.shape[2], Pl,
-                _off(Xs, col0), ldseg[seg], npd * ldseg[seg], Pl,
+                _off(Xs, col0), ldseg[seg], npd * ldseg[seg], Po,
                 _off(XTs, col0 * npd), npd, XTs.shape[1] * npd, None, 0,
                 plan.err.data_ptr(), stream()), "cf_umma_gemm_bf16")
             torch.cuda.nvtx.range_pop()
@@ -235,7 +260,12 @@ def _fisher_core(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6", N=None, 
     E.lib.cf_umma_set_all_planes(prev_ap)
     E.lib.cf_umma_set_promotion(prev_kc)
     E.lib.cf_umma_set_group(prev_gm)
-    F = torch.zeros((P, P), dtype=torch.float64, device=E.dev)
+    if nx:
+        ev = E._probe_begin("qml_mixed")
+        _extra_slabs(plan, Cp, Cinv, N, maps, X, XT, ldseg, xcol, segpad)
+        E._probe_end("qml_mixed", ev, 0)
+    Pt = P + nx
+    Fx = torch.zeros((Pt, Pt), dtype=torch.float64, device=E.dev)
     segs = list(X)
     for a, ss in enumerate(segs):
         # (s, t) and (t, s) give transposed blocks of F: compute s <= t, mirror s < t
@@ -244,71 +274,62 @@ def _fisher_core(E: Engine, Cinv: torch.Tensor, scheme: str = "bf16x6", N=None, 
             m_s, m_t = segrows[ss], segrows[tt]
             ev = E._probe_begin("trace_mixed")
             torch.cuda.nvtx.range_push("trace_mixed")
+            tpl, tnt, tta, ttb = plan.trace
             check(E.lib.cf_umma_trace_bf16_mapped(
-                P1, P2, m_t, m_s, plan.nterms, plan.ta, plan.tb,
-                _off(X[ss], plan.po[tt] * ldseg[ss]), segpad[ss], ldseg[ss], npd * ldseg[ss], Pl,
-                _off(XT[tt], plan.po[ss]), segpad[tt] * npd, npd, XT[tt].shape[1] * npd, Pl,
-                0.5, F.data_ptr(), P, pmap[ss].data_ptr(), pmap[tt].data_ptr(), int(ss != tt), 0,
+                P1, P2, m_t, m_s, tnt, ctypes.cast(tta, ctypes.c_void_p), ctypes.cast(ttb, ctypes.c_void_p),
+                _off(X[ss], plan.po[tt] * ldseg[ss]), segpad[ss], ldseg[ss], npd * ldseg[ss], tpl,
+                _off(XT[tt], plan.po[ss]), segpad[tt] * npd, npd, XT[tt].shape[1] * npd, tpl,
+                0.5, Fx.data_ptr(), Pt, pmap[ss].data_ptr(), pmap[tt].data_ptr(), int(ss != tt), 0,
                 plan.err.data_ptr(), stream()), "cf_umma_trace_bf16_mapped")
             torch.cuda.nvtx.range_pop()
-            E._probe_end("trace_mixed", ev, 2.0 * P1 * P2 * m_t * m_s * plan.nterms)
-    del XT
-    qml = None
-    if N is not None or maps is not None:
-        qml = _qml_core(plan, E, Cinv, Cp, N, maps, X, pmap, ldseg, segrows, segpad)
-    del X
+            E._probe_end("trace_mixed", ev, 2.0 * P1 * P2 * m_t * m_s * tnt)
+    del X, XT
     check(E.lib.cf_umma_status(plan.err.data_ptr(), stream()), "tensor-core kernel")
-    return F, qml
+    if not nx:
+        return Fx, None
+    F = Fx[:P, :P].contiguous()
+    bias = Fx[:P, P].contiguous() if N is not None else None
+    q = Fx[:P, Pt - nsims:].T.contiguous() if nsims else None
+    return F, (bias, q)
 
 
-def _qml_core(plan, E, Cinv, Cp, N, maps, X, pmap, ldseg, segrows, segpad):
-    """Noise bias and quadratic forms as contractions of the resident A_b slabs.
+def _extra_slabs(plan, Cp, Cinv, N, maps, X, XT, ldseg, xcol, segpad):
+    """Column slabs (and transposes) of the extra contraction partners C^-1 N
+    and y_q x_q^T, written after each segment's A_b slabs.
 
-    b_p = 1/2 Tr(C^-1 N C^-1 dC_p) = 1/2 sum_kl A_p[k,l] G[k,l], G = N C^-1;
-    q_p = 1/2 y^T dC_p y = 1/2 sum_kl A_p[k,l] x_k y_l, y = C^-1 x
-    (qube/spectra.py:1124-1186).  G comes from the split-product GEMM, the
-    outer products x y^T are split into planes, and one contraction per
-    segment pair reads every A_b slab once.
+    With A~ appended as a parameter, the trace gives 1/2 Tr(A_p A~); the bias
+    needs A~ = (N C^-1)^T = C^-1 N and the quadratic form of map q needs
+    A~ = (x y^T)^T = y x^T.
     """
-    L = E.L
-    npd, Pl, P = plan.n_pad, plan.planes, L.n_params
-    nsims = 0 if maps is None else maps.shape[1]
-    Q = 1 + nsims
-    ev = E._probe_begin("qml_mixed")
-    stack = torch.empty((Pl, Q, npd, npd), dtype=BF16, device=E.dev)
+    E = plan.E
+    npd, Pl, Po = plan.n_pad, plan.planes, plan.out_planes
+    j = 0
     if N is not None:
         Np = plan.split_cinv(N)
-        check(E.lib.cf_umma_gemm_bf16(
-            npd, npd, npd, plan.nterms, plan.ta, plan.tb, Np.data_ptr(), npd, npd * npd, Pl,
-            Cp.data_ptr(), npd, npd * npd, Pl, stack.data_ptr(), npd, Q * npd * npd, Pl, None, 0, 0, None, 0,
-            plan.err.data_ptr(), stream()), "cf_umma_gemm_bf16")
+        for f in X:
+            # X[f][:, c] = (C^-1 N)[:, po_f + c] = C^-1 (row po_f + c of N)^T
+            check(E.lib.cf_umma_gemm_bf16(
+                npd, segpad[f], npd, plan.nterms, plan.ta, plan.tb, Cp.data_ptr(), npd, npd * npd, Pl,
+                _off(Np, plan.po[f] * npd), npd, npd * npd, Pl,
+                _off(X[f], xcol[f]), ldseg[f], npd * ldseg[f], plan.out_planes,
+                _off(XT[f], xcol[f] * npd), npd, XT[f].shape[1] * npd, None, 0,
+                plan.err.data_ptr(), stream()), "cf_umma_gemm_bf16")
         del Np
-    else:
-        stack[:, 0].zero_()
-    bias = q = None
-    if nsims:
+        j = 1
+    if maps is not None:
+        nsims = maps.shape[1]
         Xm = maps.to(E.dev, torch.float64).contiguous()
         Ym = E.gemm(Cinv, Xm)
         xp, yp = plan.pad_rows(Xm), plan.pad_rows(Ym)
-        check(E.lib.cf_outer_planes(npd, nsims, xp.data_ptr(), yp.data_ptr(), nsims, Pl,
-                                    _off(stack, npd * npd), npd, npd * npd, Q * npd * npd, stream()),
-              "cf_outer_planes")
-    R = torch.zeros((P, Q), dtype=torch.float64, device=E.dev)
-    cmap = torch.arange(Q, dtype=torch.int32, device=E.dev)
-    for ss in X:
-        for tt in plan.segments:
-            check(E.lib.cf_umma_trace_bf16_mapped(
-                pmap[ss].numel(), Q, segrows[tt], segrows[ss], plan.nterms, plan.ta, plan.tb,
-                _off(X[ss], plan.po[tt] * ldseg[ss]), segpad[ss], ldseg[ss], npd * ldseg[ss], Pl,
-                _off(stack, plan.po[tt] * npd + plan.po[ss]), npd * npd, npd, Q * npd * npd, Pl,
-                0.5, R.data_ptr(), Q, pmap[ss].data_ptr(), cmap.data_ptr(), 0, 0,
-                plan.err.data_ptr(), stream()), "cf_umma_trace_bf16_mapped")
-    if N is not None:
-        bias = R[:, 0].contiguous()
-    if nsims:
-        q = R[:, 1:].T.contiguous()
-    E._probe_end("qml_mixed", ev, 0)
-    return bias, q
+        for f in X:
+            sp, c0 = segpad[f], xcol[f] + j * segpad[f]
+            xs = _off(xp, plan.po[f] * nsims)
+            # X[f][k, c0 + q sp + c] = y_q[k] x_q[po_f + c]
+            check(E.lib.cf_outer_planes_rect(npd, sp, nsims, yp.data_ptr(), xs, nsims, Po, _off(X[f], c0),
+                                             ldseg[f], sp, npd * ldseg[f], stream()), "cf_outer_planes_rect")
+            # XT[f][c0 + q sp + c, k] = x_q[po_f + c] y_q[k]
+            check(E.lib.cf_outer_planes_rect(sp, npd, nsims, xs, yp.data_ptr(), nsims, Po, _off(XT[f], c0 * npd),
+                                             npd, sp * npd, XT[f].shape[1] * npd, stream()), "cf_outer_planes_rect")
 
 
 def fisher_qml(E: Engine, Cinv: torch.Tensor, N: torch.Tensor | None = None,

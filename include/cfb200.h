@@ -251,6 +251,14 @@ int cf_split_bf16(int R, int C, const double* X, long ldx, int planes, void* out
 int cf_outer_planes(int n, int nvec, const double* x, const double* y, long ldv, int planes, void* out,
                     long ld, long q_stride, long plane_stride, void* stream);
 
+/* As cf_outer_planes for m x n products: x is m x nvec, y is n x nvec (row
+ * stride ldv), out[p][q] is m x n.  The mixed Fisher appends y_q x_q^T and
+ * C^-1 N to the A_b slabs as extra contraction partners, so one pass of the
+ * trace kernel gives F, the noise bias and the quadratic forms
+ * (qube/fisher.py:501-607, qube/spectra.py:1124-1186). */
+int cf_outer_planes_rect(int m, int n, int nvec, const double* x, const double* y, long ldv, int planes,
+                         void* out, long ld, long q_stride, long plane_stride, void* stream);
+
 /* cf_build_block writing BF16 split planes (planes 1..3, plane_stride /
  * planeT_stride elements apart) instead of FP64.  flags bit 0 (auto kinds):
  * every entry computed from its own pixel pair, no mirror writes; bit 1
