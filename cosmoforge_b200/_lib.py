@@ -59,6 +59,7 @@ SIGNATURES = {
     "cf_umma_trace_bf16": (_i, [_i, _i, _i, _i, _i, _p, _p, _p, _l, _l, _l, _i, _p, _l, _l, _l, _i, _d,
                                 _p, _l, _l, _l, _i, _i, _p, _p]),
     "cf_umma_set_promotion": (_i, [_i]),
+    "cf_umma_set_trace_pairs": (_i, [_i]),
     "cf_umma_set_wait_limit": (C.c_longlong, [C.c_longlong]),
     "cf_umma_status": (_i, [_p, _p]),
     "cf_umma_set_all_planes": (_i, [_i]),

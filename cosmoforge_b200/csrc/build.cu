@@ -185,10 +185,9 @@ struct Emitter {
         __nv_bfloat16* oT = reinterpret_cast<__nv_bfloat16*>(a.outT);
         double x = v;
         for (int p = 0; p < a.planes; ++p) {
-            const __nv_bfloat16 h = __double2bfloat16(x);
+            const __nv_bfloat16 h = cf_bf16_plane(x);
             if (prim) o[p * a.plane_stride + i] = h;
             if (mirror) oT[p * a.planeT_stride + iT] = h;
-            x -= (double)__bfloat162float(h);
         }
     }
 };

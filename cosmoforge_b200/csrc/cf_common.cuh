@@ -32,6 +32,17 @@ extern unsigned long long g_cf_launch_count;
 
 static inline int cf_cdiv(long a, long b) { return (int)((a + b - 1) / b); }
 
+#ifdef __CUDACC__
+#include <cuda_bf16.h>
+// Next BF16 split plane of x (round to nearest), and x minus it (exact in FP64).
+__device__ __forceinline__ __nv_bfloat16 cf_bf16_plane(double& x)
+{
+    const __nv_bfloat16 h = __double2bfloat16(x);
+    x -= (double)__bfloat162float(h);
+    return h;
+}
+#endif
+
 #ifdef __cplusplus
 #include <atomic>
 

@@ -239,6 +239,14 @@ __device__ __forceinline__ void tma_load_3d_pair(const CUtensorMap* map, uint32_
         ::"r"(smem_u32(dst)), "l"((uint64_t)map), "r"(mbar), "r"(c0), "r"(c1), "r"(c2)
         : "memory");
 }
+__device__ __forceinline__ void tma_load_4d_pair(const CUtensorMap* map, uint32_t mbar, void* dst, int c0, int c1,
+                                                 int c2, int c3)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], [%2];\n"
+        ::"r"(smem_u32(dst)), "l"((uint64_t)map), "r"(mbar), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+        : "memory");
+}
 __device__ __forceinline__ void mbar_arrive_remote(uint32_t mbar)
 {
     asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(mbar) : "memory");
@@ -287,7 +295,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     // are counted on the leader's barriers, MMA completions are multicast to
     // both CTAs' barriers and each CTA's epilogue drains its own TMEM half
     // (rows 128 rank ..) and reports to the leader.
-    static_assert(CG == 1 || (CG == 2 && !TRACE && PLS > 1), "CTA pairs: all-planes GEMM form only");
+    static_assert(CG == 1 || (CG == 2 && PLS > 1), "CTA pairs: all-planes forms only");
     using AccT = typename std::conditional<TRACE, double, float>::type;
     constexpr int HALF = BN / 2;
     constexpr int BNL = BN / CG;  // rows of B held by this CTA
@@ -406,8 +414,14 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         uint8_t* db = sB + s * B_STAGE + pl * B_BYTES;
                         if (TRACE) {
                             const int k = (int)(ktile / nl), l0 = (int)(ktile % nl) * BKT;
-                            tma_load_4d(&mapA, &full[s], da, l0, k, m0, pa);
-                            tma_load_4d(&mapB, &full[s], db, l0, k, n0, pb);
+                            if constexpr (CG == 2) {
+                                const uint32_t fb = at_rank(&full[s], 0);
+                                tma_load_4d_pair(&mapA, fb, da, l0, k, m0, pa);
+                                tma_load_4d_pair(&mapB, fb, db, l0, k, n0 + (int)rank * BNL, pb);
+                            } else {
+                                tma_load_4d(&mapA, &full[s], da, l0, k, m0, pa);
+                                tma_load_4d(&mapB, &full[s], db, l0, k, n0, pb);
+                            }
                         } else {
                             const int kk = (int)ktile * BKT;
                             if constexpr (CG == 2) {
@@ -698,6 +712,9 @@ int make_map4(CUtensorMap* map, const void* base, long K2, long K1, long rows, i
 
 // Promotion interval (k-tiles of 64 per FP32 accumulator): 1, 2, 4, 8, 16 or 32.
 int g_promote_kc = 16;
+// Trace mode on CTA pairs (256-row output tiles, each CTA holding half of the
+// B rows of a 128-column tile) when both operands carry two or three planes.
+int g_trace_pairs = 1;
 // Row tiles per group of the persistent tile order.
 int g_group_m = 16;
 // Bound of the kernels' waits on pipeline barriers (drains of issued work keep WAIT_NS).
@@ -783,6 +800,15 @@ int cf_umma_trace_impl(int P1, int P2, int K1, int K2, int nterms, const int* ta
 // Set the promotion interval of the tensor-core kernels (k-tiles of 64 summed
 // in one FP32 TMEM accumulator before the partial is promoted): 1, 2, 4,
 // 8, 16 (default) or 32.  Returns the previous value.
+// Trace contractions on CTA pairs (1, default) or one CTA per output tile (0);
+// returns the previous setting.
+extern "C" int cf_umma_set_trace_pairs(int on)
+{
+    const int prev = g_trace_pairs;
+    g_trace_pairs = on ? 1 : 0;
+    return prev;
+}
+
 extern "C" int cf_umma_set_promotion(int kc)
 {
     const int prev = g_promote_kc;
@@ -954,13 +980,16 @@ int cf_umma_trace_impl(int P1, int P2, int K1, int K2, int nterms, const int* ta
         t.b[i] = tb[i];
     }
     CUtensorMap ma, mb;
+    // every plane of a k-tile in one stage when both operands carry the same planes
+    const int pls = (x_planes == y_planes) ? x_planes : 1;
+    const bool narrow = P2 <= 64;
+    const bool pairs = g_trace_pairs && !narrow && P1 > BM && (pls == 2 || pls == 3);
     int rc = make_map4(&ma, X, K2, K1, P1, x_planes, ldX, sXp, x_ps, BM);
     if (rc) return rc;
-    const bool narrow = P2 <= 64;
-    rc = make_map4(&mb, Y, K2, K1, P2, y_planes, ldY, sYq, y_ps, narrow ? 64 : 128);
+    rc = make_map4(&mb, Y, K2, K1, P2, y_planes, ldY, sYq, y_ps, narrow ? 64 : (pairs ? 64 : 128));
     if (rc) return rc;
     const long tiles = (long)K1 * ((K2 + BK - 1) / BK);
-    const int out_tiles = cf_cdiv(P1, BM) * cf_cdiv(P2, narrow ? 64 : 128);
+    const int out_tiles = cf_cdiv(P1, pairs ? 2 * BM : BM) * cf_cdiv(P2, narrow ? 64 : 128);
     if (splits <= 0) splits = (148 * 2 + out_tiles - 1) / out_tiles;
     if (splits > tiles) splits = (int)tiles;
     EpiArgs e{};
@@ -968,8 +997,10 @@ int cf_umma_trace_impl(int P1, int P2, int K1, int K2, int nterms, const int* ta
     e.N = P2;
     TraceArgs tr{K1, K2, F, ldF, p_off, q_off, sym, scale, row_map, col_map};
     cudaStream_t st = (cudaStream_t)stream;
-    // every plane of a k-tile in one stage when both operands carry the same planes
-    const int pls = (x_planes == y_planes) ? x_planes : 1;
+    if (pairs) {
+        if (pls == 3) return launch_gemm_kc<128, 3, true, 4, 3, BK, false, 2>(ma, mb, P1, P2, 0, t, e, tr, splits, err, st);
+        return launch_gemm_kc<128, 4, true, 4, 2, BK, false, 2>(ma, mb, P1, P2, 0, t, e, tr, splits, err, st);
+    }
     if (narrow) {
         if (pls == 3) return launch_gemm_kc<64, 3, true, 4, 3>(ma, mb, P1, P2, 0, t, e, tr, splits, err, st);
         if (pls == 2) return launch_gemm_kc<64, 4, true, 4, 2>(ma, mb, P1, P2, 0, t, e, tr, splits, err, st);

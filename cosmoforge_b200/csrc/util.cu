@@ -65,7 +65,7 @@ extern "C" int cf_version(void) { return 1; }
 
 namespace {
 
-// out[p][r][c] = p-th BF16 split plane of X[r][c]: x_0 = bf16(x), x_1 = bf16(x - x_0), ...
+// out[p][r][c] = p-th BF16 split plane of X[r][c] (cf_bf16_plane)
 __global__ void k_split_bf16(int R, int C, const double* X, long ldx, int planes, __nv_bfloat16* out, long ldo,
                              long plane_stride)
 {
@@ -73,11 +73,7 @@ __global__ void k_split_bf16(int R, int C, const double* X, long ldx, int planes
     for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
         const long r = e / C, c = e % C;
         double x = X[r * ldx + c];
-        for (int p = 0; p < planes; ++p) {
-            __nv_bfloat16 h = __double2bfloat16(x);
-            out[p * plane_stride + r * ldo + c] = h;
-            x -= (double)__bfloat162float(h);
-        }
+        for (int p = 0; p < planes; ++p) out[p * plane_stride + r * ldo + c] = cf_bf16_plane(x);
     }
 }
 
@@ -108,11 +104,7 @@ __global__ void k_outer_planes(int m, int n, int nvec, const double* x, const do
         const long q = e / per, rem = e % per;
         const long i = rem / n, j = rem % n;
         double v = x[i * ldv + q] * y[j * ldv + q];
-        for (int p = 0; p < planes; ++p) {
-            __nv_bfloat16 h = __double2bfloat16(v);
-            out[p * plane_stride + q * q_stride + i * ld + j] = h;
-            v -= (double)__bfloat162float(h);
-        }
+        for (int p = 0; p < planes; ++p) out[p * plane_stride + q * q_stride + i * ld + j] = cf_bf16_plane(v);
     }
 }
 

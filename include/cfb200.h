@@ -361,6 +361,13 @@ int cf_umma_status(const int* err, void* stream);
  * Returns the previous value.  No counterpart in the reference. */
 int cf_umma_set_promotion(int kc);
 
+/* Trace contractions (cf_umma_trace_bf16*) on CTA pairs: 256 x 128 output
+ * tiles with tcgen05.mma.cta_group::2, each CTA loading its 128 rows of X and
+ * 64 of the tile's 128 rows of Y, when both operands carry two or three planes
+ * and P1 > 128 (on = 1, the default), or one CTA per 128 x 128 tile (on = 0).
+ * Returns the previous setting. */
+int cf_umma_set_trace_pairs(int on);
+
 /* Form of cf_umma_gemm_bf16: 1 (default) loads every plane of a 32-wide
  * k-slice into one pipeline stage and keeps the leading product apart from
  * the corrections in a second TMEM accumulator, when both operands carry the

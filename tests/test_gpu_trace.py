@@ -44,12 +44,15 @@ def _ref(Xp, Yp, terms, P, K1, K2, scale):
     return scale * F, scale * mag
 
 
+@pytest.mark.parametrize("pairs", [1, 0])
 @pytest.mark.parametrize("terms,planes", [(X6, 3), (X4, 2)])
 @pytest.mark.parametrize("P,K", [(40, 96), (150, 72), (230, 40)])
-def test_trace_matches_fp64(P, K, terms, planes):
+def test_trace_matches_fp64(P, K, terms, planes, pairs):
+    """pairs = 1: P > 128 runs on CTA pairs (256-row tiles); 0: one CTA per tile."""
     from cosmoforge_b200 import _lib
 
     lib = _lib.lib()
+    prev = lib.cf_umma_set_trace_pairs(pairs)
     g = torch.Generator(device="cuda").manual_seed(P + K)
     # A_p with a common smooth part, so the contraction has cancellation
     base = torch.randn((K, K), dtype=torch.float64, device="cuda", generator=g)
@@ -67,6 +70,7 @@ def test_trace_matches_fp64(P, K, terms, planes):
     rc = lib.cf_umma_trace_bf16_mapped(P, P, K, K, len(terms[0]), pa, pb, Xp.data_ptr(), K * ld, ld, P * K * ld,
                                        planes, Yp.data_ptr(), K * ld, ld, P * K * ld, planes, 0.5, F.data_ptr(), P,
                                        pmap.data_ptr(), pmap.data_ptr(), 0, 0, err.data_ptr(), st)
+    lib.cf_umma_set_trace_pairs(prev)
     assert rc == 0
     torch.cuda.synchronize()
     assert int(err.item()) == 0
