@@ -759,9 +759,9 @@ int launch_gemm_kc(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, i
 }
 
 // GEMM mode: 1 = all planes of a 32-wide k-slice per stage with split
-// accumulators where the planes allow it, 2 = the same for three planes on
-// CTA pairs (256-row tiles, 4 stages of 48 KB per CTA), 0 = 64-wide k-tiles
-// term by term.
+// accumulators where the planes allow it, 2 = all three planes of a 64-wide
+// k-tile per stage on CTA pairs (256-row tiles, 2 stages of 96 KB per CTA),
+// 0 = 64-wide k-tiles term by term.
 int g_all_planes = 1;
 
 template <int BN, int STAGES, bool TRACE, int PLS = 1, int BKT = BK, bool SPLIT = false, int CG = 1>
@@ -878,13 +878,19 @@ int gemm_bf16(int M, int N, int K, int nterms, const int* ta, const int* tb, con
     bool all_planes = g_all_planes && (pls == 2 || pls == 3) && t.a[0] == 0 && t.b[0] == 0;
     for (int i = 1; i < nterms && all_planes; ++i) all_planes = !(t.a[i] == 0 && t.b[i] == 0);
     if (all_planes) {
-        // form 2: three planes on CTA pairs (each CTA holds half of B's 256 rows)
-        const bool pairs = g_all_planes == 2 && pls == 3;
+        // form 2: three planes of 64-wide k-tiles on CTA pairs (each CTA holds
+        // half of B's 256 rows; 2 stages of 96 KB per CTA)
+        if (g_all_planes == 2 && pls == 3) {
+            int rc = make_map(&ma, A, K, M, lda, a_planes, a_ps, BM, 64);
+            if (rc) return rc;
+            rc = make_map(&mb, B, K, N, ldb, b_planes, b_ps, 128, 64);
+            if (rc) return rc;
+            return launch_gemm<256, 2, false, 3, 64, true, 2>(ma, mb, M, N, K, t, e, tr, 1, err, st);
+        }
         int rc = make_map(&ma, A, K, M, lda, a_planes, a_ps, BM, 32);
         if (rc) return rc;
-        rc = make_map(&mb, B, K, N, ldb, b_planes, b_ps, pairs ? 128 : 256, 32);
+        rc = make_map(&mb, B, K, N, ldb, b_planes, b_ps, 256, 32);
         if (rc) return rc;
-        if (pairs) return launch_gemm<256, 4, false, 3, 32, true, 2>(ma, mb, M, N, K, t, e, tr, 1, err, st);
         if (pls == 3) return launch_gemm<256, 3, false, 3, 32, true>(ma, mb, M, N, K, t, e, tr, 1, err, st);
         return launch_gemm<256, 4, false, 2, 32, true>(ma, mb, M, N, K, t, e, tr, 1, err, st);
     }
