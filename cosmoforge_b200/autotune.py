@@ -41,7 +41,7 @@ import torch
 from ._lib import check, stream
 from .engine_mixed import MixedPlan, _build_planes, default_gemm_forms
 
-CANDIDATES = ((1, 16), (2, 16), (1, 8), (0, 16), (0, 32))
+CANDIDATES = ((1, 16), (2, 16), (2, 32), (1, 8), (0, 16), (0, 32))
 GROUPS = (8, 16, 32)
 _MEM = {}
 
