@@ -758,7 +758,7 @@ def main():
 KERNEL_DOC = """Single-kernel timing cases (``python bench.py kernel CASE SHAPE``).
 
     python bench.py kernel umma_gemm M,N,K [--planes 3] [--reps 5] [--kc 16] [--form 1|2|0]
-    python bench.py kernel umma_trace P1,P2,K1,K2 [--planes 3]
+    python bench.py kernel umma_trace P1,P2,K1,K2 [--planes 3|2] [--layout flat|rows]
     python bench.py kernel dgemm M,N,K
     python bench.py kernel spd_inverse N
     python bench.py kernel harmonic 1        (config-1 harmonic-basis solve)
@@ -824,20 +824,39 @@ def umma_gemm_case(M, N, K, planes=3, with_outputs=True):
     return fn, 2.0 * M * N * K * nt, err
 
 
-def umma_trace_case(P1, P2, K1, K2, planes=3, splits=0):
-    """Closure launching one split-product trace contraction into an FP64 F."""
+def umma_trace_case(P1, P2, K1, K2, planes=3, splits=0, layout="flat"):
+    """Closure launching one split-product trace contraction into an FP64 F.
+
+    Three planes: the six BF16x6 products; two planes: the four products of the
+    mixed Fisher's stored slabs.  layout "flat": each parameter's (k, l) block
+    contiguous; "rows": the Fisher's segment buffers, X with the parameters'
+    column slabs side by side along each row k (X[k][p K2 + l]), Y = their
+    transposes, parameter-major (Y[q K1 + k][l])."""
     lib = _lib.lib()
-    nt, ta, tb, keep = _terms(planes)
+    if planes == 2:
+        t4 = ([0, 0, 1, 1], [0, 1, 0, 1])
+        ta_ = (ctypes.c_int * 4)(*t4[0])
+        tb_ = (ctypes.c_int * 4)(*t4[1])
+        nt, ta, tb, keep = 4, ctypes.cast(ta_, ctypes.c_void_p), ctypes.cast(tb_, ctypes.c_void_p), (ta_, tb_)
+    else:
+        nt, ta, tb, keep = _terms(planes)
     g = torch.Generator(device="cuda").manual_seed(1)
     K2p = (K2 + 7) // 8 * 8
-    Xp = torch.randn((planes, P1, K1, K2p), device="cuda", generator=g).to(torch.bfloat16)
-    Yp = torch.randn((planes, P2, K1, K2p), device="cuda", generator=g).to(torch.bfloat16)
+    Xp = torch.empty((planes, P1 * K1 * K2p), dtype=torch.bfloat16, device="cuda")
+    Yp = torch.empty((planes, P2 * K1 * K2p), dtype=torch.bfloat16, device="cuda")
+    for p in range(planes):
+        Xp[p].normal_(generator=g)
+        Yp[p].normal_(generator=g)
+    if layout == "rows":
+        sX, ldX = K2p, P1 * K2p
+    else:
+        sX, ldX = K1 * K2p, K2p
     F = torch.zeros((P1, P2), dtype=torch.float64, device="cuda")
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
     st = torch.cuda.current_stream().cuda_stream
 
     def fn():
-        rc = lib.cf_umma_trace_bf16(P1, P2, K1, K2, nt, ta, tb, Xp.data_ptr(), K1 * K2p, K2p, P1 * K1 * K2p, planes,
+        rc = lib.cf_umma_trace_bf16(P1, P2, K1, K2, nt, ta, tb, Xp.data_ptr(), sX, ldX, P1 * K1 * K2p, planes,
                                     Yp.data_ptr(), K1 * K2p, K2p, P2 * K1 * K2p, planes, 1.0, F.data_ptr(), P2, 0, 0,
                                     0, splits, err.data_ptr(), st)
         if rc != 0:
@@ -970,6 +989,8 @@ def kernel_main(argv=None):
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--kc", type=int, default=16, help="promotion interval of the tensor-core kernels")
     ap.add_argument("--splits", type=int, default=0)
+    ap.add_argument("--layout", choices=["flat", "rows"], default="flat",
+                    help="umma_trace: parameter-major X, or the Fisher's segment buffers")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed", help="map_solves and lnl")
     ap.add_argument("--form", type=int, choices=[0, 1, 2], default=1,
                     help="tensor-core GEMM form: 1 = all planes per 32-wide k-slice, 2 = the same on CTA pairs, "
@@ -982,7 +1003,7 @@ def kernel_main(argv=None):
     if a.case == "umma_gemm":
         fn, fl, err = umma_gemm_case(*dims, planes=a.planes)
     elif a.case == "umma_trace":
-        fn, fl, err = umma_trace_case(*dims, planes=a.planes, splits=a.splits)
+        fn, fl, err = umma_trace_case(*dims, planes=a.planes, splits=a.splits, layout=a.layout)
     elif a.case == "dgemm":
         fn, fl, err = dgemm_case(*dims)
     elif a.case == "harmonic":
