@@ -349,6 +349,15 @@ def secondary(args, dev):
     ms_tc, r_tc = _cuda_ms(torch, lambda: E.lnl(cl, N, X, noise_scale=s, precision="mixed", build="basis_tc"), 3)
     d = (res["mixed"][1][2] - res["fp64"][1][2]).abs()
     d_tc = (r_tc[2] - res["fp64"][1][2]).abs()
+    # the autotuner's verified choice for this problem (product kernel and C build,
+    # |dlnL| <= 0.05 against FP64 on its probe points with these maps)
+    from cosmoforge_b200 import autotune
+
+    choice, _ = autotune.tune_lnl(E, N, X, "mixed", batches=(1024,), use_cache=False)
+    prev_t = E.lib.cf_potrf_f32_set_tensor(choice["tensor"])
+    ms_tu, r_tu = _cuda_ms(torch, lambda: E.lnl(cl, N, X, noise_scale=s, precision="mixed", build=choice["build"]), 3)
+    E.lib.cf_potrf_f32_set_tensor(prev_t)
+    d_tu = (r_tu[2] - res["fp64"][1][2]).abs()
     lnl = {"workload": "config3_tqu_nside8_lnl", "n_pixels": L.n, "points_per_batch": 1024,
            "fp64_evals_per_s": 1024 / res["fp64"][0] * 1e3, "mixed_evals_per_s": 1024 / res["mixed"][0] * 1e3,
            "fp64_graph_evals_per_s": 1024 / graph_ms["fp64"] * 1e3,
@@ -358,6 +367,8 @@ def secondary(args, dev):
            "mixed_tc_build_evals_per_s": 1024 / ms_tc * 1e3,
            "mixed_tc_build_over_fp64": res["fp64"][0] / ms_tc,
            "mixed_tc_build_max_abs_dlnL": float(d_tc.max()),
+           "mixed_tuned": {"choice": choice, "evals_per_s": 1024 / ms_tu * 1e3, "over_fp64": res["fp64"][0] / ms_tu,
+                           "max_abs_dlnL": float(d_tu.max())},
            "build": "lower triangle of C(theta) from the per-multipole basis (one FP64 GEMM per block region; "
                     "mixed: the FP32 copy from the same epilogue); tc build: C in FP32 from BF16x6 tensor-core "
                     "products",

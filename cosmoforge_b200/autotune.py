@@ -295,20 +295,22 @@ def tune_patches(problems, device=None, candidates=(1, 2, 3, 4, 6), reps: int = 
 # ---------------------------------------------------------------------------
 def tune_lnl(E, N, X, precision: str = "mixed", batches=(128, 256, 512, 1024), tol: float = 0.05,
              probe_points: int = 256, use_cache: bool = True):
-    """{"batch": B, "tensor": 0/1} for engine.LnlGraph / PICSLike on this layout.
+    """{"batch": B, "tensor": 0/1, "build": ...} for engine.LnlGraph / PICSLike on this layout.
 
     Every candidate runs the probe points (scrambled Sobol points of the
     five-parameter model box) through a captured LnlGraph; the mixed form's
-    FP32 product kernel (tensor-core BF16x6 or SIMT) must keep |dlnL| <= tol
-    against the FP64 evaluation of the same points.  The fastest per point
-    wins; cached per layout shape, precision and device."""
+    FP32 product kernel (tensor-core BF16x6 or SIMT) and its build of C(theta)
+    ("auto": FP64 basis GEMM with the FP32 copy; "basis_tc": the FP32 C from
+    tensor-core products, chi2 refined against it) must keep |dlnL| <= tol
+    against the FP64 evaluation of the same points, on the caller's maps.
+    The fastest per point wins; cached per layout shape, precision and device."""
     from . import engine as eng
     from . import workloads
     from .sampler import ModelTables
 
     L = E.L
     fields = ",".join(f"{f.spin}:{f.nrows}" for f in L.fields)
-    key = f"lnl|{precision}|n{L.n}|{fields}|L{L.lmax_signal}|{torch.cuda.get_device_name(E.dev)}"
+    key = f"lnl2|{precision}|n{L.n}|{fields}|L{L.lmax_signal}|{torch.cuda.get_device_name(E.dev)}"
     if use_cache:
         got = _load_value(key)
         if got is not None:
@@ -319,26 +321,31 @@ def tune_lnl(E, N, X, precision: str = "mixed", batches=(128, 256, 512, 1024), t
     _, _, ref, _ = E.lnl(tabs, N, X, noise_scale=sc, precision="fp64")
     lib = E.lib
     kernels = (1, 0) if precision == "mixed" else (1,)
+    builds = ("auto",)
+    if precision == "mixed" and eng.SignalBasis.bytes_needed(L) <= 4 << 30:
+        builds = ("auto", "basis_tc")
     prev = lib.cf_potrf_f32_set_tensor(1)
     results = []
     free = torch.cuda.mem_get_info(E.dev)[0]
     try:
-        for tensor in kernels:
-            lib.cf_potrf_f32_set_tensor(tensor)
-            for B in batches:
-                if 4 * B * L.n * L.n * 8 > 0.6 * free:  # C, its FP32 copy and the workspaces
-                    continue
-                G = eng.LnlGraph(E, N, X, B, precision=precision)
-                got = [G(tabs[b0:b0 + B], sc[b0:b0 + B]) for b0 in range(0, probe_points, B)]
-                lnl = torch.cat([r[2] for r in got])
-                err = float((lnl - ref).abs().max())
-                ms = _graph_ms(lambda: G(tabs[:B], sc[:B]), 3)
-                results.append({"batch": B, "tensor": tensor, "us_per_point": 1e3 * ms / B, "max_abs_dlnL": err})
-                del G
+        for build in builds:
+            for tensor in kernels:
+                lib.cf_potrf_f32_set_tensor(tensor)
+                for B in batches:
+                    if 4 * B * L.n * L.n * 8 > 0.6 * free:  # C, its FP32 copy and the workspaces
+                        continue
+                    G = eng.LnlGraph(E, N, X, B, precision=precision, build=build)
+                    got = [G(tabs[b0:b0 + B], sc[b0:b0 + B]) for b0 in range(0, probe_points, B)]
+                    lnl = torch.cat([r[2] for r in got])
+                    err = float((lnl - ref).abs().max())
+                    ms = _graph_ms(lambda: G(tabs[:B], sc[:B]), 3)
+                    results.append({"batch": B, "tensor": tensor, "build": build, "us_per_point": 1e3 * ms / B,
+                                    "max_abs_dlnL": err})
+                    del G
     finally:
         lib.cf_potrf_f32_set_tensor(prev)
     ok = [r for r in results if r["max_abs_dlnL"] <= tol] or results
     best = min(ok, key=lambda r: r["us_per_point"])
-    choice = {"batch": best["batch"], "tensor": best["tensor"]}
+    choice = {"batch": best["batch"], "tensor": best["tensor"], "build": best["build"]}
     _store_value(key, choice, {"candidates": results})
     return choice, {"candidates": results}
