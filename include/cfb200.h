@@ -371,10 +371,11 @@ int cf_umma_set_trace_pairs(int on);
 /* Form of cf_umma_gemm_bf16: 1 (default) loads every plane of a 32-wide
  * k-slice into one pipeline stage and keeps the leading product apart from
  * the corrections in a second TMEM accumulator, when both operands carry the
- * same 2 or 3 planes; 2 does the same for three planes on CTA pairs
- * (clusters of two CTAs on neighbouring SMs, tcgen05.mma.cta_group::2 on
- * 256-row tiles, each CTA holding half of B); 0 walks 64-wide k-tiles term by
- * term.  Returns the previous setting.  No counterpart in the reference. */
+ * same 2 or 3 planes; 2 does the same for three planes of 64-wide k-tiles
+ * on CTA pairs (clusters of two CTAs on neighbouring SMs,
+ * tcgen05.mma.cta_group::2 on 256-row tiles, each CTA holding half of B,
+ * two stages of 96 KB per CTA); 0 walks 64-wide k-tiles term by term.
+ * Returns the previous setting.  No counterpart in the reference. */
 int cf_umma_set_all_planes(int on);
 
 /* Row tiles per group in the persistent tile order of the tcgen05 kernels
