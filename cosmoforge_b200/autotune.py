@@ -2,9 +2,9 @@
 patch batches' size buckets and the batched likelihood's launch shape.
 
 For each spectrum it times the candidate forms of the split-product GEMM
-(``cf_umma_gemm_bf16``: all planes of a 32-wide k-slice per stage with
-split accumulators, on one CTA or a CTA pair per tile, or 64-wide k-tiles term
-by term), promotion
+(``cf_umma_gemm_bf16``: all planes of a k-slice per stage with split
+accumulators, 32-wide on one CTA per tile or 64-wide on a CTA pair, or 64-wide
+k-tiles term by term), promotion
 intervals and the row-tile group of the persistent tile order on the
 spectrum's own operands, checks every candidate's accuracy where it matters
 for the Fisher matrix, and keeps the fastest one within tolerance:
@@ -22,8 +22,10 @@ for the Fisher matrix, and keeps the fastest one within tolerance:
 
 ``tune_patches`` picks the number of size buckets of ``batch.PatchBatch``
 (the fastest graph replay); ``tune_lnl`` the points per captured likelihood
-graph and the FP32 factor's product kernel (tensor-core BF16x6 or SIMT, the
-latter kept only if it is faster within the lnL tolerance).
+graph, the FP32 factor's product kernel (tensor-core BF16x6 or SIMT) and the
+build of C(theta) (the FP64 basis GEMM with its FP32 copy, or the FP32 C from
+tensor-core products), each kept only within the lnL tolerance on the
+caller's maps.
 
 Results are cached per (scheme, problem shape, device) in-process and in a
 JSON file (``CFB200_TUNE_CACHE``, default ``~/.cache/cosmoforge_b200/
